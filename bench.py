@@ -1,0 +1,353 @@
+"""Benchmark of the viscous KT step (cell-updates per second).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload glauber_161x161x41] [--precision fp64|mixed]
+
+A step is one TVDRK2 time step (two RK stages) of the whole grid.  The
+default workload is the 3+1D Milne event of 161x161x41 cells (dx = dy = 0.1
+fm, d eta = 0.25, dtau = 0.02 fm/c from tau0 = 0.6 fm/c), MC-Glauber Pb+Pb at
+b = 7 fm (seed 0), synthetic EOS table, eta/s = 0.08, FP64.  The device state
+(52 arrays x 1.3 M cells, 545 MB in FP64) is larger than L2, so no flush is
+needed between steps.  value = interior cells x steps / device seconds.
+
+One process per GPU; with N > 1 every rank evolves its own replica of the
+event (the step does not shard: replicas only), value is the sum over ranks
+and the time the max over ranks.
+
+--impl reference times the reference's own CPU step (its NEWEST5 headers
+built in oracle/_ref, TVDRK2 on a 40x40x10 Milne grid, the compile-time grid
+of its default scenario block) in one process per host core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="glauber_161x161x41")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- reference CPU
+
+
+def _ref_worker(args):
+    """One process: the reference's TVDRK2 on its compile-time 3+1D grid for
+    about `seconds` seconds; returns (interior cells x steps, seconds)."""
+    seconds, seed = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from pyoracle import Oracle, OracleConfig, RefBuild, smooth_state
+    R = RefBuild("milne_3d")
+    x, y, z = R.coords()
+    tau, ts = 0.6, 0.02
+    f = smooth_state(x, y, z, tau, ts, seed=seed)
+    O = Oracle(OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=R.gz - 6, boost_invariant=False, dx=R.dx, dy=R.dy,
+                            dz=R.dz, eos_kind=0, eos_a=R.factor, etas0=1 / (4 * math.pi), hbarc=R.gevfm))
+    O.set_state(f)
+    O.fill_tmunu(tau)
+    R.set_state(O.get_state())
+    cells = (R.ir - R.il) * (R.jr - R.jl) * (R.kr - R.kl)
+    R.step(tau, ts)  # warm-up
+    tau += ts
+    n, t0 = 0, time.perf_counter()
+    while True:
+        R.step(tau, ts)
+        tau += ts
+        n += 1
+        dt = time.perf_counter() - t0
+        if dt >= seconds:
+            break
+    return cells * n, dt
+
+
+def cpu_reference(seconds: float, procs: int):
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(seconds, s) for s in range(procs)])
+    rate = sum(c / t for c, t in res)
+    return rate, procs
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_procs() -> int:
+    n = os.cpu_count() or 1
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    return max(1, min(n, 64))
+
+
+# ---------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for line in (self.out or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                               parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workload
+
+
+def build_workload(name: str, precision: str):
+    from viral_b200 import _abi as A
+    from viral_b200 import configs as C
+    prec = A.PREC_MIXED if precision == "mixed" else A.PREC_FP64
+    if name == "glauber_161x161x41":
+        cfg = C.glauber_config(precision=prec)
+        inp = C.glauber_inputs(cfg, b=7.0, seed=0)
+        desc = {"workload": "glauber_161x161x41", "grid": [161, 161, 41], "coords": "milne", "dx_fm": 0.1,
+                "deta": 0.25, "dtau_fm": 0.02, "tau0_fm": 0.6, "eos": "synthetic table (2000 rows)",
+                "eta_over_s": 0.08, "ic": "MC-Glauber Pb+Pb b=7 fm seed 0, 208 nucleons, sigma_nn=6.4 fm^2",
+                "recon": "WENO5", "precision": precision}
+    elif name == "gubser_129":
+        cfg = C.gubser_config(precision=prec)
+        inp = C.gubser_inputs(cfg)
+        desc = {"workload": "gubser_129", "grid": [129, 129, 1], "coords": "milne (boost invariant)",
+                "dx_fm": 0.1, "dtau_fm": 0.01, "tau0_fm": 1.0, "eos": "conformal", "eta_over_s": 0.2,
+                "recon": "WENO5", "precision": precision}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return cfg, inp, desc
+
+
+def algorithmic_bytes(cfg, kernel: str) -> float:
+    """Bytes one launch of `kernel` must move per interior cell (state words
+    it has to read and write once; halo re-reads not counted)."""
+    w = 4 if cfg.precision == 1 else 8
+    if kernel.startswith("k_dir"):
+        # reads e, u(4), T(4), pi(5); writes (or read+writes) res(9) and du(4)
+        first = kernel.endswith("x")
+        return w * (14 + (9 if first else 18) + 4)
+    if kernel == "k_update_stage1":
+        # reads res 9, du 12, e, u 4, pu 4, A 9; writes B 9, v1t 4, e, u 4, pu 4
+        return w * (9 + 12 + 1 + 4 + 4 + 9 + 9 + 4 + 1 + 4 + 4)
+    # stage 2: reads res 9, du 12, e, u 4, pu 4, B 9, A 4, v1t 4; writes A 9, e, u 4
+    return w * (9 + 12 + 1 + 4 + 4 + 9 + 4 + 4 + 9 + 1 + 4)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_ours(args, rank, world, dist):
+    import numpy as np
+    import torch
+    from viral_b200 import _abi as A
+    from viral_b200 import configs as C
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    cfg, inp, desc = build_workload(args.workload, args.precision)
+    H = C.make_hydro(cfg, inp)
+    A.check(A.lib().vh_set_stream(H.h, ctypes_void_p(stream.cuda_stream)), H.h)
+    cells = cfg.nx * cfg.ny * (1 if cfg.boost_invariant else cfg.nz)
+    launches_per_step = 2 * ((2 if cfg.boost_invariant else 3) + 1)
+
+    H.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        H.step(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = cells * args.steps * world / (ms / 1e3)
+
+    # per-kernel device times (outside the timed region) for the roofline
+    kt = H.time_kernels(2)
+    names = ["k_dir_x", "k_dir_y", "k_dir_eta", "k_update_stage1", "k_update_stage2"]
+    launches = {"k_dir_x": 4, "k_dir_y": 4, "k_dir_eta": 0 if cfg.boost_invariant else 4, "k_update_stage1": 2,
+                "k_update_stage2": 2}
+    per_launch = {nm: (kt[q] / launches[nm] if launches[nm] else 0.0) for q, nm in enumerate(names)}
+    share = {nm: kt[q] / max(sum(kt), 1e-30) for q, nm in enumerate(names)}
+    top = max(names, key=lambda nm: kt[names.index(nm)])
+    peak, peak_kind = measured_peaks()
+    ach = algorithmic_bytes(cfg, top) * cells / (per_launch[top] / 1e3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers
+    n18 = 18 * H.n
+    host = torch.empty(n18, dtype=torch.float64, pin_memory=True).numpy()
+    H_state = H.get_state()
+    host[:] = H_state.reshape(-1)
+    tau_now = H.tau
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        A.check(A.lib().vh_set_state(H.h, A.ptr(host), tau_now), H.h)
+        H.step(1)
+        A.check(A.lib().vh_get_state(H.h, A.ptr(host)), H.h)
+        tau_now += cfg.dtau
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_value = cells * args.e2e_steps * world / (e2e_ms / 1e3)
+    H.close()
+
+    out = None
+    if rank == 0:
+        clocks = clk.summary()
+        out = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if cfg.precision == 0 else "f32 state / f64 root-find",
+            "data": "synthetic (seeded MC-Glauber initial state)",
+            "config": dict(desc, interior_cells=cells, parallelism=f"replicas x{world}",
+                           l2="state (52 arrays, %.0f MB) larger than the 126 MB L2; no flush" %
+                              (52 * H_state.shape[1] * (8 if cfg.precision == 0 else 4) / 1e6)),
+            "clocks": clocks,
+            "gpu_launches": launches_per_step * args.steps,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n18 * 8, "d2h_bytes_per_step": n18 * 8,
+                    "what": "vh_set_state (pinned host) + vh_step(1) + vh_get_state per step"},
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_cell": algorithmic_bytes(cfg, top),
+                         "kernel_ms_per_launch": per_launch, "kernel_share": share},
+        }
+    return out
+
+
+def ctypes_void_p(v):
+    import ctypes
+    return ctypes.c_void_p(v)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        t0 = time.perf_counter()
+        procs = reference_procs()
+        rates = []
+        for s in range(args.warmup + args.steps):
+            r, _ = cpu_reference(max(1.0, args.cpu_seconds / max(1, args.steps + args.warmup)), procs)
+            if s >= args.warmup:
+                rates.append(r)
+        value = statistics.mean(rates)
+        out = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded smooth viscous state)",
+               "config": {"workload": args.workload, "sample": "reference TVDRK2 on its compile-time 40x40x10 grid"},
+               "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference",
+                                "sample": f"{procs} processes x reference TVDRK2 (NEWEST5 headers, 1 MPI rank "
+                                          f"each) on 40x40x10 cells; {cpu_model()}"},
+               "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+               "wall_s": time.perf_counter() - t0}
+        print(json.dumps(out), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    out = run_ours(args, rank, world, dist)
+    if rank == 0:
+        if world == 1:
+            procs = reference_procs()
+            rate, cores = cpu_reference(args.cpu_seconds, procs)
+            out["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference",
+                                   "sample": f"{cores} processes x reference TVDRK2 (NEWEST5 headers, 1 MPI rank "
+                                             f"each) on 40x40x10 cells for {args.cpu_seconds:.0f} s; {cpu_model()}"}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

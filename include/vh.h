@@ -1,0 +1,189 @@
+/* vh.h - C ABI of the B200 viscous Kurganov-Tadmor hydro step.
+ *
+ * Drop-in boundary for the CPU step of rjfries/VIRAL ("3-1ViscousHydro").
+ * The reference has no library API: its step is TVDRK2(GRID, tau, ts)
+ * operating on a global grid (NEWEST5/time.h:333), initialised by
+ * init(tau, ts) (NEWEST5/init.h:556), stopped by MaxTempGev (NEWEST5/
+ * utils.h:263) and written by WriteResults[XY] (NEWEST5/write.h:51,225).
+ * This header replaces those entry points with a handle-based interface:
+ * no globals, no exit(), plain pointers and sizes, an int status on every
+ * call.  Every entry point cites the reference routine it stands in for.
+ *
+ * State layout (host and device): structure of arrays over the
+ * ghost-inclusive grid GX x GY x GZ with GX = nx + 6, GY = ny + 6,
+ * GZ = nz + 6 (or 1 when boost invariant), index (k*GY + j)*GX + i, x
+ * fastest; 3 ghost layers per face as the reference's BORDER
+ * (NEWEST5/maindef.h:369-371).  The 18 state fields, in this order:
+ *   0 e, 1..4 u^tau u^x u^y u^eta, 5..9 pi^xx pi^yy pi^xy pi^x-eta pi^y-eta,
+ *   10..13 T^{tau tau} T^{tau x} T^{tau y} T^{tau eta}, 14..17 previous u^mu
+ * (the reference's cell fields En, u[4], pi[5], T00..T30, prevu[4],
+ * NEWEST5/maindef.h:392-466).  Units: fm^-4 for e, pi and T^{mu nu},
+ * fm^-1 for temperature, fm for lengths, fm/c for tau.
+ *
+ * Threading: one handle per host thread; calls on a handle are issued on
+ * that handle's CUDA stream (vh_set_stream) and do not synchronise except
+ * where a result is returned to the host.
+ */
+#ifndef VH_H
+#define VH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VH_NFIELDS 18
+#define VH_NGHOST 3
+
+typedef enum {
+  VH_OK = 0,
+  VH_E_ARG = 1,        /* bad argument (null pointer, size, enum) */
+  VH_E_CUDA = 2,       /* a CUDA call failed; see vh_last_error */
+  VH_E_ROOTFIND = 3,   /* conserved-to-primitive Newton failed in some cell
+                          (NEWEST5/multiroot.h:398-420 exits there) */
+  VH_E_CAUSALITY = 4,  /* |v| >= 1 after the root-find (multiroot.h:480-488) */
+  VH_E_NEG_ENERGY = 5, /* e <= 0 after the root-find (multiroot.h:480-488) */
+  VH_E_TIMEOUT = 6,    /* a bounded device wait ran out */
+  VH_E_STATE = 7,      /* call out of order (e.g. step before state is set) */
+  VH_E_NOMEM = 8,      /* device allocation failed */
+  VH_E_UNSUPPORTED = 9 /* option not built into this library */
+} vh_status;
+
+enum { VH_COORD_MILNE = 0, VH_COORD_CARTESIAN = 1 };
+enum { VH_PREC_FP64 = 0, VH_PREC_MIXED = 1 };
+enum { VH_RECON_WENO5 = 0, VH_RECON_MINMOD = 1 };
+enum { VH_EOS_CONFORMAL = 0, VH_EOS_TABLE = 1 };
+/* relaxation time: 1.5 eta / P (NEWEST5/maindef.h:69,126,286) or
+ * 5 eta / (e + P) (NEWEST5/maindef.h:339, the Gubser test) */
+enum { VH_TAUPI_15_ETA_OVER_P = 0, VH_TAUPI_5_ETA_OVER_EPP = 1 };
+/* initial pi: given, zero, or Navier-Stokes (NEWEST5/Source.h:535-630) */
+enum { VH_PI_GIVEN = 0, VH_PI_ZERO = 1, VH_PI_NS = 2 };
+/* snapshot layouts of NEWEST5/write.h: one xy plane, or the full grid */
+enum { VH_WRITE_XY = 0, VH_WRITE_FULL = 1 };
+
+typedef struct {
+  int coords;           /* VH_COORD_* (NEWEST5 Milne, TXYZ5 Cartesian) */
+  int precision;        /* VH_PREC_FP64, or VH_PREC_MIXED: FP32 state, fluxes,
+                           reconstruction and sources; FP64 root-find, EOS
+                           inversion and compensated conservation sums */
+  int recon;            /* VH_RECON_* */
+  int nx, ny, nz;       /* interior cells (nz = 1 when boost_invariant) */
+  int boost_invariant;  /* 1: no eta direction, no eta ghosts (reference LBI) */
+  double dx, dy, dz;    /* cell sizes (fm, fm, 1 or fm) */
+  double tau0, dtau;    /* start time and step (fm/c) */
+  int eos_kind;         /* VH_EOS_* */
+  double eos_a;         /* conformal EOS: e = a T^4 in fm units */
+  int eos_n;            /* table rows (log-spaced in e, increasing) */
+  const double* eos_e;  /* table: e (fm^-4) */
+  const double* eos_p;  /* table: P (fm^-4) */
+  const double* eos_cs2;/* table: dP/de */
+  const double* eos_t;  /* table: T (fm^-1) */
+  /* eta/s(T) = etas0 + etas1 * max(T*hbarc - etas_tc, 0), T*hbarc in GeV */
+  double etas0, etas1, etas_tc, hbarc;
+  int taupi_kind;       /* VH_TAUPI_* */
+  int gubser_mirror;    /* ghost u^x,u^y mirrored across the face (NEWEST5/
+                           boundary.h:32-37, Gubser test) */
+  double minmod_theta;  /* generalized-minmod theta (NEWEST5/maindef.h:370) */
+} vh_config;
+
+typedef struct vh_handle vh_handle;
+
+/* Create a handle and allocate the device state for one event.
+ * Replaces StoreInHeap/init bookkeeping (NEWEST5/alloc.h:33, init.h:556-589). */
+int vh_create(const vh_config* cfg, vh_handle** out);
+/* Free everything (NEWEST5/alloc.h FreeFromHeap). */
+int vh_destroy(vh_handle* h);
+/* Issue all later work on this cudaStream_t (NULL: the legacy stream). */
+int vh_set_stream(vh_handle* h, void* stream);
+/* Extents of the ghost-inclusive grid. */
+int vh_dims(const vh_handle* h, int* gx, int* gy, int* gz);
+
+/* Full state from / to host memory, 18 fields x GX*GY*GZ doubles.
+ * Setting the state sets the current time to tau. */
+int vh_set_state(vh_handle* h, const double* host, double tau);
+int vh_get_state(vh_handle* h, double* host);
+/* The same with device pointers to 18 x G doubles (no host copies). */
+int vh_set_state_device(vh_handle* h, const double* dev, double tau);
+int vh_get_state_device(vh_handle* h, double* dev);
+
+/* Initialise from a profile (the reference's init(tau, ts) with a scenario,
+ * NEWEST5/init.h:556-704): e, u^x, u^y, u^eta on the ghost-inclusive grid
+ * (u^tau from normalisation), optional previous velocity prevu (4 fields;
+ * NULL: prevu = u), and pi by pi_mode: VH_PI_GIVEN takes pi5 (5 fields),
+ * VH_PI_ZERO sets 0, VH_PI_NS computes Navier-Stokes pi on every cell
+ * (NEWEST5/Source.h:607-630).  T^{tau mu} follows from (e,u,pi)
+ * (NEWEST5/init.h:539-549).  Host arrays of G doubles each. */
+int vh_init_profile(vh_handle* h, double tau, const double* e, const double* ux, const double* uy,
+                    const double* ueta, const double* prevu4, int pi_mode, const double* pi5);
+
+/* Advance nsteps TVDRK2 steps of dtau (NEWEST5/time.h:333 TVDRK2, called
+ * from the main loop NEWEST5/main.cpp:132-206).  Returns VH_E_ROOTFIND /
+ * VH_E_CAUSALITY / VH_E_NEG_ENERGY if a cell failed (the state is then
+ * that of the failing step). */
+int vh_step(vh_handle* h, int nsteps);
+/* Current time tau. */
+int vh_get_time(const vh_handle* h, double* tau);
+
+/* Maximum temperature over the interior in GeV (NEWEST5/utils.h:263). */
+int vh_max_temperature(vh_handle* h, double* tmax_gev);
+/* Compensated FP64 sums over the interior of tau*T^{tau mu} times the cell
+ * volume: out[4] = {E, Px, Py, Peta} (conservation monitor). */
+int vh_conservation_sums(vh_handle* h, double* out4);
+/* Largest signal speed over the interior faces and the CFL step
+ * dx/(8 max|lambda|) the reference suggests (NEWEST5/hydroKT.h:317-344). */
+int vh_cfl(vh_handle* h, double* max_speed, double* dtau_suggest);
+
+/* Snapshot in the reference's binary layout: 12 doubles per interior cell
+ * (e, T, P, v^x, v^y, v^eta, pi^xx..pi^y-eta, Pi), x outer, y inner, at
+ * the central eta slice (VH_WRITE_XY, NEWEST5/write.h:51-115) or for every
+ * eta slice (VH_WRITE_FULL, NEWEST5/write.h:225-290); `every` keeps every
+ * n-th cell as the reference's FREQ. */
+int vh_write(vh_handle* h, const char* path, int layout, int every);
+
+/* Stage-1 terms for tests: the flux divergence res[9*G], sources src[9*G]
+ * and velocity gradients du[16*G] at the current state (the reference's
+ * CalcSource + hydroExplicit, NEWEST5/Source.h:165, hydroKT.h:391). */
+int vh_debug_stage_terms(vh_handle* h, double* res, double* src, double* du);
+
+/* Diagnostic: advance nsteps steps with a CUDA event pair around every
+ * kernel launch and return device milliseconds summed per kernel kind:
+ * ms_out[0..2] the x / y / eta flux kernels, ms_out[3] the stage-1 update,
+ * ms_out[4] the stage-2 update.  Slower than vh_step (one sync per launch). */
+int vh_time_kernels(vh_handle* h, int nsteps, double* ms_out);
+
+/* Newton iterations of the last step, summed over cells (diagnostic). */
+int vh_last_iterations(vh_handle* h, long long* iters);
+
+/* Message of the last error on this handle (or the last vh_create). */
+const char* vh_last_error(const vh_handle* h);
+
+/* ---------------------------------------------------------------- inputs */
+/* Seeded host generators shared by the GPU path and its tests, so that
+ * identical inputs hold by construction.  All fill ghost-inclusive arrays. */
+
+/* Synthetic tabulated EOS: n rows log-spaced in e over [emin, emax] GeV/fm^3,
+ * c_s^2(e) = 1/3 - 0.2 exp(-ln^2(e/0.5)/2), P(emin) = c_s^2(emin) emin,
+ * T anchored to e = a T^4 at emax; outputs in fm units. */
+int vh_eos_table_synthetic(int n, double emin_gev, double emax_gev, double a, double hbarc,
+                           double* e, double* p, double* cs2, double* t);
+/* Ideal Gubser flow (q, tau0, central temperature in GeV): e, u^x, u^y at
+ * tau0 and the velocity at tau0 - dtau (prevu) for the 2+1D grid. */
+int vh_profile_gubser(int nx, int ny, double dx, double dy, double q, double tau0, double dtau,
+                      double t0_gev, double a, double hbarc, double* e, double* ux, double* uy,
+                      double* prevu4);
+/* Monte-Carlo Glauber energy density (two Woods-Saxon nuclei): A nucleons
+ * per nucleus, radius R, diffuseness aws, hard core dmin, impact parameter
+ * b, sigma_nn (fm^2), Gaussian width w per participant, peak e in GeV/fm^3,
+ * eta plateau half-width and Gaussian tail width; seed.  Writes e (fm^-4)
+ * on the ghost-inclusive grid and returns the participant count in *npart. */
+int vh_profile_glauber(int nx, int ny, int nz, int boost_invariant, double dx, double dy, double dz,
+                       int A, double R, double aws, double dmin, double b, double sigma_nn,
+                       double w, double epeak_gev, double eta_flat, double eta_sigma,
+                       double hbarc, uint64_t seed, double* e, int* npart);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

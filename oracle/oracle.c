@@ -679,6 +679,10 @@ int vho_con2prim(const vho_grid* g, const double* Tt, const double* p, double ta
       if (!(fabs(dx[i]) < 1e-16 * fabs(x[i]) || dx[i] == 0.0)) { conv = 0; break; }
     if (conv) break;
   }
+  /* an iterate that is not a root counts as a failure (the reference keeps
+   * it silently after 100 iterations): residual above 1e-8 of |T^{tau mu}| */
+  double scale = fabs(Tt[0]) + fabs(Tt[1]) + fabs(Tt[2]) + fabs(Tt[3]);
+  if (!(phi <= 1e-8 * scale)) return -1;
   return it;
 }
 

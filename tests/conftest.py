@@ -1,0 +1,58 @@
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libvh.so")
+
+
+def _ensure_oracle():
+    lib = os.path.join(ROOT, "oracle", "liboracle.so")
+    src = os.path.join(ROOT, "oracle", "oracle.c")
+    if not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True,
+                       capture_output=True)
+
+
+def _ensure_libvh():
+    from viral_b200 import build
+    build.build()
+
+
+@pytest.fixture(scope="session", autouse=True)
+def built_libs():
+    _ensure_oracle()
+    _ensure_libvh()
+
+
+def gpu_available() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def pytest_collection_modifyitems(config, items):
+    if gpu_available():
+        return
+    skip = pytest.mark.skip(reason="no CUDA GPU in this environment")
+    for it in items:
+        if "gpu" in it.keywords:
+            it.add_marker(skip)
+
+
+def rel_err(a, b):
+    """max |a-b| / max |b| (0 when both vanish)."""
+    a = np.asarray(a); b = np.asarray(b)
+    den = np.max(np.abs(b))
+    num = np.max(np.abs(a - b))
+    return 0.0 if num == 0 else num / (den if den > 0 else 1.0)

@@ -1,0 +1,180 @@
+"""GPU step versus the oracle (FP64 mode) through the C ABI.
+
+Tolerances: the FP64 GPU step and the oracle differ only by rounding
+(fused multiply-adds, division and pow implementations), so single-stage
+terms agree to 1e-12 relative (max norm over the grid) and full runs to
+1e-10 relative, the FP64 bar of the reference comparison.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from helpers import interior_mask, oracle_config, oracle_from_inputs, smooth_inputs
+from pyoracle import Oracle
+from viral_b200 import _abi as A
+from viral_b200 import configs as C
+from viral_b200.hydro import Config, Hydro
+
+pytestmark = pytest.mark.gpu
+
+STAGE_TOL = 1e-12
+RUN_TOL = 1e-10
+
+
+def milne3d(**kw):
+    base = dict(nx=20, ny=18, nz=12, boost_invariant=False, dx=0.1, dy=0.1, dz=0.1, tau0=1.3, dtau=0.01,
+                eos_kind=A.EOS_CONFORMAL, eos_a=13.899692864867510, etas0=1 / (4 * np.pi))
+    base.update(kw)
+    return Config(**base)
+
+
+def compare_states(a, b, tol, fields=range(14), mask=None):
+    errs = {}
+    for q in fields:
+        x, y = (a[q], b[q]) if mask is None else (a[q][mask], b[q][mask])
+        errs[q] = rel_err(x, y)
+    worst = max(errs.values())
+    assert worst <= tol, f"max rel err {worst:.3e} > {tol:.1e}: {errs}"
+    return worst
+
+
+@pytest.mark.parametrize("cfgkw", [
+    dict(),
+    dict(boost_invariant=True, nz=1),
+    dict(coords=A.COORD_CARTESIAN, tau0=1.0),
+    dict(recon=A.RECON_MINMOD),
+    dict(eos_kind=A.EOS_TABLE, eos_table=C.eos_table(), etas0=0.08, etas1=1.0),
+    dict(gubser_mirror=True, taupi_kind=A.TAUPI_5_ETA_OVER_EPP, etas0=0.2, boost_invariant=True, nz=1),
+])
+def test_stage_terms_match_oracle(cfgkw):
+    cfg = milne3d(**cfgkw)
+    f = smooth_inputs(cfg, cfg.tau0, seed=11)
+    O = Oracle(oracle_config(cfg))
+    O.set_state(f)
+    so, ro, do = O.stage_terms(cfg.tau0, cfg.dtau)
+    with Hydro(cfg) as H:
+        H.set_state(f, cfg.tau0)
+        rg, sg, dg = H.debug_stage_terms()
+    m = interior_mask(cfg)
+    for l in range(9):
+        assert rel_err(rg[l][m], ro[l][m]) <= STAGE_TOL, f"flux divergence {l}"
+        assert rel_err(sg[l][m], so[l][m]) <= STAGE_TOL, f"source {l}"
+    assert rel_err(dg[:, m], do[:, m]) <= STAGE_TOL
+
+
+@pytest.mark.parametrize("cfgkw", [
+    dict(),
+    dict(boost_invariant=True, nz=1),
+    dict(coords=A.COORD_CARTESIAN, tau0=1.0),
+    dict(recon=A.RECON_MINMOD),
+    dict(eos_kind=A.EOS_TABLE, eos_table=C.eos_table(), etas0=0.08, etas1=1.0),
+])
+def test_steps_match_oracle(cfgkw):
+    cfg = milne3d(**cfgkw)
+    f = smooth_inputs(cfg, cfg.tau0, seed=5)
+    O = Oracle(oracle_config(cfg))
+    O.set_state(f)
+    tau = cfg.tau0
+    for _ in range(4):
+        assert O.step(tau, cfg.dtau) == 0
+        tau += cfg.dtau
+    with Hydro(cfg) as H:
+        H.set_state(f, cfg.tau0)
+        H.step(4)
+        g = H.get_state()
+        assert abs(H.tau - tau) < 1e-12
+    compare_states(g, O.get_state(), 1e-11, fields=range(18))
+
+
+def test_gubser_run_matches_oracle():
+    """The boost-invariant Gubser test (129x129, NS pi, mirrored ghosts),
+    50 steps of the GPU step against the oracle."""
+    cfg = C.gubser_config()
+    inp = C.gubser_inputs(cfg)
+    O = oracle_from_inputs(cfg, inp)
+    with C.make_hydro(cfg, inp) as H:
+        compare_states(H.get_state(), O.get_state(), 1e-13, fields=range(18))
+        tau = cfg.tau0
+        for _ in range(50):
+            assert O.step(tau, cfg.dtau) == 0
+            tau += cfg.dtau
+        H.step(50)
+        compare_states(H.get_state(), O.get_state(), RUN_TOL, fields=range(18))
+        assert abs(H.max_temperature() - O.max_temp_gev()) <= 1e-12 * O.max_temp_gev()
+
+
+def test_glauber_boost_invariant_matches_oracle():
+    cfg = C.glauber_config(nx=64, ny=64, boost_invariant=True)
+    inp = C.glauber_inputs(cfg, b=7.0, seed=3)
+    O = oracle_from_inputs(cfg, inp)
+    with C.make_hydro(cfg, inp) as H:
+        tau = cfg.tau0
+        for _ in range(40):
+            assert O.step(tau, cfg.dtau) == 0
+            tau += cfg.dtau
+        H.step(40)
+        compare_states(H.get_state(), O.get_state(), RUN_TOL, fields=range(18))
+
+
+def test_glauber_3d_matches_oracle():
+    cfg = C.glauber_config(nx=40, ny=36, nz=12, deta=0.25)
+    inp = C.glauber_inputs(cfg, b=7.0, seed=0)
+    O = oracle_from_inputs(cfg, inp)
+    with C.make_hydro(cfg, inp) as H:
+        tau = cfg.tau0
+        for _ in range(10):
+            assert O.step(tau, cfg.dtau) == 0
+            tau += cfg.dtau
+        H.step(10)
+        compare_states(H.get_state(), O.get_state(), RUN_TOL, fields=range(18))
+
+
+def test_mixed_precision_tracks_fp64():
+    """FP32 state/fluxes/sources with the FP64 root-find stay close to the
+    FP64 step on a smooth event (relative max error in e, u, pi)."""
+    cfg64 = C.glauber_config(nx=64, ny=64, boost_invariant=True)
+    cfg32 = C.glauber_config(nx=64, ny=64, boost_invariant=True, precision=A.PREC_MIXED)
+    inp = C.glauber_inputs(cfg64, b=7.0, seed=1)
+    with C.make_hydro(cfg64, inp) as H64, C.make_hydro(cfg32, inp) as H32:
+        H64.step(40)
+        H32.step(40)
+        a, b = H32.get_state(), H64.get_state()
+    m = interior_mask(cfg64)
+    assert rel_err(a[0][m], b[0][m]) < 1e-4
+    for q in (2, 3):
+        assert rel_err(a[q][m], b[q][m]) < 1e-3
+    for q in (5, 6, 7):
+        assert rel_err(a[q][m], b[q][m]) < 1e-2
+
+
+def test_reductions():
+    cfg = C.gubser_config(nx=33, ny=33)
+    inp = C.gubser_inputs(cfg)
+    O = oracle_from_inputs(cfg, inp)
+    f = O.get_state()
+    with Hydro(cfg) as H:
+        H.set_state(f, cfg.tau0)
+        assert abs(H.max_temperature() - O.max_temp_gev()) <= 1e-13
+        sums = H.conservation_sums()
+        m = interior_mask(cfg)
+        ref = [np.sum(cfg.tau0 * f[10 + l][m]) * cfg.dx * cfg.dy for l in range(4)]
+        for l in range(4):
+            assert abs(sums[l] - ref[l]) <= 1e-12 * max(1.0, abs(ref[0]))
+        a, dt = H.cfl()
+        assert 0 < a < 1 and abs(dt - cfg.dx / (8 * a)) < 1e-15
+
+
+def test_step_errors_are_reported():
+    """A superluminal T^{tau mu} makes the root-find fail; the call returns
+    an error status instead of exiting, and the handle stays usable."""
+    cfg = milne3d(boost_invariant=True, nz=1)
+    f = smooth_inputs(cfg, cfg.tau0, seed=2)
+    f[11] *= 50.0  # |T^{tau x}| >> T^{tau tau} in every cell
+    with Hydro(cfg) as H:
+        H.set_state(f, cfg.tau0)
+        with pytest.raises(A.VhError) as ei:
+            H.step(1)
+        assert ei.value.code in (A.E_ROOTFIND, A.E_CAUSALITY, A.E_NEG_ENERGY)
+        good = smooth_inputs(cfg, cfg.tau0, seed=2)
+        H.set_state(good, cfg.tau0)
+        H.step(1)

@@ -1,0 +1,67 @@
+"""Named workloads of the viscous KT step and their inputs.
+
+gubser_129        boost-invariant Gubser test: 129x129, dx = 0.1 fm, q = 1/fm,
+                  tau0 = 1 fm/c, T(0,0) = 0.6 GeV, conformal e = a T^4,
+                  eta/s = 0.2, tau_pi = 5 eta/(e+P), Navier-Stokes pi,
+                  dtau = 0.01 fm/c to tau = 4 fm/c (300 steps), mirrored
+                  u^x,u^y ghosts as the reference's Gubser scenario.
+glauber_161x161x41 3+1D Milne event: 161x161x41, dx = dy = 0.1 fm,
+                  d eta = 0.25, tau0 = 0.6 -> 10 fm/c, dtau = 0.02 (470 steps),
+                  MC-Glauber Pb+Pb b = 7 fm (seed 0), synthetic EOS table,
+                  eta/s = 0.08, tau_pi = 1.5 eta/P, u = 0, pi = 0.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _abi as A
+from .hydro import A_QGP, HBARC, Config, eos_table_synthetic, profile_glauber, profile_gubser
+
+_EOS_CACHE: dict = {}
+
+
+def eos_table() -> np.ndarray:
+    if "t" not in _EOS_CACHE:
+        _EOS_CACHE["t"] = eos_table_synthetic(2000, 1e-3, 500.0, A_QGP, HBARC)
+    return _EOS_CACHE["t"]
+
+
+def gubser_config(nx=129, ny=129, dx=0.1, precision=A.PREC_FP64, recon=A.RECON_WENO5) -> Config:
+    return Config(nx=nx, ny=ny, nz=1, boost_invariant=True, precision=precision, recon=recon, dx=dx, dy=dx,
+                  tau0=1.0, dtau=0.01, eos_kind=A.EOS_CONFORMAL, eos_a=A_QGP, etas0=0.2, etas1=0.0,
+                  taupi_kind=A.TAUPI_5_ETA_OVER_EPP, gubser_mirror=True)
+
+
+def gubser_inputs(cfg: Config, t0_gev=0.6, q=1.0):
+    e, ux, uy, pu = profile_gubser(cfg.nx, cfg.ny, cfg.dx, cfg.dy, q, cfg.tau0, cfg.dtau, t0_gev, cfg.eos_a,
+                                   cfg.hbarc)
+    return dict(tau=cfg.tau0, e=e, ux=ux, uy=uy, ueta=None, prevu=pu, pi_mode=A.PI_NS)
+
+
+def glauber_config(nx=161, ny=161, nz=41, boost_invariant=False, precision=A.PREC_FP64, dx=0.1, deta=0.25,
+                   tau0=0.6, dtau=0.02, etas0=0.08, etas1=0.0, recon=A.RECON_WENO5) -> Config:
+    return Config(nx=nx, ny=ny, nz=(1 if boost_invariant else nz), boost_invariant=boost_invariant,
+                  precision=precision, recon=recon, dx=dx, dy=dx, dz=deta, tau0=tau0, dtau=dtau,
+                  eos_kind=A.EOS_TABLE, eos_table=eos_table(), etas0=etas0, etas1=etas1, etas_tc=0.154,
+                  taupi_kind=A.TAUPI_15_ETA_OVER_P)
+
+
+def glauber_inputs(cfg: Config, b=7.0, seed=0):
+    e, npart = profile_glauber(cfg.nx, cfg.ny, cfg.nz, cfg.boost_invariant, cfg.dx, cfg.dy, cfg.dz, b=b, seed=seed,
+                               hbarc=cfg.hbarc)
+    z = np.zeros_like(e)
+    return dict(tau=cfg.tau0, e=e, ux=z, uy=z, ueta=z, prevu=None, pi_mode=A.PI_ZERO, npart=npart)
+
+
+def make_hydro(cfg: Config, inputs: dict):
+    from .hydro import Hydro
+    h = Hydro(cfg)
+    h.init_profile(inputs["tau"], inputs["e"], inputs["ux"], inputs["uy"], inputs.get("ueta"), inputs.get("prevu"),
+                   inputs["pi_mode"], inputs.get("pi5"))
+    return h
+
+
+def steps_between(t0: float, t1: float, dt: float) -> int:
+    return int(math.floor((t1 - t0) / dt + 0.5))

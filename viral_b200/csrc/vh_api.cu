@@ -1,0 +1,527 @@
+// C ABI of the B200 viscous KT step (include/vh.h): handle, device buffers,
+// state transfer, the TVDRK2 step loop and the reductions.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vh.h"
+#include "vh_aux.cuh"
+#include "vh_internal.h"
+
+using namespace vh;
+
+struct vh_handle {
+  vh_config cfg{};
+  DevCfg C{};
+  cudaStream_t stream = nullptr;
+  bool mixed = false;
+  size_t esz = 8;            // bytes per state element
+  void* state = nullptr;     // 18 canonical fields + B(9) + v1t(4) + res(9) + du(12)
+  double* stage = nullptr;   // 18*n doubles: host<->device staging for the mixed path / du16 scratch
+  double* eos_d = nullptr;
+  float* eos_f = nullptr;
+  unsigned int* status = nullptr;
+  unsigned long long* iters = nullptr;
+  unsigned long long* red = nullptr;  // reduction slots
+  double* part = nullptr;              // conservation partial sums
+  int part_blocks = 0;
+  DevPtrs<double> pd{};
+  DevPtrs<float> pf{};
+  std::vector<double> eos_host;  // 4 x eos_n
+  double tau = 0;
+  bool have_state = false;
+  std::string err;
+};
+
+static std::string g_create_err;
+
+#define VH_CUDA(h, call)                                                                        \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess) {                                                                    \
+      (h)->err = std::string(#call) + ": " + cudaGetErrorString(_e);                            \
+      return VH_E_CUDA;                                                                         \
+    }                                                                                           \
+  } while (0)
+
+static int fail(vh_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+template <class R>
+static void set_ptrs(DevPtrs<R>& P, void* base, long long n, unsigned int* status, unsigned long long* iters) {
+  R* b = static_cast<R*>(base);
+  auto f = [&](int q) { return b + (long long)q * n; };
+  P.e = f(0);
+  for (int l = 0; l < 4; l++) P.u[l] = f(1 + l);
+  for (int l = 0; l < 4; l++) P.A[l] = f(10 + l);
+  for (int l = 0; l < 5; l++) P.A[4 + l] = f(5 + l);
+  for (int l = 0; l < 4; l++) P.pu[l] = f(14 + l);
+  for (int l = 0; l < 9; l++) P.B[l] = f(18 + l);
+  for (int l = 0; l < 4; l++) P.v1t[l] = f(27 + l);
+  for (int l = 0; l < 9; l++) P.res[l] = f(31 + l);
+  for (int l = 0; l < 12; l++) P.du[l] = f(40 + l);
+  P.status = status;
+  P.iters = iters;
+}
+static constexpr int kStateArrays = 52;
+
+template <class R>
+static int set_smem_attrs(vh_handle* h);
+
+static int validate(const vh_config* c, std::string& why) {
+  if (!c) { why = "null config"; return VH_E_ARG; }
+  if (c->coords != VH_COORD_MILNE && c->coords != VH_COORD_CARTESIAN) { why = "coords"; return VH_E_ARG; }
+  if (c->precision != VH_PREC_FP64 && c->precision != VH_PREC_MIXED) { why = "precision"; return VH_E_ARG; }
+  if (c->recon != VH_RECON_WENO5 && c->recon != VH_RECON_MINMOD) { why = "recon"; return VH_E_ARG; }
+  if (c->nx < 3 || c->ny < 3 || (!c->boost_invariant && c->nz < 3)) { why = "grid needs >= 3 interior cells per axis"; return VH_E_ARG; }
+  if (c->boost_invariant && c->nz != 1) { why = "boost-invariant grids have nz = 1"; return VH_E_ARG; }
+  if (!(c->dx > 0 && c->dy > 0 && (c->boost_invariant || c->dz > 0))) { why = "cell sizes"; return VH_E_ARG; }
+  if (!(c->dtau > 0) || (c->coords == VH_COORD_MILNE && !(c->tau0 > 0))) { why = "tau0/dtau"; return VH_E_ARG; }
+  if (c->eos_kind == VH_EOS_CONFORMAL) {
+    if (!(c->eos_a > 0)) { why = "eos_a"; return VH_E_ARG; }
+  } else if (c->eos_kind == VH_EOS_TABLE) {
+    if (c->eos_n < 2 || !c->eos_e || !c->eos_p || !c->eos_cs2 || !c->eos_t) { why = "eos table"; return VH_E_ARG; }
+    for (int i = 1; i < c->eos_n; i++)
+      if (!(c->eos_e[i] > c->eos_e[i - 1])) { why = "eos table e must increase"; return VH_E_ARG; }
+  } else { why = "eos_kind"; return VH_E_ARG; }
+  if (c->taupi_kind != VH_TAUPI_15_ETA_OVER_P && c->taupi_kind != VH_TAUPI_5_ETA_OVER_EPP) { why = "taupi_kind"; return VH_E_ARG; }
+  return VH_OK;
+}
+
+extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
+  std::string why;
+  if (!out) return VH_E_ARG;
+  *out = nullptr;
+  int v = validate(cfg, why);
+  if (v != VH_OK) { g_create_err = "vh_create: " + why; return v; }
+  vh_handle* h = new vh_handle();
+  h->cfg = *cfg;
+  h->cfg.eos_e = h->cfg.eos_p = h->cfg.eos_cs2 = h->cfg.eos_t = nullptr;
+  h->mixed = cfg->precision == VH_PREC_MIXED;
+  h->esz = h->mixed ? 4 : 8;
+  DevCfg& C = h->C;
+  C.nx = cfg->nx; C.ny = cfg->ny; C.nz = cfg->boost_invariant ? 1 : cfg->nz;
+  C.gx = cfg->nx + 2 * NG; C.gy = cfg->ny + 2 * NG; C.gz = cfg->boost_invariant ? 1 : cfg->nz + 2 * NG;
+  C.il = NG; C.ir = NG + cfg->nx; C.jl = NG; C.jr = NG + cfg->ny;
+  C.kl = cfg->boost_invariant ? 0 : NG; C.kr = cfg->boost_invariant ? 1 : NG + cfg->nz;
+  C.n = (long long)C.gx * C.gy * C.gz;
+  C.cart = cfg->coords == VH_COORD_CARTESIAN;
+  C.bi = cfg->boost_invariant != 0;
+  C.recon = cfg->recon;
+  C.mirror = cfg->gubser_mirror != 0;
+  C.dx = cfg->dx; C.dy = cfg->dy; C.dz = cfg->boost_invariant ? 1.0 : cfg->dz;
+  C.eos_kind = cfg->eos_kind; C.eos_a = cfg->eos_a; C.eos_n = 0;
+  C.etas0 = cfg->etas0; C.etas1 = cfg->etas1; C.etas_tc = cfg->etas_tc; C.hbarc = cfg->hbarc;
+  C.taupi_kind = cfg->taupi_kind;
+  C.mm_theta = cfg->minmod_theta;
+  h->tau = cfg->tau0;
+
+  auto bail = [&](cudaError_t e, const char* what) {
+    g_create_err = std::string("vh_create: ") + what + ": " + cudaGetErrorString(e);
+    vh_destroy(h);
+    return e == cudaErrorMemoryAllocation ? VH_E_NOMEM : VH_E_CUDA;
+  };
+  cudaError_t e;
+  if (cfg->eos_kind == VH_EOS_TABLE) {
+    const int n = cfg->eos_n;
+    std::vector<double> t(4 * (size_t)n);
+    std::vector<float> tf(4 * (size_t)n);
+    for (int i = 0; i < n; i++) {
+      t[i] = cfg->eos_e[i]; t[n + i] = cfg->eos_p[i]; t[2 * n + i] = cfg->eos_cs2[i]; t[3 * n + i] = cfg->eos_t[i];
+    }
+    for (size_t i = 0; i < t.size(); i++) tf[i] = (float)t[i];
+    h->eos_host = t;
+    if ((e = cudaMalloc(&h->eos_d, sizeof(double) * t.size())) != cudaSuccess) return bail(e, "eos table");
+    if ((e = cudaMalloc(&h->eos_f, sizeof(float) * t.size())) != cudaSuccess) return bail(e, "eos table");
+    cudaMemcpy(h->eos_d, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->eos_f, tf.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice);
+    C.eos_n = n;
+    C.eos_l0 = std::log(cfg->eos_e[0]);
+    C.eos_idl = (n - 1) / (std::log(cfg->eos_e[n - 1]) - C.eos_l0);
+    C.eos_d = h->eos_d;
+    C.eos_f = h->eos_f;
+  }
+  const size_t bytes = (size_t)kStateArrays * C.n * h->esz;
+  if ((e = cudaMalloc(&h->state, bytes)) != cudaSuccess) return bail(e, "state");
+  if ((e = cudaMemset(h->state, 0, bytes)) != cudaSuccess) return bail(e, "state");
+  if ((e = cudaMalloc(&h->stage, sizeof(double) * 18 * C.n)) != cudaSuccess) return bail(e, "staging");
+  if ((e = cudaMalloc(&h->status, sizeof(unsigned int))) != cudaSuccess) return bail(e, "status");
+  if ((e = cudaMalloc(&h->iters, sizeof(unsigned long long))) != cudaSuccess) return bail(e, "iters");
+  if ((e = cudaMalloc(&h->red, sizeof(unsigned long long) * 4)) != cudaSuccess) return bail(e, "reduce");
+  h->part_blocks = 296;
+  if ((e = cudaMalloc(&h->part, sizeof(double) * 8 * h->part_blocks + 32)) != cudaSuccess) return bail(e, "reduce");
+  cudaMemset(h->status, 0, sizeof(unsigned int));
+  cudaMemset(h->iters, 0, sizeof(unsigned long long));
+  set_ptrs(h->pd, h->state, C.n, h->status, h->iters);
+  set_ptrs(h->pf, h->state, C.n, h->status, h->iters);
+  if ((h->mixed ? set_smem_attrs<float>(h) : set_smem_attrs<double>(h)) != VH_OK) {
+    g_create_err = "vh_create: " + h->err;
+    vh_destroy(h);
+    return VH_E_CUDA;
+  }
+  *out = h;
+  return VH_OK;
+}
+
+extern "C" int vh_destroy(vh_handle* h) {
+  if (!h) return VH_OK;
+  cudaFree(h->state); cudaFree(h->stage); cudaFree(h->eos_d); cudaFree(h->eos_f);
+  cudaFree(h->status); cudaFree(h->iters); cudaFree(h->red); cudaFree(h->part);
+  delete h;
+  return VH_OK;
+}
+
+extern "C" int vh_set_stream(vh_handle* h, void* stream) {
+  if (!h) return VH_E_ARG;
+  h->stream = static_cast<cudaStream_t>(stream);
+  return VH_OK;
+}
+
+extern "C" int vh_dims(const vh_handle* h, int* gx, int* gy, int* gz) {
+  if (!h || !gx || !gy || !gz) return VH_E_ARG;
+  *gx = h->C.gx; *gy = h->C.gy; *gz = h->C.gz;
+  return VH_OK;
+}
+
+static inline unsigned grid1(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// device canonical doubles (18*n) -> state
+static int import_device(vh_handle* h, const double* dev) {
+  const long long n18 = 18 * h->C.n;
+  if (h->mixed) {
+    k_d2f<<<grid1(n18, 256), 256, 0, h->stream>>>(dev, static_cast<float*>(h->state), n18);
+  } else if (dev != h->state) {
+    VH_CUDA(h, cudaMemcpyAsync(h->state, dev, sizeof(double) * n18, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  VH_CUDA(h, cudaGetLastError());
+  return VH_OK;
+}
+static int export_device(vh_handle* h, double* dev) {
+  const long long n18 = 18 * h->C.n;
+  if (h->mixed) k_f2d<<<grid1(n18, 256), 256, 0, h->stream>>>(static_cast<const float*>(h->state), dev, n18);
+  else VH_CUDA(h, cudaMemcpyAsync(dev, h->state, sizeof(double) * n18, cudaMemcpyDeviceToDevice, h->stream));
+  VH_CUDA(h, cudaGetLastError());
+  return VH_OK;
+}
+
+extern "C" int vh_set_state_device(vh_handle* h, const double* dev, double tau) {
+  if (!h || !dev) return VH_E_ARG;
+  int r = import_device(h, dev);
+  if (r) return r;
+  h->tau = tau;
+  h->have_state = true;
+  VH_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(unsigned int), h->stream));
+  return VH_OK;
+}
+extern "C" int vh_get_state_device(vh_handle* h, double* dev) {
+  if (!h || !dev) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  return export_device(h, dev);
+}
+extern "C" int vh_set_state(vh_handle* h, const double* host, double tau) {
+  if (!h || !host) return VH_E_ARG;
+  const long long n18 = 18 * h->C.n;
+  double* dst = h->mixed ? h->stage : static_cast<double*>(h->state);
+  VH_CUDA(h, cudaMemcpyAsync(dst, host, sizeof(double) * n18, cudaMemcpyHostToDevice, h->stream));
+  return vh_set_state_device(h, dst, tau);
+}
+extern "C" int vh_get_state(vh_handle* h, double* host) {
+  if (!h || !host) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  const long long n18 = 18 * h->C.n;
+  if (h->mixed) {
+    int r = export_device(h, h->stage);
+    if (r) return r;
+    VH_CUDA(h, cudaMemcpyAsync(host, h->stage, sizeof(double) * n18, cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    VH_CUDA(h, cudaMemcpyAsync(host, h->state, sizeof(double) * n18, cudaMemcpyDeviceToHost, h->stream));
+  }
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VH_OK;
+}
+
+template <class R>
+static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, double tau, int first) {
+  const DevCfg& C = h->C;
+  const int nzi = C.kr - C.kl;
+  dim3 grid, block;
+  size_t sm;
+  const double hh = dir == 0 ? C.dx : (dir == 1 ? C.dy : C.dz);
+  const R inv_h = (R)(1.0 / hh), hr = (R)hh;
+  if (dir == 0) {
+    using T = Tile<0, R>;
+    block = dim3(T::NA, T::NC);
+    grid = dim3((C.nx + T::NA - 7) / (T::NA - 6), (C.ny + T::NC - 1) / T::NC, nzi);
+    sm = sizeof(DirSmem<R, 0>);
+    k_dir<R, 0><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
+  } else if (dir == 1) {
+    using T = Tile<1, R>;
+    block = dim3(T::NC, T::NA);
+    grid = dim3((C.nx + T::NC - 1) / T::NC, (C.ny + T::NA - 7) / (T::NA - 6), nzi);
+    sm = sizeof(DirSmem<R, 1>);
+    k_dir<R, 1><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
+  } else {
+    using T = Tile<2, R>;
+    block = dim3(T::NC, T::NA);
+    grid = dim3((C.nx + T::NC - 1) / T::NC, (C.nz + T::NA - 7) / (T::NA - 6), C.ny);
+    sm = sizeof(DirSmem<R, 2>);
+    k_dir<R, 2><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
+  }
+  VH_CUDA(h, cudaGetLastError());
+  return VH_OK;
+}
+
+template <class R>
+static int set_smem_attrs(vh_handle* h) {
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 0>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 1>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 2>)));
+  return VH_OK;
+}
+
+// the flux-divergence part of a stage: every direction into res, du
+template <class R>
+static int stage_rhs(vh_handle* h, const DevPtrs<R>& P, int use_b, double tau) {
+  int r;
+  if ((r = launch_dir<R>(h, P, 0, use_b, tau, 1))) return r;
+  if ((r = launch_dir<R>(h, P, 1, use_b, tau, 0))) return r;
+  if (!h->C.bi && (r = launch_dir<R>(h, P, 2, use_b, tau, 0))) return r;
+  return VH_OK;
+}
+
+template <class R>
+static int step_once(vh_handle* h, const DevPtrs<R>& P) {
+  const DevCfg& C = h->C;
+  const double tau = h->tau, ts = h->cfg.dtau;
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  int r;
+  if ((r = stage_rhs<R>(h, P, 0, tau))) return r;
+  k_update<R, 1><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
+  VH_CUDA(h, cudaGetLastError());
+  if ((r = stage_rhs<R>(h, P, 1, tau + ts))) return r;
+  k_update<R, 2><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
+  VH_CUDA(h, cudaGetLastError());
+  h->tau = tau + ts;
+  return VH_OK;
+}
+
+static int read_status(vh_handle* h) {
+  unsigned int st = 0;
+  VH_CUDA(h, cudaMemcpyAsync(&st, h->status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (st & ST_ROOT) return fail(h, VH_E_ROOTFIND, "root-find failed in at least one cell");
+  if (st & ST_NEGE) return fail(h, VH_E_NEG_ENERGY, "non-positive energy density after the root-find");
+  if (st & ST_CAUSAL) return fail(h, VH_E_CAUSALITY, "superluminal velocity after the root-find");
+  return VH_OK;
+}
+
+extern "C" int vh_step(vh_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "vh_step before vh_set_state / vh_init_profile");
+  VH_CUDA(h, cudaMemsetAsync(h->iters, 0, sizeof(unsigned long long), h->stream));
+  for (int s = 0; s < nsteps; s++) {
+    int r = h->mixed ? step_once<float>(h, h->pf) : step_once<double>(h, h->pd);
+    if (r) return r;
+  }
+  return read_status(h);
+}
+
+// Steps with a CUDA event pair around every launch, accumulating device
+// milliseconds per kernel kind: out[0..2] k_dir x/y/eta, out[3] k_update
+// stage 1, out[4] k_update stage 2 (summed over nsteps steps).
+template <class R>
+static int timed_steps(vh_handle* h, const DevPtrs<R>& P, int nsteps, double* out) {
+  const DevCfg& C = h->C;
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  cudaEvent_t ev[2];
+  VH_CUDA(h, cudaEventCreate(&ev[0]));
+  VH_CUDA(h, cudaEventCreate(&ev[1]));
+  for (int q = 0; q < 5; q++) out[q] = 0;
+  auto timed = [&](int slot, auto&& launch) -> int {
+    VH_CUDA(h, cudaEventRecord(ev[0], h->stream));
+    int r = launch();
+    if (r) return r;
+    VH_CUDA(h, cudaEventRecord(ev[1], h->stream));
+    VH_CUDA(h, cudaEventSynchronize(ev[1]));
+    float ms = 0;
+    VH_CUDA(h, cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    out[slot] += ms;
+    return VH_OK;
+  };
+  int r = VH_OK;
+  for (int s = 0; s < nsteps && !r; s++) {
+    const double tau = h->tau, ts = h->cfg.dtau;
+    for (int stage = 0; stage < 2 && !r; stage++) {
+      const double t = stage ? tau + ts : tau;
+      for (int d = 0; d < (C.bi ? 2 : 3) && !r; d++)
+        r = timed(d, [&]() { return launch_dir<R>(h, P, d, stage, t, d == 0); });
+      if (r) break;
+      r = timed(3 + stage, [&]() -> int {
+        if (stage == 0) k_update<R, 1><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
+        else k_update<R, 2><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
+        VH_CUDA(h, cudaGetLastError());
+        return VH_OK;
+      });
+    }
+    h->tau = tau + ts;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  return r;
+}
+
+extern "C" int vh_time_kernels(vh_handle* h, int nsteps, double* ms_out) {
+  if (!h || !ms_out || nsteps < 0) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  int r = h->mixed ? timed_steps<float>(h, h->pf, nsteps, ms_out) : timed_steps<double>(h, h->pd, nsteps, ms_out);
+  if (r) return r;
+  return read_status(h);
+}
+
+extern "C" int vh_get_time(const vh_handle* h, double* tau) {
+  if (!h || !tau) return VH_E_ARG;
+  *tau = h->tau;
+  return VH_OK;
+}
+
+extern "C" int vh_last_iterations(vh_handle* h, long long* iters) {
+  if (!h || !iters) return VH_E_ARG;
+  unsigned long long v = 0;
+  VH_CUDA(h, cudaMemcpyAsync(&v, h->iters, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  *iters = (long long)v;
+  return VH_OK;
+}
+
+template <class R>
+static int init_tail(vh_handle* h, const DevPtrs<R>& P, int pi_mode, double tau) {
+  const DevCfg& C = h->C;
+  if (pi_mode == VH_PI_NS) {
+    R* du16 = reinterpret_cast<R*>(h->stage);  // 16*n fits in the 18*n staging buffer
+    k_du_full<R><<<grid1(C.n, 128), 128, 0, h->stream>>>(C, P, du16, h->cfg.dtau);
+    k_ns_pi<R><<<grid1(C.n, 128), 128, 0, h->stream>>>(C, P, du16, tau);
+  }
+  k_fill_tmunu<R><<<grid1(C.n, 256), 256, 0, h->stream>>>(C, P, tau);
+  VH_CUDA(h, cudaGetLastError());
+  return VH_OK;
+}
+
+extern "C" int vh_init_profile(vh_handle* h, double tau, const double* e, const double* ux, const double* uy,
+                               const double* ueta, const double* prevu4, int pi_mode, const double* pi5) {
+  if (!h || !e || !ux || !uy) return VH_E_ARG;
+  if (pi_mode != VH_PI_GIVEN && pi_mode != VH_PI_ZERO && pi_mode != VH_PI_NS) return fail(h, VH_E_ARG, "pi_mode");
+  if (pi_mode == VH_PI_GIVEN && !pi5) return fail(h, VH_E_ARG, "pi5 is required with VH_PI_GIVEN");
+  const long long n = h->C.n;
+  const double t2 = h->C.cart ? 1.0 : tau * tau;
+  std::vector<double> f(18 * (size_t)n, 0.0);
+  for (long long c = 0; c < n; c++) {
+    const double ue = ueta ? ueta[c] : 0.0;
+    f[c] = e[c];
+    f[2 * n + c] = ux[c];
+    f[3 * n + c] = uy[c];
+    f[4 * n + c] = ue;
+    f[1 * n + c] = std::sqrt(1 + ux[c] * ux[c] + uy[c] * uy[c] + t2 * ue * ue);
+    for (int l = 0; l < 5; l++) f[(5 + l) * n + c] = (pi_mode == VH_PI_GIVEN) ? pi5[l * n + c] : 0.0;
+    for (int l = 0; l < 4; l++) f[(14 + l) * n + c] = prevu4 ? prevu4[l * n + c] : f[(1 + l) * n + c];
+  }
+  int r = vh_set_state(h, f.data(), tau);
+  if (r) return r;
+  r = h->mixed ? init_tail<float>(h, h->pf, pi_mode, tau) : init_tail<double>(h, h->pd, pi_mode, tau);
+  if (r) return r;
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VH_OK;
+}
+
+extern "C" int vh_max_temperature(vh_handle* h, double* tmax_gev) {
+  if (!h || !tmax_gev) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  VH_CUDA(h, cudaMemsetAsync(h->red, 0, sizeof(unsigned long long), h->stream));
+  if (h->mixed) k_max_temp<float><<<296, 256, 0, h->stream>>>(h->C, h->pf, h->red);
+  else k_max_temp<double><<<296, 256, 0, h->stream>>>(h->C, h->pd, h->red);
+  VH_CUDA(h, cudaGetLastError());
+  unsigned long long bits = 0;
+  VH_CUDA(h, cudaMemcpyAsync(&bits, h->red, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(tmax_gev, &bits, sizeof(double));
+  return VH_OK;
+}
+
+extern "C" int vh_conservation_sums(vh_handle* h, double* out4) {
+  if (!h || !out4) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  const double dv = h->C.dx * h->C.dy * (h->C.bi ? 1.0 : h->C.dz);
+  double* fin = h->part + 8 * h->part_blocks;
+  if (h->mixed) k_conserve_part<float><<<h->part_blocks, 256, 0, h->stream>>>(h->C, h->pf, h->tau, dv, h->part);
+  else k_conserve_part<double><<<h->part_blocks, 256, 0, h->stream>>>(h->C, h->pd, h->tau, dv, h->part);
+  k_conserve_final<<<1, 32, 0, h->stream>>>(h->part, h->part_blocks, fin);
+  VH_CUDA(h, cudaGetLastError());
+  VH_CUDA(h, cudaMemcpyAsync(out4, fin, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VH_OK;
+}
+
+extern "C" int vh_cfl(vh_handle* h, double* max_speed, double* dtau_suggest) {
+  if (!h || !max_speed || !dtau_suggest) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  VH_CUDA(h, cudaMemsetAsync(h->red, 0, sizeof(unsigned long long), h->stream));
+  if (h->mixed) k_cfl<float><<<296, 256, 0, h->stream>>>(h->C, h->pf, h->tau, h->red);
+  else k_cfl<double><<<296, 256, 0, h->stream>>>(h->C, h->pd, h->tau, h->red);
+  VH_CUDA(h, cudaGetLastError());
+  unsigned long long bits = 0;
+  VH_CUDA(h, cudaMemcpyAsync(&bits, h->red, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(max_speed, &bits, sizeof(double));
+  *dtau_suggest = *max_speed > 0 ? h->C.dx / (8.0 * *max_speed) : INFINITY;
+  return VH_OK;
+}
+
+template <class R>
+static int debug_terms(vh_handle* h, const DevPtrs<R>& P, double* res, double* src, double* du) {
+  const DevCfg& C = h->C;
+  const long long n = C.n;
+  int r;
+  if ((r = stage_rhs<R>(h, P, 0, h->tau))) return r;
+  R* du16 = reinterpret_cast<R*>(h->stage);
+  k_du_full<R><<<grid1(n, 128), 128, 0, h->stream>>>(C, P, du16, h->cfg.dtau);
+  // the spatial derivatives along each direction come from k_dir (interior)
+  R* src9 = nullptr;
+  VH_CUDA(h, cudaMallocAsync(&src9, sizeof(R) * 9 * n, h->stream));
+  k_debug_src<R><<<grid1(n, 128), 128, 0, h->stream>>>(C, P, du16, src9, h->tau);
+  VH_CUDA(h, cudaGetLastError());
+  std::vector<R> tmp(16 * (size_t)n);
+  VH_CUDA(h, cudaMemcpyAsync(tmp.data(), P.res[0], sizeof(R) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (long long q = 0; q < 9 * n; q++) res[q] = (double)tmp[q];
+  VH_CUDA(h, cudaMemcpyAsync(tmp.data(), src9, sizeof(R) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (long long q = 0; q < 9 * n; q++) src[q] = (double)tmp[q];
+  VH_CUDA(h, cudaMemcpyAsync(tmp.data(), du16, sizeof(R) * 16 * n, cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (long long q = 0; q < 16 * n; q++) du[q] = (double)tmp[q];
+  VH_CUDA(h, cudaFreeAsync(src9, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VH_OK;
+}
+
+extern "C" int vh_debug_stage_terms(vh_handle* h, double* res, double* src, double* du) {
+  if (!h || !res || !src || !du) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  return h->mixed ? debug_terms<float>(h, h->pf, res, src, du) : debug_terms<double>(h, h->pd, res, src, du);
+}
+
+extern "C" const char* vh_last_error(const vh_handle* h) {
+  return h ? h->err.c_str() : g_create_err.c_str();
+}
+
+int vh_internal_config(const vh_handle* h, vh_config* out, std::vector<double>* eos4) {
+  if (!h || !out) return VH_E_ARG;
+  *out = h->cfg;
+  if (eos4) *eos4 = h->eos_host;
+  return VH_OK;
+}

@@ -1,0 +1,239 @@
+// Initialisation, reduction and diagnostic kernels around the step.
+#pragma once
+
+#include "vh_kernels.cuh"
+
+namespace vh {
+
+// T^{tau mu} = (e+P) u^tau u^mu - P g^{tau mu} + pi^{tau mu} on every cell
+// of set A (NEWEST5/init.h:539-549, NEWEST5/Source.h:618-626).
+template <class R>
+__global__ void k_fill_tmunu(DevCfg C, DevPtrs<R> P, double tau) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C.n) return;
+  const R t2 = C.cart ? (R)1 : (R)(tau * tau);
+  R u[4], p[5];
+  const R e = P.e[c];
+#pragma unroll
+  for (int l = 0; l < 4; l++) u[l] = P.u[l][c];
+#pragma unroll
+  for (int l = 0; l < 5; l++) p[l] = P.A[4 + l][c];
+  const R Pp = eos_P<R>(C, e), ep = e + Pp;
+  PiDep<R> d = pi_dep<R>(u[0], u[1], u[2], u[3], p, t2);
+  P.A[0][c] = -Pp + ep * (u[0] * u[0]) + d.tt;
+  P.A[1][c] = ep * u[0] * u[1] + d.tx;
+  P.A[2][c] = ep * u[0] * u[2] + d.ty;
+  P.A[3][c] = ep * u[0] * u[3] + d.te;
+}
+
+// Velocity gradients with the coverage the reference's CalcDer4Vel has
+// (NEWEST5/Source.h:3-101): d_tau on the interior; d_x for i in [2, gx-3]
+// on interior (j,k); d_y likewise; d_eta for every k on interior (i,j) with
+// the edge stencils clamped; zero elsewhere.  Written to du16 (16 x n).
+template <class R>
+__global__ void k_du_full(DevCfg C, DevPtrs<R> P, R* du16, double ts) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C.n) return;
+  const int i = (int)(c % C.gx), j = (int)((c / C.gx) % C.gy), k = (int)(c / ((long long)C.gx * C.gy));
+  const bool ii = i >= C.il && i < C.ir, jj = j >= C.jl && j < C.jr, kk = k >= C.kl && k < C.kr;
+#pragma unroll 1
+  for (int l = 0; l < 4; l++) {
+    const R* u = P.u[l];
+    R d0 = 0, d1 = 0, d2 = 0, d3 = 0;
+    if (ii && jj && kk) d0 = (u[c] - P.pu[l][c]) / (R)ts;
+    if (jj && kk && i >= 2 && i < C.gx - 2) {
+      const R L = weno_left<R>(u[c - 2], u[c - 1], u[c], u[c + 1], u[c + 2]);
+      const R Rr = weno_right<R>(u[c - 2], u[c - 1], u[c], u[c + 1], u[c + 2]);
+      d1 = (L - Rr) / (R)C.dx;
+    }
+    if (ii && kk && j >= 2 && j < C.gy - 2) {
+      const long long s = C.gx;
+      const R L = weno_left<R>(u[c - 2 * s], u[c - s], u[c], u[c + s], u[c + 2 * s]);
+      const R Rr = weno_right<R>(u[c - 2 * s], u[c - s], u[c], u[c + s], u[c + 2 * s]);
+      d2 = (L - Rr) / (R)C.dy;
+    }
+    if (!C.bi && ii && jj) {
+      const long long s = (long long)C.gx * C.gy;
+      const int Z = C.gz;
+      R qm2, qm1, qc = u[c], qp1, qp2;
+      if (k > 1 && k < Z - 2) { qm1 = u[c - s]; qm2 = u[c - 2 * s]; qp1 = u[c + s]; qp2 = u[c + 2 * s]; }
+      else if (k == 0) { qm2 = qm1 = qc; qp1 = u[c + s]; qp2 = u[c + 2 * s]; }
+      else if (k == 1) { qm2 = qm1 = u[c - s]; qp1 = u[c + s]; qp2 = u[c + 2 * s]; }
+      else if (k == Z - 2) { qm1 = u[c - s]; qm2 = u[c - 2 * s]; qp2 = qp1 = u[c + s]; }
+      else { qm1 = u[c - s]; qm2 = u[c - 2 * s]; qp2 = qp1 = qc; }
+      const R L = weno_left<R>(qm2, qm1, qc, qp1, qp2);
+      const R Rr = weno_right<R>(qm2, qm1, qc, qp1, qp2);
+      d3 = (L - Rr) / (R)C.dz;
+    }
+    du16[(l * 4 + 0) * C.n + c] = d0;
+    du16[(l * 4 + 1) * C.n + c] = d1;
+    du16[(l * 4 + 2) * C.n + c] = d2;
+    du16[(l * 4 + 3) * C.n + c] = d3;
+  }
+}
+
+// Navier-Stokes pi = 2 eta sigma on every cell from du16
+// (NEWEST5/Source.h:535-605, NSInit 607-630).
+template <class R>
+__global__ void k_ns_pi(DevCfg C, DevPtrs<R> P, const R* du16, double tau) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C.n) return;
+  R u[4], du[4][4];
+  const R e = P.e[c];
+#pragma unroll
+  for (int l = 0; l < 4; l++) u[l] = P.u[l][c];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) du[a][b] = du16[(a * 4 + b) * C.n + c];
+  const R Pp = eos_P<R>(C, e);
+  R eta, tp;
+  transport<R>(C, e, Pp, &eta, &tp);
+  R sig[4][4], th, acc[4];
+  is_kinematics<R>(C.cart, (R)tau, u, du, sig, th, acc);
+  P.A[4][c] = (R)2 * eta * sig[1][1];
+  P.A[5][c] = (R)2 * eta * sig[2][2];
+  P.A[6][c] = (R)2 * eta * sig[1][2];
+  P.A[7][c] = (R)2 * eta * sig[1][3];
+  P.A[8][c] = (R)2 * eta * sig[2][3];
+}
+
+// Sources at the current state for the debug dump (interior only).
+template <class R>
+__global__ void k_debug_src(DevCfg C, DevPtrs<R> P, const R* du16, R* src9, double tau) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C.n) return;
+  const int i = (int)(c % C.gx), j = (int)((c / C.gx) % C.gy), k = (int)(c / ((long long)C.gx * C.gy));
+  for (int l = 0; l < 9; l++) src9[l * C.n + c] = 0;
+  if (!(i >= C.il && i < C.ir && j >= C.jl && j < C.jr && k >= C.kl && k < C.kr)) return;
+  R u[4], p[5], du[4][4];
+  const R e = P.e[c];
+#pragma unroll
+  for (int l = 0; l < 4; l++) u[l] = P.u[l][c];
+#pragma unroll
+  for (int l = 0; l < 5; l++) p[l] = P.A[4 + l][c];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) du[a][b] = du16[(a * 4 + b) * C.n + c];
+  const R ts = (R)tau;
+  if (!C.cart) {
+    const R t2 = ts * ts, Pp = eos_P<R>(C, e), ep = e + Pp;
+    PiDep<R> d = pi_dep<R>(u[0], u[1], u[2], u[3], p, t2);
+    src9[0 * C.n + c] = -Pp - t2 * (d.ee + ep * u[3] * u[3]);
+    src9[3 * C.n + c] = -(R)2 * (d.te + ep * u[0] * u[3]);
+  }
+  R s5[5];
+  is_source<R>(C, ts, e, u, p, du, s5);
+  if (C.cart && !C.bi && (k - C.kl) >= C.nz - NG) s5[0] = s5[1] = s5[2] = s5[3] = s5[4] = 0;
+  for (int q = 0; q < 5; q++) src9[(4 + q) * C.n + c] = s5[q];
+}
+
+// ---------------------------------------------------------- reductions
+
+__device__ inline void atomic_max_nonneg(unsigned long long* slot, double v) {
+  // the bit patterns of non-negative doubles order like the values
+  atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+
+// max over the interior of hbarc * T(e) (NEWEST5/utils.h:263-283)
+template <class R>
+__global__ void k_max_temp(DevCfg C, DevPtrs<R> P, unsigned long long* out) {
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  double m = 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long long)gridDim.x * blockDim.x) {
+    const int i = C.il + (int)(t % C.nx), j = C.jl + (int)((t / C.nx) % C.ny);
+    const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
+    const double T = C.hbarc * (double)eos_T<R>(C, P.e[cix(C, i, j, k)]);
+    m = fmax(m, T);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+}
+
+// Neumaier-compensated sums of tau T^{tau mu} dV over the interior of set A.
+// One (sum, compensation) pair per block and component into part[4][2][nb].
+__device__ inline void two_sum_add(double& s, double& c, double v) {
+  const double t = s + v;
+  if (fabs(s) >= fabs(v)) c += (s - t) + v; else c += (v - t) + s;
+  s = t;
+}
+template <class R>
+__global__ void k_conserve_part(DevCfg C, DevPtrs<R> P, double tau, double dv, double* part) {
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  double s[4] = {0, 0, 0, 0}, cc[4] = {0, 0, 0, 0};
+  const double tf = C.cart ? 1.0 : tau;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long long)gridDim.x * blockDim.x) {
+    const int i = C.il + (int)(t % C.nx), j = C.jl + (int)((t / C.nx) % C.ny);
+    const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
+    const long long c = cix(C, i, j, k);
+#pragma unroll
+    for (int l = 0; l < 4; l++) two_sum_add(s[l], cc[l], tf * (double)P.A[l][c] * dv);
+  }
+  __shared__ double sh[2][4][256];
+#pragma unroll
+  for (int l = 0; l < 4; l++) { sh[0][l][threadIdx.x] = s[l]; sh[1][l][threadIdx.x] = cc[l]; }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int l = threadIdx.x;
+    double S = 0, Cc = 0;
+    for (int q = 0; q < (int)blockDim.x; q++) { two_sum_add(S, Cc, sh[0][l][q]); Cc += sh[1][l][q]; }
+    part[(l * 2 + 0) * gridDim.x + blockIdx.x] = S;
+    part[(l * 2 + 1) * gridDim.x + blockIdx.x] = Cc;
+  }
+}
+__global__ void k_conserve_final(const double* part, int nb, double* out4) {
+  const int l = threadIdx.x;
+  if (l >= 4) return;
+  double S = 0, Cc = 0;
+  for (int q = 0; q < nb; q++) { two_sum_add(S, Cc, part[(l * 2) * nb + q]); Cc += part[(l * 2 + 1) * nb + q]; }
+  out4[l] = S + Cc;
+}
+
+// Largest sqrt(ax^2 + ay^2 + az^2) of the face signal speeds right of each
+// interior cell (NEWEST5/hydroKT.h:317-344 CFL).
+template <class R>
+__global__ void k_cfl(DevCfg C, DevPtrs<R> P, double tau, unsigned long long* out) {
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  double m = 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long long)gridDim.x * blockDim.x) {
+    const int i = C.il + (int)(t % C.nx), j = C.jl + (int)((t / C.nx) % C.ny);
+    const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
+    double a2 = 0;
+    for (int d = 0; d < (C.bi ? 2 : 3); d++) {
+      const long long s = d == 0 ? 1 : (d == 1 ? (long long)C.gx : (long long)C.gx * C.gy);
+      const int pos = d == 0 ? i : (d == 1 ? j : k);
+      const int lo = d == 0 ? C.il : (d == 1 ? C.jl : C.kl), hi = d == 0 ? C.ir : (d == 1 ? C.jr : C.kr);
+      R q[6];
+      for (int o = -2; o <= 3; o++) {
+        const int g = pos + o;
+        R v = 0;
+        if (g >= lo && g < hi) {
+          const long long cc = cix(C, i, j, k) + (long long)o * s;
+          const R u0 = P.u[0][cc];
+          v = d == 0 ? P.u[1][cc] / u0 : (d == 1 ? P.u[2][cc] / u0 : (C.cart ? P.u[3][cc] / u0 : (R)tau * P.u[3][cc] / u0));
+        }
+        q[o + 2] = v;
+      }
+      const R sl = weno_left<R>(q[0], q[1], q[2], q[3], q[4]);
+      const R sr = weno_right<R>(q[1], q[2], q[3], q[4], q[5]);
+      const double a = fmax(fabs((double)sl), fabs((double)sr));
+      a2 += a * a;
+    }
+    m = fmax(m, sqrt(a2));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+}
+
+// precision conversion between the canonical double layout and float state
+__global__ void k_d2f(const double* in, float* out, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = (float)in[t];
+}
+__global__ void k_f2d(const float* in, double* out, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = (double)in[t];
+}
+
+}  // namespace vh

@@ -1,0 +1,112 @@
+// Snapshot writer in the reference's binary layout (NEWEST5/write.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vh.h"
+#include "vh_internal.h"
+
+namespace {
+
+// host evaluation of T(e), the same formulas as the device EOS
+struct HostEos {
+  int kind = 0;
+  double a = 1;
+  std::vector<double> e, p, c, t;
+  double T(double x) const {
+    if (kind == VH_EOS_CONFORMAL) return std::pow(x / a, 0.25);
+    const int n = (int)e.size();
+    if (x <= e[0]) return t[0] * std::sqrt(std::sqrt(x / e[0]));
+    if (x >= e[n - 1]) return t[n - 1] * std::sqrt(std::sqrt(x / e[n - 1]));
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) { int m = (lo + hi) / 2; if (x >= e[m]) lo = m; else hi = m; }
+    const double w = (x - e[lo]) / (e[lo + 1] - e[lo]);
+    return t[lo] + w * (t[lo + 1] - t[lo]);
+  }
+  double P(double x) const {
+    if (kind == VH_EOS_CONFORMAL) return x / 3.0;
+    const int n = (int)e.size();
+    if (x <= e[0]) return c[0] * x;
+    if (x >= e[n - 1]) return p[n - 1] + c[n - 1] * (x - e[n - 1]);
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) { int m = (lo + hi) / 2; if (x >= e[m]) lo = m; else hi = m; }
+    const double w = (x - e[lo]) / (e[lo + 1] - e[lo]);
+    return p[lo] + w * (p[lo + 1] - p[lo]);
+  }
+};
+
+}  // namespace
+
+extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
+  if (!h || !path || every < 1 || (layout != VH_WRITE_XY && layout != VH_WRITE_FULL)) return VH_E_ARG;
+  vh_config cfg;
+  std::vector<double> tab;
+  int r = vh_internal_config(h, &cfg, &tab);
+  if (r) return r;
+  int gx, gy, gz;
+  vh_dims(h, &gx, &gy, &gz);
+  const long long n = (long long)gx * gy * gz;
+  std::vector<double> f(18 * (size_t)n);
+  if ((r = vh_get_state(h, f.data()))) return r;
+  HostEos eos;
+  eos.kind = cfg.eos_kind;
+  eos.a = cfg.eos_a;
+  if (eos.kind == VH_EOS_TABLE) {
+    const size_t m = tab.size() / 4;
+    eos.e.assign(tab.begin(), tab.begin() + m);
+    eos.p.assign(tab.begin() + m, tab.begin() + 2 * m);
+    eos.c.assign(tab.begin() + 2 * m, tab.begin() + 3 * m);
+    eos.t.assign(tab.begin() + 3 * m, tab.end());
+  }
+  const int nx = cfg.nx, ny = cfg.ny, bi = cfg.boost_invariant;
+  const int nzi = bi ? 1 : cfg.nz, kl = bi ? 0 : 3;
+  auto rec = [&](int i, int j, int k, double* o) {
+    const long long c = ((long long)k * gy + j) * gx + i;
+    const double e = f[c], u0 = f[n + c];
+    o[0] = e;
+    o[1] = eos.T(e);
+    o[2] = eos.P(e);
+    o[3] = f[2 * n + c] / u0;
+    o[4] = f[3 * n + c] / u0;
+    o[5] = f[4 * n + c] / u0;
+    for (int l = 0; l < 5; l++) o[6 + l] = f[(5 + l) * n + c];
+    o[11] = 0.0;  // bulk pressure is not evolved
+  };
+  const size_t R = 12 * sizeof(double);
+  std::vector<unsigned char> file;
+  auto put = [&](size_t off, const double* src, size_t ndouble) {
+    const size_t bytes = ndouble * sizeof(double);
+    if (file.size() < off + bytes) file.resize(off + bytes, 0);
+    std::memcpy(file.data() + off, src, bytes);
+  };
+  if (layout == VH_WRITE_XY) {
+    // NEWEST5/write.h:51-115: per x row a chunk of (12*ny)/FREQ doubles at
+    // offset (gi/FREQ * (ny/FREQ)) records, central eta slice k0
+    const int k0 = bi ? 0 : (gz - 1) / 2;
+    const int ypts = ny / every;
+    const size_t chunk = (size_t)(12 * ny) / every;
+    std::vector<double> buf(12 * (size_t)(ny / every + 2), 0.0);
+    for (int i = 3; i < 3 + nx; i += every) {
+      const int gi = i - 3;
+      for (int j = 3, jj = 0; j < 3 + ny; j += every, jj++) rec(i, j, k0, &buf[12 * (size_t)jj]);
+      put((size_t)(gi / every) * ypts * R, buf.data(), chunk);
+    }
+  } else {
+    // NEWEST5/write.h:204-290: per (x,y) column the eta records, at offset
+    // (gi/FREQ * ypts * zpts + gj/FREQ * zpts) records
+    const int ypts = ny / every, zpts = nzi;
+    std::vector<double> buf(12 * (size_t)nzi);
+    for (int i = 3; i < 3 + nx; i += every)
+      for (int j = 3; j < 3 + ny; j += every) {
+        for (int k = kl, kk = 0; k < kl + nzi; k++, kk++) rec(i, j, k, &buf[12 * (size_t)kk]);
+        put(((size_t)((i - 3) / every) * ypts * zpts + (size_t)((j - 3) / every) * zpts) * R, buf.data(), buf.size());
+      }
+  }
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return VH_E_ARG;
+  const size_t w = std::fwrite(file.data(), 1, file.size(), fp);
+  std::fclose(fp);
+  return w == file.size() ? VH_OK : VH_E_ARG;
+}

@@ -1,0 +1,377 @@
+// Kernels of one RK stage of the viscous KT step and its helpers.
+//
+// A stage is D+1 launches (D = 2 or 3 directions):
+//   k_dir<DIR>  one per direction: stages a tile of cells plus 3 halo cells
+//               along DIR in shared memory as (F^DIR, tau T^{tau mu}, pi,
+//               speed), forms WENO5 (or minmod) face states and the KT flux
+//               at every face of the tile, adds the flux difference to the
+//               divergence accumulator, and writes the WENO velocity
+//               derivative along DIR (NEWEST5/hydroKT.h:16-491,
+//               NEWEST5/Source.h:3-101).
+//   k_update    one thread per interior cell: sources, RK2 combination,
+//               FP64 root-find, and the ghost copy of boundary cells
+//               (NEWEST5/Source.h:165-433, time.h:1-387, multiroot.h:331-493,
+//               boundary.h:1-276).
+#pragma once
+
+#include "vh_device.cuh"
+
+namespace vh {
+
+// Tile shapes: NA cells along the direction (6 of them halo), NC cells
+// across it.  Along x the warp runs along the direction; along y and eta
+// it runs across (x), so global loads stay coalesced.
+template <int DIR, class R>
+struct Tile;
+template <class R>
+struct Tile<0, R> { static constexpr int NA = 32, NC = 4; };
+template <class R>
+struct Tile<1, R> { static constexpr int NA = 22, NC = 8; };
+template <class R>
+struct Tile<2, R> { static constexpr int NA = 22, NC = 8; };
+
+template <class R, int DIR>
+struct DirSmem {
+  static constexpr int NA = Tile<DIR, R>::NA, NC = Tile<DIR, R>::NC;
+  static constexpr int TL = NA - 6;
+  static constexpr int NCELL = NA * NC;
+  static constexpr int NFACE = (TL + 1) * NC;
+  R q[19][NCELL];  // 0..8 F^DIR, 9..17 Var, 18 signal speed
+  R u[4][NCELL];   // u^mu for the velocity derivative
+  R h[9][NFACE];   // KT face fluxes
+};
+
+// Centre flux along DIR, Var and signal speed of one cell
+// (NEWEST5/hydroKT.h:16-83, 161-245, 349-367).
+template <class R, int DIR>
+__device__ inline void cell_terms(const DevCfg& C, R tau, R e, const R* u, const R* p, const R* T, bool interior,
+                                  R* F, R* V, R& spd) {
+  const bool cart = C.cart;
+  const R t2 = cart ? (R)1 : tau * tau;
+  const R tf = cart ? (R)1 : tau;
+  const R P = eos_P<R>(C, e);
+  const R ep = e + P;
+  const R u0 = u[0], u1 = u[1], u2 = u[2], u3 = u[3];
+  PiDep<R> d = pi_dep<R>(u0, u1, u2, u3, p, t2);
+  if (DIR == 0) {
+    F[0] = tf * (d.tx + u1 * u0 * ep);
+    F[1] = tf * (p[0] + P + u1 * u1 * ep);
+    F[2] = tf * (p[2] + u1 * u2 * ep);
+    F[3] = tf * (p[3] + u1 * u3 * ep);
+#pragma unroll
+    for (int l = 0; l < 5; l++) F[4 + l] = (p[l] * u1) / u0;
+    spd = interior ? u1 / u0 : (R)0;
+  } else if (DIR == 1) {
+    F[0] = tf * (d.ty + u2 * u0 * ep);
+    F[1] = tf * (p[2] + u2 * u1 * ep);
+    F[2] = tf * (p[1] + P + u2 * u2 * ep);
+    F[3] = tf * (p[4] + u2 * u3 * ep);
+#pragma unroll
+    for (int l = 0; l < 5; l++) F[4 + l] = (p[l] * u2) / u0;
+    spd = interior ? u2 / u0 : (R)0;
+  } else {
+    F[0] = tf * (d.te + u3 * u0 * ep);
+    F[1] = tf * (p[3] + u3 * u1 * ep);
+    F[2] = tf * (p[4] + u3 * u2 * ep);
+    F[3] = cart ? (d.ee + P + u3 * u3 * ep) : tf * (d.ee + P / t2 + u3 * u3 * ep);
+    // the eta flux of pi carries a factor tau (NEWEST5/hydroKT.h:76-81)
+#pragma unroll
+    for (int l = 0; l < 5; l++) F[4 + l] = cart ? (p[l] * u3) / u0 : tau * (p[l] * u3) / u0;
+    spd = interior ? (cart ? u3 / u0 : tau * u3 / u0) : (R)0;
+  }
+#pragma unroll
+  for (int l = 0; l < 4; l++) V[l] = cart ? T[l] : tf * T[l];
+#pragma unroll
+  for (int l = 0; l < 5; l++) V[4 + l] = p[l];
+}
+
+template <class R>
+__device__ inline R face_left(const DevCfg& C, const R* q, int s_m3, int s_m2, int s_m1, int s_0, int s_p1) {
+  // left state at the face between cells -1 and 0 (stencil centred on -1)
+  if (C.recon == 0) return weno_left<R>(q[s_m3], q[s_m2], q[s_m1], q[s_0], q[s_p1]);
+  return mm_left<R>((R)C.mm_theta, q[s_m2], q[s_m1], q[s_0]);
+}
+template <class R>
+__device__ inline R face_right(const DevCfg& C, const R* q, int s_m2, int s_m1, int s_0, int s_p1, int s_p2) {
+  // right state at the face between cells -1 and 0 (stencil centred on 0)
+  if (C.recon == 0) return weno_right<R>(q[s_m2], q[s_m1], q[s_0], q[s_p1], q[s_p2]);
+  return mm_right<R>((R)C.mm_theta, q[s_m1], q[s_0], q[s_p1]);
+}
+
+template <class R, int DIR>
+__global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
+    k_dir(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, R h, int first) {
+  using S = DirSmem<R, DIR>;
+  constexpr int NA = S::NA, NC = S::NC, TL = S::TL, NT = NA * NC;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& sm = *reinterpret_cast<S*>(smem_raw);
+  if (*P.status) return;
+
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  int lo, hi, galong;
+  if (DIR == 0) { lo = C.il; hi = C.ir; galong = C.gx; }
+  else if (DIR == 1) { lo = C.jl; hi = C.jr; galong = C.gy; }
+  else { lo = C.kl; hi = C.kr; galong = C.gz; }
+  const int a0 = lo - NG + (DIR == 0 ? blockIdx.x : blockIdx.y) * TL;  // global along index of local 0
+  const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)C.gx : (long long)C.gx * C.gy);
+
+  // cross coordinates of local column c
+  auto cross_base = [&](int c, bool& ok) -> long long {
+    int i, j, k;
+    if (DIR == 0) { i = 0; j = C.jl + blockIdx.y * NC + c; k = C.kl + blockIdx.z; ok = j < C.jr; }
+    else if (DIR == 1) { i = C.il + blockIdx.x * NC + c; j = 0; k = C.kl + blockIdx.z; ok = i < C.ir; }
+    else { i = C.il + blockIdx.x * NC + c; j = C.jl + blockIdx.z; k = 0; ok = i < C.ir; }
+    return cix(C, i, j, k);
+  };
+  auto sidx = [](int a, int c) { return DIR == 0 ? c * NA + a : a * NC + c; };
+
+  R* const* set = use_b ? P.B : P.A;
+  // ---- load and per-cell terms
+  {
+    const int ta = DIR == 0 ? threadIdx.x : threadIdx.y;
+    const int tc = DIR == 0 ? threadIdx.y : threadIdx.x;
+    bool ok;
+    const long long cb = cross_base(tc, ok);
+    const int g = a0 + ta;
+    const int s = sidx(ta, tc);
+    R F[9], V[9], spd = 0, uu[4] = {0, 0, 0, 0};
+    if (ok && g >= 0 && g < galong) {
+      const long long c = cb + (long long)g * stride;
+      R p[5], T[4];
+      const R e = P.e[c];
+#pragma unroll
+      for (int l = 0; l < 4; l++) uu[l] = P.u[l][c];
+#pragma unroll
+      for (int l = 0; l < 4; l++) T[l] = set[l][c];
+#pragma unroll
+      for (int l = 0; l < 5; l++) p[l] = set[4 + l][c];
+      cell_terms<R, DIR>(C, tau, e, uu, p, T, g >= lo && g < hi, F, V, spd);
+    } else {
+#pragma unroll
+      for (int l = 0; l < 9; l++) { F[l] = 0; V[l] = 0; }
+    }
+#pragma unroll
+    for (int l = 0; l < 9; l++) { sm.q[l][s] = F[l]; sm.q[9 + l][s] = V[l]; }
+    sm.q[18][s] = spd;
+#pragma unroll
+    for (int l = 0; l < 4; l++) sm.u[l][s] = uu[l];
+  }
+  __syncthreads();
+
+  // ---- KT flux at faces: face f of column c lies between local cells f+2 and f+3
+  for (int idx = tid; idx < S::NFACE; idx += NT) {
+    const int f = idx % (TL + 1), c = idx / (TL + 1);
+    const int a = f + 3;
+    const int g = a0 + a;  // global index of the cell right of the face
+    bool ok;
+    cross_base(c, ok);
+    if (!ok || g > hi) continue;
+    const int sm3 = sidx(a - 3, c), sm2 = sidx(a - 2, c), sm1 = sidx(a - 1, c), s0 = sidx(a, c),
+              sp1 = sidx(a + 1, c), sp2 = sidx(a + 2, c);
+    R amax = 0;
+    // the face left of the first interior cell takes no dissipation: its
+    // max speed sits in a ghost cell the reference never fills
+    // (NEWEST5/hydroKT.h:265-314 vs 435-440)
+    if (g != lo) {
+      R sl = face_left<R>(C, sm.q[18], sm3, sm2, sm1, s0, sp1);
+      R sr = face_right<R>(C, sm.q[18], sm2, sm1, s0, sp1, sp2);
+      amax = fmax(fabs(sl), fabs(sr));
+    }
+#pragma unroll 1
+    for (int l = 0; l < 9; l++) {
+      const R fl = face_left<R>(C, sm.q[l], sm3, sm2, sm1, s0, sp1);
+      const R fr = face_right<R>(C, sm.q[l], sm2, sm1, s0, sp1, sp2);
+      const R vl = face_left<R>(C, sm.q[9 + l], sm3, sm2, sm1, s0, sp1);
+      const R vr = face_right<R>(C, sm.q[9 + l], sm2, sm1, s0, sp1, sp2);
+      sm.h[l][idx] = (R)0.5 * (fl + fr) - (R)0.5 * amax * (vr - vl);
+    }
+  }
+  __syncthreads();
+
+  // ---- flux difference and velocity derivative of interior cells
+  for (int idx = tid; idx < TL * NC; idx += NT) {
+    const int a = idx % TL + 3, c = idx / TL;
+    const int g = a0 + a;
+    bool ok;
+    const long long cb = cross_base(c, ok);
+    if (!ok || g >= hi) continue;
+    const long long cell = cb + (long long)g * stride;
+    const int fr = c * (TL + 1) + (a - 2), fl = c * (TL + 1) + (a - 3);
+#pragma unroll
+    for (int l = 0; l < 9; l++) {
+      const R r = -inv_h * (sm.h[l][fr] - sm.h[l][fl]);
+      P.res[l][cell] = first ? r : P.res[l][cell] + r;
+    }
+    const int sm2 = sidx(a - 2, c), sm1 = sidx(a - 1, c), s0 = sidx(a, c), sp1 = sidx(a + 1, c), sp2 = sidx(a + 2, c);
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const R* q = sm.u[l];
+      const R L = weno_left<R>(q[sm2], q[sm1], q[s0], q[sp1], q[sp2]);
+      const R Rr = weno_right<R>(q[sm2], q[sm1], q[s0], q[sp1], q[sp2]);
+      P.du[l * 3 + DIR][cell] = (L - Rr) / h;
+    }
+  }
+}
+
+// Copy one cell's fields into a ghost cell (NEWEST5/boundary.h).
+template <class R>
+__device__ inline void ghost_put(const DevPtrs<R>& P, R* const* set, long long dst, R e, const R* u, const R* pu,
+                                 const R* q9, bool skip_u12) {
+  P.e[dst] = e;
+  P.u[0][dst] = u[0];
+  if (!skip_u12) { P.u[1][dst] = u[1]; P.u[2][dst] = u[2]; }
+  P.u[3][dst] = u[3];
+#pragma unroll
+  for (int l = 0; l < 4; l++) P.pu[l][dst] = pu[l];
+#pragma unroll
+  for (int l = 0; l < 9; l++) set[l][dst] = q9[l];
+}
+
+// One thread per interior cell: du_tau, sources, the RK combination, the
+// root-find and the ghost copy.  STAGE 1 reads set A and writes set B and
+// v1t; STAGE 2 reads A (its own cell), B and v1t and writes A.
+template <class R, int STAGE>
+__global__ void __launch_bounds__(128) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
+  if (*P.status) return;
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long my_it = 0;
+  if (t < nint) {
+    const int i = C.il + (int)(t % C.nx);
+    const int j = C.jl + (int)((t / C.nx) % C.ny);
+    const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
+    const long long c = cix(C, i, j, k);
+    const double tau1 = tau_n + ts;
+    const R tau_s = (R)(STAGE == 1 ? tau_n : tau1);  // time of the sources
+    const bool cart = C.cart;
+
+    R u[4], pu[4], p[5], e = P.e[c];
+#pragma unroll
+    for (int l = 0; l < 4; l++) { u[l] = P.u[l][c]; pu[l] = P.pu[l][c]; }
+    R* const* cur = STAGE == 1 ? P.A : P.B;
+    R Tc[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) Tc[l] = cur[l][c];
+#pragma unroll
+    for (int l = 0; l < 5; l++) p[l] = cur[4 + l][c];
+
+    // velocity gradients
+    R du[4][4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      du[l][0] = (u[l] - pu[l]) / (R)ts;
+      du[l][1] = P.du[l * 3 + 0][c];
+      du[l][2] = P.du[l * 3 + 1][c];
+      du[l][3] = C.bi ? (R)0 : P.du[l * 3 + 2][c];
+    }
+    // sources (NEWEST5/Source.h:165-191 geometric, 311-433 shear)
+    R src[9];
+    {
+      const R Pp = eos_P<R>(C, e);
+      if (cart) {
+        src[0] = src[1] = src[2] = src[3] = 0;
+      } else {
+        const R t2 = tau_s * tau_s;
+        PiDep<R> d = pi_dep<R>(u[0], u[1], u[2], u[3], p, t2);
+        const R ep = e + Pp;
+        src[0] = -Pp - t2 * (d.ee + ep * u[3] * u[3]);
+        src[1] = 0;
+        src[2] = 0;
+        src[3] = -(R)2 * (d.te + ep * u[0] * u[3]);
+      }
+      R s5[5];
+      is_source<R>(C, tau_s, e, u, p, du, s5);
+      // TXYZ5/Source.h:268-270: the Cartesian 3+1D shear source skips the
+      // last three interior z layers
+      if (cart && !C.bi && (k - C.kl) >= C.nz - NG) s5[0] = s5[1] = s5[2] = s5[3] = s5[4] = 0;
+#pragma unroll
+      for (int q = 0; q < 5; q++) src[4 + q] = s5[q];
+    }
+    // RK combination (NEWEST5/time.h:2-140)
+    R Vn[9];
+    R* const* out = STAGE == 1 ? P.B : P.A;
+    if (STAGE == 1) {
+#pragma unroll
+      for (int l = 0; l < 9; l++) {
+        const R L0 = P.res[l][c] + src[l];
+        const R v0 = l < 4 ? (cart ? Tc[l] : (R)tau_n * Tc[l]) : p[l - 4];
+        Vn[l] = v0 + (R)ts * L0;
+      }
+#pragma unroll
+      for (int l = 0; l < 4; l++) P.v1t[l][c] = Vn[l];
+    } else {
+#pragma unroll
+      for (int l = 0; l < 9; l++) {
+        const R L1 = P.res[l][c] + src[l];
+        const R v0 = l < 4 ? (cart ? P.A[l][c] : (R)tau_n * P.A[l][c]) : P.A[l][c];
+        const R v1 = l < 4 ? P.v1t[l][c] : p[l - 4];
+        Vn[l] = (R)0.5 * v0 + (R)0.5 * v1 + (R)0.5 * (R)ts * L1;
+      }
+    }
+    R q9[9];
+#pragma unroll
+    for (int l = 0; l < 4; l++) q9[l] = cart ? Vn[l] : Vn[l] / (R)tau1;
+#pragma unroll
+    for (int l = 0; l < 5; l++) q9[4 + l] = Vn[4 + l];
+#pragma unroll
+    for (int l = 0; l < 9; l++) out[l][c] = q9[l];
+    // previous velocity (NEWEST5/time.h:166, stage 1 only)
+    if (STAGE == 1) {
+#pragma unroll
+      for (int l = 0; l < 4; l++) { pu[l] = u[l]; P.pu[l][c] = u[l]; }
+    }
+    // root-find (FP64) with the current primitives as the guess
+    double Tt[4], pd[5], x[4] = {(double)e, (double)u[1], (double)u[2], (double)u[3]};
+#pragma unroll
+    for (int l = 0; l < 4; l++) Tt[l] = (double)q9[l];
+#pragma unroll
+    for (int l = 0; l < 5; l++) pd[l] = (double)q9[4 + l];
+    const int it = con2prim(C, Tt, pd, tau1, x);
+    if (it < 0) {
+      atomicOr(P.status, ST_ROOT);
+    } else {
+      my_it = (unsigned long long)it;
+      const double tt = cart ? 1.0 : tau1;
+      const double u0 = sqrt(1 + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] * tt * tt);
+      const double vx = x[1] / u0, vy = x[2] / u0, ve = x[3] / u0;
+      if (sqrt(vx * vx + vy * vy + tt * tt * ve * ve) >= 1) atomicOr(P.status, ST_CAUSAL);
+      if (x[0] <= 0) atomicOr(P.status, ST_NEGE);
+      e = (R)x[0];
+      u[0] = (R)u0; u[1] = (R)x[1]; u[2] = (R)x[2]; u[3] = (R)x[3];
+      P.e[c] = e;
+#pragma unroll
+      for (int l = 0; l < 4; l++) P.u[l][c] = u[l];
+    }
+    // ghost copy of boundary cells: faces only, corners untouched
+    // (NEWEST5/boundary.h:1-276); Gubser test mirrors u^x,u^y
+    const bool mir = C.mirror;
+    if (i == C.il)
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, m, j, k), e, u, pu, q9, mir);
+    if (i == C.ir - 1)
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, C.ir + m, j, k), e, u, pu, q9, mir);
+    if (j == C.jl)
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, m, k), e, u, pu, q9, mir);
+    if (j == C.jr - 1)
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, C.jr + m, k), e, u, pu, q9, mir);
+    if (!C.bi) {
+      if (k == C.kl)
+        for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, j, m), e, u, pu, q9, false);
+      if (k == C.kr - 1)
+        for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, j, C.kr + m), e, u, pu, q9, false);
+    }
+    if (mir) {
+      // ghost m <- cell il + 2 - m on the left, ghost ir + m <- ir - 1 - m on the right
+      const int dl = i - C.il, dr = C.ir - 1 - i;
+      if (dl < NG) { long long g = cix(C, C.il - 1 - dl, j, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
+      if (dr < NG) { long long g = cix(C, C.ir + dr, j, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
+      const int el = j - C.jl, er = C.jr - 1 - j;
+      if (el < NG) { long long g = cix(C, i, C.jl - 1 - el, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
+      if (er < NG) { long long g = cix(C, i, C.jr + er, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
+    }
+  }
+  // one atomic per warp for the iteration counter
+  for (int o = 16; o > 0; o >>= 1) my_it += __shfl_down_sync(0xffffffffu, my_it, o);
+  if ((threadIdx.x & 31) == 0 && my_it) atomicAdd(P.iters, my_it);
+}
+
+}  // namespace vh

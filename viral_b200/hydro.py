@@ -1,0 +1,186 @@
+"""Python handle over the C ABI (include/vh.h), mirroring the reference's
+driver surface: initialise from a profile, evolve per step, read the
+conserved and primitive arrays, maximum temperature, snapshot writers
+(NEWEST5/main.cpp:90-223, init.h:556, time.h:333, utils.h:263, write.h).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi as A
+
+HBARC = 0.19733
+A_QGP = math.pi ** 2 * (16 + 31.5) / 90  # e = a T^4 (fm units)
+
+F_E, F_U, F_PI, F_T, F_PU = 0, 1, 5, 10, 14
+
+
+@dataclass
+class Config:
+    nx: int
+    ny: int
+    nz: int = 1
+    boost_invariant: bool = True
+    coords: int = A.COORD_MILNE
+    precision: int = A.PREC_FP64
+    recon: int = A.RECON_WENO5
+    dx: float = 0.1
+    dy: float = 0.1
+    dz: float = 0.1
+    tau0: float = 0.6
+    dtau: float = 0.02
+    eos_kind: int = A.EOS_CONFORMAL
+    eos_a: float = A_QGP
+    eos_table: np.ndarray | None = None  # (4, n): e, P, cs2, T (fm units)
+    etas0: float = 0.08
+    etas1: float = 0.0
+    etas_tc: float = 0.154
+    hbarc: float = HBARC
+    taupi_kind: int = A.TAUPI_15_ETA_OVER_P
+    gubser_mirror: bool = False
+    minmod_theta: float = 1.1
+    _keep: list = field(default_factory=list, repr=False)
+
+    def gdims(self):
+        return self.nx + 6, self.ny + 6, (1 if self.boost_invariant else self.nz + 6)
+
+    def to_c(self) -> A.VhConfig:
+        c = A.VhConfig()
+        c.coords, c.precision, c.recon = self.coords, self.precision, self.recon
+        c.nx, c.ny, c.nz = self.nx, self.ny, (1 if self.boost_invariant else self.nz)
+        c.boost_invariant = int(self.boost_invariant)
+        c.dx, c.dy, c.dz = self.dx, self.dy, self.dz
+        c.tau0, c.dtau = self.tau0, self.dtau
+        c.eos_kind, c.eos_a = self.eos_kind, self.eos_a
+        if self.eos_kind == A.EOS_TABLE:
+            t = np.ascontiguousarray(self.eos_table, dtype=np.float64)
+            self._keep = [t]
+            c.eos_n = t.shape[1]
+            c.eos_e, c.eos_p, c.eos_cs2, c.eos_t = (A.ptr(t[q]) for q in range(4))
+        c.etas0, c.etas1, c.etas_tc, c.hbarc = self.etas0, self.etas1, self.etas_tc, self.hbarc
+        c.taupi_kind = self.taupi_kind
+        c.gubser_mirror = int(self.gubser_mirror)
+        c.minmod_theta = self.minmod_theta
+        return c
+
+
+class Hydro:
+    """One event on the GPU behind a vh_handle."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self._c = cfg.to_c()
+        h = ctypes.c_void_p()
+        A.check(A.lib().vh_create(ctypes.byref(self._c), ctypes.byref(h)))
+        self.h = h
+        self.gx, self.gy, self.gz = cfg.gdims()
+        self.n = self.gx * self.gy * self.gz
+
+    def close(self):
+        if getattr(self, "h", None):
+            A.lib().vh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, code):
+        A.check(code, self.h)
+
+    # ---- state
+    def set_state(self, f: np.ndarray, tau: float):
+        f = np.ascontiguousarray(f, dtype=np.float64).reshape(A.NFIELDS, self.n)
+        self._chk(A.lib().vh_set_state(self.h, A.ptr(f), tau))
+
+    def get_state(self) -> np.ndarray:
+        f = np.empty((A.NFIELDS, self.n))
+        self._chk(A.lib().vh_get_state(self.h, A.ptr(f)))
+        return f
+
+    def init_profile(self, tau, e, ux, uy, ueta=None, prevu=None, pi_mode=A.PI_ZERO, pi5=None):
+        c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        self._chk(A.lib().vh_init_profile(self.h, tau, A.ptr(c(e)), A.ptr(c(ux)), A.ptr(c(uy)), A.ptr(c(ueta)),
+                                          A.ptr(c(prevu)), pi_mode, A.ptr(c(pi5))))
+
+    # ---- evolution
+    def step(self, nsteps: int = 1):
+        self._chk(A.lib().vh_step(self.h, nsteps))
+
+    @property
+    def tau(self) -> float:
+        t = ctypes.c_double()
+        self._chk(A.lib().vh_get_time(self.h, ctypes.byref(t)))
+        return t.value
+
+    def time_kernels(self, nsteps: int) -> np.ndarray:
+        out = np.zeros(5)
+        self._chk(A.lib().vh_time_kernels(self.h, nsteps, A.ptr(out)))
+        return out
+
+    def last_iterations(self) -> int:
+        v = ctypes.c_longlong()
+        self._chk(A.lib().vh_last_iterations(self.h, ctypes.byref(v)))
+        return v.value
+
+    # ---- diagnostics
+    def max_temperature(self) -> float:
+        t = ctypes.c_double()
+        self._chk(A.lib().vh_max_temperature(self.h, ctypes.byref(t)))
+        return t.value
+
+    def conservation_sums(self) -> np.ndarray:
+        out = np.zeros(4)
+        self._chk(A.lib().vh_conservation_sums(self.h, A.ptr(out)))
+        return out
+
+    def cfl(self):
+        a, d = ctypes.c_double(), ctypes.c_double()
+        self._chk(A.lib().vh_cfl(self.h, ctypes.byref(a), ctypes.byref(d)))
+        return a.value, d.value
+
+    def write(self, path: str, layout: int = A.WRITE_XY, every: int = 1):
+        self._chk(A.lib().vh_write(self.h, path.encode(), layout, every))
+
+    def debug_stage_terms(self):
+        res = np.zeros((9, self.n)); src = np.zeros((9, self.n)); du = np.zeros((16, self.n))
+        self._chk(A.lib().vh_debug_stage_terms(self.h, A.ptr(res), A.ptr(src), A.ptr(du)))
+        return res, src, du
+
+
+# ------------------------------------------------------------ generators
+
+def eos_table_synthetic(n=2000, emin=1e-3, emax=500.0, a=A_QGP, hbarc=HBARC) -> np.ndarray:
+    t = np.zeros((4, n))
+    A.check(A.lib().vh_eos_table_synthetic(n, emin, emax, a, hbarc, A.ptr(t[0]), A.ptr(t[1]), A.ptr(t[2]),
+                                           A.ptr(t[3])))
+    return t
+
+
+def profile_gubser(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, t0_gev=0.6, a=A_QGP, hbarc=HBARC):
+    gx, gy = nx + 6, ny + 6
+    e = np.zeros(gx * gy); ux = np.zeros_like(e); uy = np.zeros_like(e); pu = np.zeros(4 * gx * gy)
+    A.check(A.lib().vh_profile_gubser(nx, ny, dx, dy, q, tau0, dtau, t0_gev, a, hbarc, A.ptr(e), A.ptr(ux),
+                                      A.ptr(uy), A.ptr(pu)))
+    return e, ux, uy, pu
+
+
+def profile_glauber(nx, ny, nz=1, boost_invariant=True, dx=0.1, dy=0.1, dz=0.25, A_nuc=208, R=6.62, aws=0.546,
+                    dmin=0.4, b=7.0, sigma_nn=6.4, w=0.5, epeak_gev=40.0, eta_flat=1.5, eta_sigma=1.3,
+                    hbarc=HBARC, seed=0):
+    gz = 1 if boost_invariant else nz + 6
+    e = np.zeros((nx + 6) * (ny + 6) * gz)
+    npart = ctypes.c_int()
+    A.check(A.lib().vh_profile_glauber(nx, ny, nz, int(boost_invariant), dx, dy, dz, A_nuc, R, aws, dmin, b,
+                                       sigma_nn, w, epeak_gev, eta_flat, eta_sigma, hbarc, seed, A.ptr(e),
+                                       ctypes.byref(npart)))
+    return e, npart.value
