@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libvh.so")
 
 NFIELDS = 18
 NGHOST = 3
+STATIC_MAX_CELLS = 61680  # VH_STATIC_MAX_CELLS
 
 # vh_status
 OK, E_ARG, E_CUDA, E_ROOTFIND, E_CAUSALITY, E_NEG_ENERGY, E_TIMEOUT, E_STATE, E_NOMEM, E_UNSUPPORTED = range(10)
@@ -67,6 +68,8 @@ SIGNATURES = [
     ("vh_time_kernels", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     ("vh_last_iterations", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("vh_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("vh_step_static", ctypes.c_int, [ctypes.POINTER(VhConfig), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                      ctypes.c_int, ctypes.c_void_p]),
     ("vh_eos_table_synthetic", ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                               ctypes.c_double, _dp, _dp, _dp, _dp]),
     ("vh_profile_gubser", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
