@@ -167,10 +167,11 @@ def build_workload(name: str, precision: str):
     from viral_b200 import _abi as A
     from viral_b200 import configs as C
     prec = A.PREC_MIXED if precision == "mixed" else A.PREC_FP64
-    if name == "glauber_161x161x41":
-        cfg = C.glauber_config(precision=prec)
+    if name.startswith("glauber_"):
+        nx, ny, nz = (int(v) for v in name.split("_", 1)[1].split("x"))
+        cfg = C.glauber_config(nx=nx, ny=ny, nz=nz, boost_invariant=nz == 1, precision=prec)
         inp = C.glauber_inputs(cfg, b=7.0, seed=0)
-        desc = {"workload": "glauber_161x161x41", "grid": [161, 161, 41], "coords": "milne", "dx_fm": 0.1,
+        desc = {"workload": name, "grid": [nx, ny, nz], "coords": "milne", "dx_fm": 0.1,
                 "deta": 0.25, "dtau_fm": 0.02, "tau0_fm": 0.6, "eos": "synthetic table (2000 rows)",
                 "eta_over_s": 0.08, "ic": "MC-Glauber Pb+Pb b=7 fm seed 0, 208 nucleons, sigma_nn=6.4 fm^2",
                 "recon": "WENO5", "precision": precision}
@@ -256,6 +257,10 @@ def run_ours(args, rank, world, dist):
 
     # end to end through the C ABI with pinned host buffers
     n18 = 18 * H.n
+    if args.e2e_steps <= 0:
+        H.close()
+        return None if rank else {"metric": METRIC, "value": value, "ms_per_step": ms / args.steps,
+                                  "config": desc, "kernel_ms": dict(zip(names, kt.tolist()))}
     host = torch.empty(n18, dtype=torch.float64, pin_memory=True).numpy()
     H_state = H.get_state()
     host[:] = H_state.reshape(-1)
@@ -337,7 +342,7 @@ def main():
         dist = tdist
     out = run_ours(args, rank, world, dist)
     if rank == 0:
-        if world == 1:
+        if world == 1 and args.cpu_seconds > 0 and "e2e" in out:
             procs = reference_procs()
             rate, cores = cpu_reference(args.cpu_seconds, procs)
             out["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference",

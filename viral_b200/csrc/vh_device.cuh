@@ -155,13 +155,14 @@ struct PiDep {
 template <class R>
 __device__ inline PiDep<R> pi_dep(R u0, R u1, R u2, R u3, const R* p, R t2) {
   PiDep<R> d;
-  R D = u0 * u0 - t2 * u3 * u3;
-  R Q = u1 * u1 * p[0] + (R)2 * u1 * u2 * p[2] + u2 * u2 * p[1] + (R)2 * t2 * u3 * (u1 * p[3] + u2 * p[4]);
-  d.tt = (Q - t2 * u3 * u3 * (p[0] + p[1])) / D;
-  d.ee = (Q - u0 * u0 * (p[0] + p[1])) / (t2 * D);
-  d.tx = (p[0] * u1 + p[2] * u2 + p[3] * u3 * t2) / u0;
-  d.ty = (p[2] * u1 + p[1] * u2 + p[4] * u3 * t2) / u0;
-  d.te = (u1 * p[3] + u2 * p[4] + t2 * u3 * d.ee) / u0;
+  const R iD = (R)1 / (u0 * u0 - t2 * u3 * u3);
+  const R iu0 = (R)1 / u0;
+  const R Q = u1 * u1 * p[0] + (R)2 * u1 * u2 * p[2] + u2 * u2 * p[1] + (R)2 * t2 * u3 * (u1 * p[3] + u2 * p[4]);
+  d.tt = (Q - t2 * u3 * u3 * (p[0] + p[1])) * iD;
+  d.ee = (Q - u0 * u0 * (p[0] + p[1])) * iD / t2;
+  d.tx = (p[0] * u1 + p[2] * u2 + p[3] * u3 * t2) * iu0;
+  d.ty = (p[2] * u1 + p[1] * u2 + p[4] * u3 * t2) * iu0;
+  d.te = (u1 * p[3] + u2 * p[4] + t2 * u3 * d.ee) * iu0;
   return d;
 }
 
@@ -178,33 +179,39 @@ __device__ inline void weno_beta(R qm2, R qm1, R qc, R qp1, R qp2, R& b0, R& b1,
   a = qm2 - (R)2 * qm1 + qc; c = qm2 - (R)4 * qm1 + (R)3 * qc;
   b2 = c13 * (a * a) + (R)0.25 * (c * c);
 }
+// The nonlinear weights w_k = a_k / sum(a), a_k = d_k / (eps + b_k)^2, are
+// formed with a single division: multiplying every a_k by the product of
+// the three (eps + b)^2 gives n_k = d_k prod_{j != k} (eps + b_j)^2, so the
+// face value is sum(n_k q_k) / sum(n_k).  The 1/6 of the candidate
+// polynomials is folded into the same division.  This is the reference's
+// WENO5 (NEWEST5/utils.h:102-160) up to rounding.
 // value at face i+1/2 from the stencil centred on i (genWENOL)
 template <class R>
 __device__ inline R weno_left(R qm2, R qm1, R qc, R qp1, R qp2) {
   R b0, b1, b2;
   weno_beta<R>(qm2, qm1, qc, qp1, qp2, b0, b1, b2);
-  R q0 = ((R)2 * qc + (R)5 * qp1 - qp2) / (R)6;
-  R q1 = (-qm1 + (R)5 * qc + (R)2 * qp1) / (R)6;
-  R q2 = ((R)2 * qm2 - (R)7 * qm1 + (R)11 * qc) / (R)6;
   const R eps = (R)1e-6;
-  R e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
-  R a0 = (R)0.3 / (e0 * e0), a1 = (R)0.6 / (e1 * e1), a2 = (R)0.1 / (e2 * e2);
-  R s = a0 + a1 + a2;
-  return (a0 / s) * q0 + (a1 / s) * q1 + (a2 / s) * q2;
+  const R e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+  const R E0 = e0 * e0, E1 = e1 * e1, E2 = e2 * e2;
+  const R n0 = (R)0.3 * (E1 * E2), n1 = (R)0.6 * (E0 * E2), n2 = (R)0.1 * (E0 * E1);
+  const R q0 = (R)2 * qc + (R)5 * qp1 - qp2;
+  const R q1 = -qm1 + (R)5 * qc + (R)2 * qp1;
+  const R q2 = (R)2 * qm2 - (R)7 * qm1 + (R)11 * qc;
+  return (n0 * q0 + n1 * q1 + n2 * q2) / ((R)6 * (n0 + n1 + n2));
 }
 // value at face i-1/2 from the stencil centred on i (genWENOR)
 template <class R>
 __device__ inline R weno_right(R qm2, R qm1, R qc, R qp1, R qp2) {
   R b0, b1, b2;
   weno_beta<R>(qm2, qm1, qc, qp1, qp2, b0, b1, b2);
-  R q0 = ((R)11 * qc - (R)7 * qp1 + (R)2 * qp2) / (R)6;
-  R q1 = ((R)2 * qm1 + (R)5 * qc - qp1) / (R)6;
-  R q2 = (-qm2 + (R)5 * qm1 + (R)2 * qc) / (R)6;
   const R eps = (R)1e-6;
-  R e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
-  R a0 = (R)0.1 / (e0 * e0), a1 = (R)0.6 / (e1 * e1), a2 = (R)0.3 / (e2 * e2);
-  R s = a0 + a1 + a2;
-  return (a0 / s) * q0 + (a1 / s) * q1 + (a2 / s) * q2;
+  const R e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+  const R E0 = e0 * e0, E1 = e1 * e1, E2 = e2 * e2;
+  const R n0 = (R)0.1 * (E1 * E2), n1 = (R)0.6 * (E0 * E2), n2 = (R)0.3 * (E0 * E1);
+  const R q0 = (R)11 * qc - (R)7 * qp1 + (R)2 * qp2;
+  const R q1 = (R)2 * qm1 + (R)5 * qc - qp1;
+  const R q2 = -qm2 + (R)5 * qm1 + (R)2 * qc;
+  return (n0 * q0 + n1 * q1 + n2 * q2) / ((R)6 * (n0 + n1 + n2));
 }
 // generalized minmod (theta) piecewise-linear face values (utils.h:33-55)
 template <class R>
@@ -245,9 +252,10 @@ __device__ inline void is_kinematics(int cart, R tau, const R* u, const R du[4][
 #pragma unroll
     for (int a = 0; a < 4; a++) Dm[l][a] = du[l][a];
   if (!cart) {
+    const R itau = (R)1 / tau;
     Dm[0][3] += tau * u[3];
-    Dm[3][0] += u[3] / tau;
-    Dm[3][3] += u[0] / tau;
+    Dm[3][0] += u[3] * itau;
+    Dm[3][3] += u[0] * itau;
   }
   R Dl[4][4];
 #pragma unroll
@@ -265,6 +273,7 @@ __device__ inline void is_kinematics(int cart, R tau, const R* u, const R du[4][
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 4; b++) tr += Dt[a][b] * Dl[a][b];
+  const R tr3 = tr * ((R)1 / (R)3);
   R S[4][4], M[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++)
@@ -286,7 +295,7 @@ __device__ inline void is_kinematics(int cart, R tau, const R* u, const R du[4][
       R s = 0;
 #pragma unroll
       for (int b = 0; b < 4; b++) s += M[m][b] * Dt[v][b];
-      sig[m][v] = s - Dt[m][v] * tr / (R)3;
+      sig[m][v] = s - Dt[m][v] * tr3;
     }
 #pragma unroll
   for (int v = 0; v < 4; v++) {
@@ -310,24 +319,25 @@ __device__ inline void is_source(const DevCfg& C, R tau, R e, const R* u, const 
   R pa[4];
 #pragma unroll
   for (int v = 0; v < 4; v++) pa[v] = pi[v][0] * acc[0] + pi[v][1] * acc[1] + pi[v][2] * acc[2] + pi[v][3] * acc[3];
+  const R iu0 = (R)1 / u[0], itp = (R)1 / tp, itau = cart ? (R)1 : (R)1 / tau;
   R divv = 0;
 #pragma unroll
-  for (int i = 1; i < 4; i++) divv += du[i][i] / u[0] - u[i] * du[0][i] / (u[0] * u[0]);
+  for (int i = 1; i < 4; i++) divv += du[i][i] * iu0 - u[i] * du[0][i] * (iu0 * iu0);
   const int MU[5] = {1, 2, 1, 1, 2}, NU[5] = {1, 2, 2, 3, 3};
 #pragma unroll
   for (int q = 0; q < 5; q++) {
     const int m = MU[q], v = NU[q];
-    R rhs = -(pi[m][v] - (R)2 * eta * sig[m][v]) / tp - ((R)4 / (R)3) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
+    R rhs = -(pi[m][v] - (R)2 * eta * sig[m][v]) * itp - ((R)4 / (R)3) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
     R chr = 0;
     if (!cart) {
 #pragma unroll
       for (int w = 0; w < 2; w++) {
         const int Aa = w ? v : m, Bb = w ? m : v;
         if (Aa == 0) chr += u[3] * tau * pi[3][Bb];
-        if (Aa == 3) chr += (u[0] * pi[3][Bb] + u[3] * pi[0][Bb]) / tau;
+        if (Aa == 3) chr += (u[0] * pi[3][Bb] + u[3] * pi[0][Bb]) * itau;
       }
     }
-    out[q] = (rhs - chr) / u[0] + pi[m][v] * divv;
+    out[q] = (rhs - chr) * iu0 + pi[m][v] * divv;
   }
 }
 
@@ -390,11 +400,13 @@ __device__ inline bool solve4(double A[4][4], double b[4]) {
         double t = b[c]; b[c] = b[r]; b[r] = t;
       }
     }
+    const double ip = 1.0 / A[c][c];
+    A[c][c] = ip;  // keep the reciprocal pivot for the back substitution
 #pragma unroll
     for (int r = c + 1; r < 4; r++) {
-      double m = A[r][c] / A[c][c];
+      const double m = A[r][c] * ip;
 #pragma unroll
-      for (int k = c; k < 4; k++) A[r][k] -= m * A[c][k];
+      for (int k = c + 1; k < 4; k++) A[r][k] -= m * A[c][k];
       b[r] -= m * b[c];
     }
   }
@@ -403,7 +415,7 @@ __device__ inline bool solve4(double A[4][4], double b[4]) {
     double s = b[c];
 #pragma unroll
     for (int k = c + 1; k < 4; k++) s -= A[c][k] * b[k];
-    b[c] = s / A[c][c];
+    b[c] = s * A[c][c];
   }
   return true;
 }

@@ -53,22 +53,23 @@ __device__ inline void cell_terms(const DevCfg& C, R tau, R e, const R* u, const
   const R ep = e + P;
   const R u0 = u[0], u1 = u[1], u2 = u[2], u3 = u[3];
   PiDep<R> d = pi_dep<R>(u0, u1, u2, u3, p, t2);
+  const R iu0 = (R)1 / u0;
   if (DIR == 0) {
     F[0] = tf * (d.tx + u1 * u0 * ep);
     F[1] = tf * (p[0] + P + u1 * u1 * ep);
     F[2] = tf * (p[2] + u1 * u2 * ep);
     F[3] = tf * (p[3] + u1 * u3 * ep);
 #pragma unroll
-    for (int l = 0; l < 5; l++) F[4 + l] = (p[l] * u1) / u0;
-    spd = interior ? u1 / u0 : (R)0;
+    for (int l = 0; l < 5; l++) F[4 + l] = (p[l] * u1) * iu0;
+    spd = interior ? u1 * iu0 : (R)0;
   } else if (DIR == 1) {
     F[0] = tf * (d.ty + u2 * u0 * ep);
     F[1] = tf * (p[2] + u2 * u1 * ep);
     F[2] = tf * (p[1] + P + u2 * u2 * ep);
     F[3] = tf * (p[4] + u2 * u3 * ep);
 #pragma unroll
-    for (int l = 0; l < 5; l++) F[4 + l] = (p[l] * u2) / u0;
-    spd = interior ? u2 / u0 : (R)0;
+    for (int l = 0; l < 5; l++) F[4 + l] = (p[l] * u2) * iu0;
+    spd = interior ? u2 * iu0 : (R)0;
   } else {
     F[0] = tf * (d.te + u3 * u0 * ep);
     F[1] = tf * (p[3] + u3 * u1 * ep);
@@ -76,8 +77,8 @@ __device__ inline void cell_terms(const DevCfg& C, R tau, R e, const R* u, const
     F[3] = cart ? (d.ee + P + u3 * u3 * ep) : tf * (d.ee + P / t2 + u3 * u3 * ep);
     // the eta flux of pi carries a factor tau (NEWEST5/hydroKT.h:76-81)
 #pragma unroll
-    for (int l = 0; l < 5; l++) F[4 + l] = cart ? (p[l] * u3) / u0 : tau * (p[l] * u3) / u0;
-    spd = interior ? (cart ? u3 / u0 : tau * u3 / u0) : (R)0;
+    for (int l = 0; l < 5; l++) F[4 + l] = cart ? (p[l] * u3) * iu0 : tau * (p[l] * u3) * iu0;
+    spd = interior ? (cart ? u3 * iu0 : tau * u3 * iu0) : (R)0;
   }
 #pragma unroll
   for (int l = 0; l < 4; l++) V[l] = cart ? T[l] : tf * T[l];
