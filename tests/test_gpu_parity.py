@@ -93,7 +93,7 @@ def test_gubser_run_matches_oracle():
     inp = C.gubser_inputs(cfg)
     O = oracle_from_inputs(cfg, inp)
     with C.make_hydro(cfg, inp) as H:
-        compare_states(H.get_state(), O.get_state(), 1e-13, fields=range(18))
+        compare_states(H.get_state(), O.get_state(), STAGE_TOL, fields=range(18))
         tau = cfg.tau0
         for _ in range(50):
             assert O.step(tau, cfg.dtau) == 0
