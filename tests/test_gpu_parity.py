@@ -28,11 +28,22 @@ def milne3d(**kw):
     return Config(**base)
 
 
+# field groups normalised together: e; u^mu; pi^{mu nu}; T^{tau mu}; prevu
+GROUPS = [(0,), (1, 2, 3, 4), (5, 6, 7, 8, 9), (10, 11, 12, 13), (14, 15, 16, 17)]
+
+
 def compare_states(a, b, tol, fields=range(14), mask=None):
+    """Max |a-b| of each field over the largest |b| of its tensor group
+    (a component that stays near zero is judged on the scale of its tensor)."""
     errs = {}
-    for q in fields:
-        x, y = (a[q], b[q]) if mask is None else (a[q][mask], b[q][mask])
-        errs[q] = rel_err(x, y)
+    for grp in GROUPS:
+        scale = max(float(np.max(np.abs(b[q] if mask is None else b[q][mask]))) for q in grp)
+        for q in grp:
+            if q not in fields:
+                continue
+            x, y = (a[q], b[q]) if mask is None else (a[q][mask], b[q][mask])
+            d = float(np.max(np.abs(x - y)))
+            errs[q] = 0.0 if d == 0 else d / (scale if scale > 0 else 1.0)
     worst = max(errs.values())
     assert worst <= tol, f"max rel err {worst:.3e} > {tol:.1e}: {errs}"
     return worst
