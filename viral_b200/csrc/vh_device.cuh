@@ -70,7 +70,9 @@ __device__ inline float d_sqrt(float x) { return sqrtf(x); }
 template <class R>
 __device__ inline int eos_row(const DevCfg& C, const R* t, R e) {
   const int n = C.eos_n;
-  int i = (int)((d_log(e) - (R)C.eos_l0) * (R)C.eos_idl);
+  // a single-precision log is enough for the guess: the loops below make
+  // the bracket exact
+  int i = (int)((__logf((float)e) - (float)C.eos_l0) * (float)C.eos_idl);
   i = i < 0 ? 0 : (i > n - 2 ? n - 2 : i);
   while (i > 0 && e < t[i]) i--;
   while (i < n - 2 && e >= t[i + 1]) i++;
@@ -279,8 +281,10 @@ __device__ inline void is_kinematics(int cart, R tau, const R* u, const R du[4][
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 4; b++) S[a][b] = (R)0.5 * (Dl[a][b] + Dl[b][a]);
+  // only sigma^{xx}, sigma^{yy}, sigma^{xy}, sigma^{x eta}, sigma^{y eta}
+  // (rows x, y and columns x, y, eta) are used
 #pragma unroll
-  for (int m = 0; m < 4; m++)
+  for (int m = 1; m < 3; m++)
 #pragma unroll
     for (int b = 0; b < 4; b++) {
       R s = 0;
@@ -289,9 +293,9 @@ __device__ inline void is_kinematics(int cart, R tau, const R* u, const R du[4][
       M[m][b] = s;
     }
 #pragma unroll
-  for (int m = 0; m < 4; m++)
+  for (int m = 1; m < 3; m++)
 #pragma unroll
-    for (int v = 0; v < 4; v++) {
+    for (int v = 1; v < 4; v++) {
       R s = 0;
 #pragma unroll
       for (int b = 0; b < 4; b++) s += M[m][b] * Dt[v][b];
@@ -341,6 +345,14 @@ __device__ inline void is_source(const DevCfg& C, R tau, R e, const R* u, const 
   }
 }
 
+// P and dP/de together (one table lookup)
+template <class R>
+__device__ inline void eos_P_cs2(const DevCfg& C, R e, R& P, R& cs2) {
+  if (C.eos_kind == 0) { P = e / (R)3; cs2 = (R)1 / (R)3; return; }
+  R T;
+  eos_table<R>(C, e, &P, &cs2, &T);
+}
+
 // -------------------------------------------------------------- con2prim
 // Residuals of T^{tau nu} u_nu = e u^tau for x = (e, u^x, u^y, u^eta) and
 // their Jacobian (NEWEST5/multiroot.h:202-319), in double.
@@ -349,7 +361,8 @@ __device__ inline void c2p_fj(const DevCfg& C, const double* Tt, const double* p
   double e = x[0];
   const double u1 = x[1], u2 = x[2], u3 = x[3];
   if (e <= 0) e = 1e-6;  // NEWEST5/multiroot.h:225-226
-  const double P = eos_P<double>(C, e);
+  double P, a;
+  eos_P_cs2<double>(C, e, P, a);
   const double W = Tt[0], X = Tt[1], Y = Tt[2], Z = Tt[3];
   const double p1 = p[0], p2 = p[1], p3 = p[2], p4 = p[3], p5 = p[4];
   const double S = 1 + u1 * u1 + u2 * u2 + t2 * u3 * u3;
@@ -360,7 +373,6 @@ __device__ inline void c2p_fj(const DevCfg& C, const double* Tt, const double* p
   y[2] = Y * u0 - e * u2 - u1 * (p3 + ep * u1 * u2) - u2 * (P + p2 + ep * u2 * u2) - t2 * u3 * (p5 + ep * u2 * u3);
   y[3] = Z * u0 - p4 * u1 - p5 * u2 - u3 * (P + W - p1 - p2);
   if (!jac) return;
-  const double a = eos_cs2<double>(C, e);
   const double iu = 1.0 / u0;
   J[0][0] = -u0;
   J[0][1] = (W - e) * u1 * iu - X;
@@ -425,7 +437,12 @@ __device__ inline bool solve4(double A[4][4], double b[4]) {
 // NEWEST5/multiroot.h:389-422).  A step that raises |f| is shortened by
 // t = (sqrt(1+6r)-1)/(3r), r = |f_new|^2/|f_old|^2, at most 64 times.
 // Returns the iteration count, or -1 on failure.
-__device__ inline int con2prim(const DevCfg& C, const double* Tt, const double* p, double tau, double* x) {
+// rtol = 1e-16 is the reference's rule; the mixed step, which stores the
+// result in single precision, stops at rtol = 1e-10.  The Jacobian is
+// formed together with the residual at every trial point, so an accepted
+// full step (the common case) costs one evaluation.
+__device__ inline int con2prim(const DevCfg& C, const double* Tt, const double* p, double tau, double* x,
+                               double rtol = 1e-16) {
   const double t2 = C.cart ? 1.0 : tau * tau;
   double y[4], J[4][4];
   c2p_fj(C, Tt, p, t2, x, y, J, true);
@@ -435,14 +452,14 @@ __device__ inline int con2prim(const DevCfg& C, const double* Tt, const double* 
     it++;
     double st[4] = {-y[0], -y[1], -y[2], -y[3]};
     if (!solve4(J, st)) return -1;
-    double t = 1.0, xt[4], yt[4], phi1 = 0;
+    double t = 1.0, xt[4], phi1 = 0;
     bool ok = false;
     for (int tries = 0; tries < 64; tries++) {
 #pragma unroll
       for (int i = 0; i < 4; i++) xt[i] = x[i] + t * st[i];
-      c2p_fj(C, Tt, p, t2, xt, yt, J, false);
-      if (!(isfinite(yt[0]) && isfinite(yt[1]) && isfinite(yt[2]) && isfinite(yt[3]))) return -1;
-      phi1 = sqrt(yt[0] * yt[0] + yt[1] * yt[1] + yt[2] * yt[2] + yt[3] * yt[3]);
+      c2p_fj(C, Tt, p, t2, xt, y, J, true);
+      if (!(isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && isfinite(y[3]))) return -1;
+      phi1 = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
       if (phi1 <= phi || phi == 0.0) { ok = true; break; }
       double r = (phi1 * phi1) / (phi * phi);
       t *= (sqrt(1.0 + 6.0 * r) - 1.0) / (3.0 * r);
@@ -453,10 +470,9 @@ __device__ inline int con2prim(const DevCfg& C, const double* Tt, const double* 
     for (int i = 0; i < 4; i++) {
       double dx = xt[i] - x[i];
       x[i] = xt[i];
-      if (!(fabs(dx) < 1e-16 * fabs(x[i]) || dx == 0.0)) conv = false;
+      if (!(fabs(dx) < rtol * fabs(x[i]) || dx == 0.0)) conv = false;
     }
     phi = phi1;
-    c2p_fj(C, Tt, p, t2, x, y, J, true);
     if (conv) break;
   }
   // an iterate that is not a root is a failure (the reference keeps it

@@ -161,7 +161,10 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
 
   // ---- KT flux at faces: face f of column c lies between local cells f+2 and f+3
   for (int idx = tid; idx < S::NFACE; idx += NT) {
-    const int f = idx % (TL + 1), c = idx / (TL + 1);
+    // consecutive threads take consecutive shared-memory words: along the
+    // direction for x (cells of a column are contiguous), across it else
+    const int f = DIR == 0 ? idx % (TL + 1) : idx / NC;
+    const int c = DIR == 0 ? idx / (TL + 1) : idx % NC;
     const int a = f + 3;
     const int g = a0 + a;  // global index of the cell right of the face
     bool ok;
@@ -184,14 +187,15 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
       const R fr = face_right<R>(C, sm.q[l], sm2, sm1, s0, sp1, sp2);
       const R vl = face_left<R>(C, sm.q[9 + l], sm3, sm2, sm1, s0, sp1);
       const R vr = face_right<R>(C, sm.q[9 + l], sm2, sm1, s0, sp1, sp2);
-      sm.h[l][idx] = (R)0.5 * (fl + fr) - (R)0.5 * amax * (vr - vl);
+      sm.h[l][c * (TL + 1) + f] = (R)0.5 * (fl + fr) - (R)0.5 * amax * (vr - vl);
     }
   }
   __syncthreads();
 
   // ---- flux difference and velocity derivative of interior cells
   for (int idx = tid; idx < TL * NC; idx += NT) {
-    const int a = idx % TL + 3, c = idx / TL;
+    const int a = (DIR == 0 ? idx % TL : idx / NC) + 3;
+    const int c = DIR == 0 ? idx / TL : idx % NC;
     const int g = a0 + a;
     bool ok;
     const long long cb = cross_base(c, ok);
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(128) k_update(DevCfg C, DevPtrs<R> P, double t
     for (int l = 0; l < 4; l++) Tt[l] = (double)q9[l];
 #pragma unroll
     for (int l = 0; l < 5; l++) pd[l] = (double)q9[4 + l];
-    const int it = con2prim(C, Tt, pd, tau1, x);
+    const int it = con2prim(C, Tt, pd, tau1, x, sizeof(R) == 4 ? 1e-10 : 1e-16);
     if (it < 0) {
       atomicOr(P.status, ST_ROOT);
     } else {
