@@ -46,6 +46,9 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--precision-report", action="store_true",
+                   help="run the workload to tau_end in FP64 and mixed precision; report errors and speedup")
+    p.add_argument("--tau-end", type=float, default=10.0)
     return p.parse_args()
 
 
@@ -302,6 +305,51 @@ def run_ours(args, rank, world, dist):
     return out
 
 
+def precision_report(args):
+    """Both precisions from the same initial state to tau_end: max and L2
+    relative errors of e, u^mu, pi^{mu nu} of the mixed step against the FP64
+    step over the interior, and the device-time ratio."""
+    import numpy as np
+    import torch
+    from viral_b200 import configs as C
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    res = {}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        cfg, inp, desc = build_workload(args.workload, prec)
+        nsteps = C.steps_between(cfg.tau0, args.tau_end, cfg.dtau)
+        H = C.make_hydro(cfg, inp)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        H.step(nsteps)
+        e1.record()
+        torch.cuda.synchronize()
+        res[prec] = {"ms": e0.elapsed_time(e1), "steps": nsteps, "tau": H.tau, "tmax_gev": H.max_temperature()}
+        states[prec] = H.get_state()
+        H.close()
+    gx, gy, gz = cfg.gdims()
+    idx = np.arange(gx * gy * gz)
+    i, j, k = idx % gx, (idx // gx) % gy, idx // (gx * gy)
+    kl, kr = (0, 1) if cfg.boost_invariant else (3, 3 + cfg.nz)
+    m = (i >= 3) & (i < 3 + cfg.nx) & (j >= 3) & (j < 3 + cfg.ny) & (k >= kl) & (k < kr)
+    a, b = states["mixed"][:, m], states["fp64"][:, m]
+    groups = {"e": [0], "u": [1, 2, 3, 4], "pi": [5, 6, 7, 8, 9]}
+    err = {}
+    for g, qs in groups.items():
+        d = a[qs] - b[qs]
+        scale = np.max(np.abs(b[qs]))
+        err[g] = {"max_rel": float(np.max(np.abs(d)) / scale),
+                  "l2_rel": float(np.sqrt(np.sum(d * d)) / np.sqrt(np.sum(b[qs] * b[qs])))}
+    out = {"report": "mixed vs fp64", "workload": args.workload, "tau_end": res["fp64"]["tau"],
+           "steps": res["fp64"]["steps"], "ms_fp64": res["fp64"]["ms"], "ms_mixed": res["mixed"]["ms"],
+           "speedup": res["fp64"]["ms"] / res["mixed"]["ms"], "errors": err,
+           "tmax_gev": {"fp64": res["fp64"]["tmax_gev"], "mixed": res["mixed"]["tmax_gev"]},
+           "error_norms": "max_rel = max|mixed-fp64| / max|fp64| over the group's components; "
+                          "l2_rel = ||mixed-fp64||_2 / ||fp64||_2"}
+    print(json.dumps(out), flush=True)
+
+
 def ctypes_void_p(v):
     import ctypes
     return ctypes.c_void_p(v)
@@ -311,6 +359,10 @@ def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.precision_report:
+        if rank == 0:
+            precision_report(args)
+        return
     if args.impl == "reference":
         if rank != 0:
             return

@@ -198,11 +198,12 @@ int vh_profile_gubser(int nx, int ny, double dx, double dy, double q, double tau
 /* Monte-Carlo Glauber energy density (two Woods-Saxon nuclei): A nucleons
  * per nucleus, radius R, diffuseness aws, hard core dmin, impact parameter
  * b, sigma_nn (fm^2), Gaussian width w per participant, peak e in GeV/fm^3,
- * eta plateau half-width and Gaussian tail width; seed.  Writes e (fm^-4)
- * on the ghost-inclusive grid and returns the participant count in *npart. */
+ * eta plateau half-width and Gaussian tail width, a floor efloor_gev
+ * (GeV/fm^3) under which no cell starts; seed.  Writes e (fm^-4) on the
+ * ghost-inclusive grid and returns the participant count in *npart. */
 int vh_profile_glauber(int nx, int ny, int nz, int boost_invariant, double dx, double dy, double dz,
                        int A, double R, double aws, double dmin, double b, double sigma_nn,
-                       double w, double epeak_gev, double eta_flat, double eta_sigma,
+                       double w, double epeak_gev, double eta_flat, double eta_sigma, double efloor_gev,
                        double hbarc, uint64_t seed, double* e, int* npart);
 
 #ifdef __cplusplus

@@ -79,7 +79,8 @@ SIGNATURES = [
                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
-                                          ctypes.c_double, ctypes.c_uint64, _dp, ctypes.POINTER(ctypes.c_int)]),
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_uint64, _dp,
+                                          ctypes.POINTER(ctypes.c_int)]),
 ]
 
 _lib = None

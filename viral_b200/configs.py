@@ -48,9 +48,17 @@ def glauber_config(nx=161, ny=161, nz=41, boost_invariant=False, precision=A.PRE
                   taupi_kind=A.TAUPI_15_ETA_OVER_P)
 
 
-def glauber_inputs(cfg: Config, b=7.0, seed=0):
+# Initial energy-density floor (GeV/fm^3), 1e-3 of the 40 GeV/fm^3 peak.
+# Lower floors let the viscous stress outgrow e in the near-vacuum outside
+# the fireball (pi/e > 20, |v| -> 1) until the root-find has no solution
+# before tau = 10 fm/c; the reference enables no regulator for that.
+GLAUBER_FLOOR_GEV = 0.04
+
+
+def glauber_inputs(cfg: Config, b=7.0, seed=0, efloor_gev=None):
+    floor = GLAUBER_FLOOR_GEV if efloor_gev is None else efloor_gev
     e, npart = profile_glauber(cfg.nx, cfg.ny, cfg.nz, cfg.boost_invariant, cfg.dx, cfg.dy, cfg.dz, b=b, seed=seed,
-                               hbarc=cfg.hbarc)
+                               efloor_gev=floor, hbarc=cfg.hbarc)
     z = np.zeros_like(e)
     return dict(tau=cfg.tau0, e=e, ux=z, uy=z, ueta=z, prevu=None, pi_mode=A.PI_ZERO, npart=npart)
 

@@ -119,8 +119,8 @@ extern "C" int vh_profile_gubser(int nx, int ny, double dx, double dy, double q,
 
 extern "C" int vh_profile_glauber(int nx, int ny, int nz, int boost_invariant, double dx, double dy, double dz, int A,
                                   double R, double aws, double dmin, double b, double sigma_nn, double w,
-                                  double epeak_gev, double eta_flat, double eta_sigma, double hbarc, uint64_t seed,
-                                  double* e, int* npart) {
+                                  double epeak_gev, double eta_flat, double eta_sigma, double efloor_gev,
+                                  double hbarc, uint64_t seed, double* e, int* npart) {
   if (nx < 1 || ny < 1 || A < 1 || !e || !(w > 0) || !(sigma_nn > 0) || !(epeak_gev > 0)) return VH_E_ARG;
   Rng rng(seed * 0x9E3779B97F4A7C15ull + 12345);
   // nucleon positions: radius from r^2 / (1 + exp((r-R)/a)) by rejection,
@@ -183,10 +183,10 @@ extern "C" int vh_profile_glauber(int nx, int ny, int nz, int boost_invariant, d
       et[(size_t)j * gx + i] = s;
       if (i >= 3 && i < 3 + nx && j >= 3 && j < 3 + ny) emax = std::max(emax, s);
     }
-  // peak e over the interior is epeak; a floor of 1e-5 of the peak keeps
-  // pressure and temperature positive far outside the fireball
+  // peak e over the interior is epeak; the floor keeps pressure and
+  // temperature positive far outside the fireball
   const double scale = emax > 0 ? epeak_gev / hbarc / emax : 0.0;
-  const double floor_fm = 1e-5 * epeak_gev / hbarc;
+  const double floor_fm = efloor_gev / hbarc;
   for (int k = 0; k < gz; k++) {
     const double ae = std::fabs(Z[k]);
     const double fz = ae <= eta_flat ? 1.0 : std::exp(-0.5 * (ae - eta_flat) * (ae - eta_flat) / (eta_sigma * eta_sigma));

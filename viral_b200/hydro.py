@@ -176,11 +176,11 @@ def profile_gubser(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, t0_gev=0.6, a=A_Q
 
 def profile_glauber(nx, ny, nz=1, boost_invariant=True, dx=0.1, dy=0.1, dz=0.25, A_nuc=208, R=6.62, aws=0.546,
                     dmin=0.4, b=7.0, sigma_nn=6.4, w=0.5, epeak_gev=40.0, eta_flat=1.5, eta_sigma=1.3,
-                    hbarc=HBARC, seed=0):
+                    efloor_gev=0.04, hbarc=HBARC, seed=0):
     gz = 1 if boost_invariant else nz + 6
     e = np.zeros((nx + 6) * (ny + 6) * gz)
     npart = ctypes.c_int()
     A.check(A.lib().vh_profile_glauber(nx, ny, nz, int(boost_invariant), dx, dy, dz, A_nuc, R, aws, dmin, b,
-                                       sigma_nn, w, epeak_gev, eta_flat, eta_sigma, hbarc, seed, A.ptr(e),
+                                       sigma_nn, w, epeak_gev, eta_flat, eta_sigma, efloor_gev, hbarc, seed, A.ptr(e),
                                        ctypes.byref(npart)))
     return e, npart.value
