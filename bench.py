@@ -189,6 +189,22 @@ def build_workload(name: str, precision: str):
     return cfg, inp, desc
 
 
+def max_over_ranks(ms: float, dist, device: str) -> float:
+    """The slowest rank's device time (every rank calls this)."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def whole_job_rate(cells: int, steps: int, world: int, ms: float) -> float:
+    """Cell updates per second of all replicas together (weak scaling)."""
+    return cells * steps * world / (ms / 1e3)
+
+
 def algorithmic_bytes(cfg, kernel: str) -> float:
     """Bytes one launch of `kernel` must move per interior cell (state words
     it has to read and write once; halo re-reads not counted)."""
@@ -239,13 +255,8 @@ def run_ours(args, rank, world, dist):
         H.step(args.steps)
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    value = cells * args.steps * world / (ms / 1e3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
+    value = whole_job_rate(cells, args.steps, world, ms)
 
     # per-kernel device times (outside the timed region) for the roofline
     kt = H.time_kernels(2)

@@ -640,6 +640,16 @@ static int solve4(double A[4][4], double b[4]) {
   return 0;
 }
 
+/* residuals and Jacobian of the conserved-to-primitive system (test hook) */
+void vho_residual(const vho_grid* g, const double* x, const double* prm, double* y, double* J16) {
+  /* prm = {T00, T10, T20, T30, pi1..pi5, Pi (ignored, 0), tau} */
+  double J[4][4];
+  double t2 = g->c.cartesian ? 1.0 : prm[10] * prm[10];
+  c2p_fj(&g->c, prm, prm + 4, t2, x, y, J);
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) J16[a * 4 + b] = J[a][b];
+}
+
 /* Globally convergent Newton with the reference's stopping rule
  * (|dx_i| < 1e-16 |x_i| or dx_i == 0 for all i, at most 100 iterations,
  * NEWEST5/multiroot.h:389-422).  Step control restates GSL's documented

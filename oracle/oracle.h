@@ -90,6 +90,10 @@ long long vho_last_iterations(const vho_grid* g);
  * x[4] = (e,u1,u2,u3); on return x holds the root; returns iterations or -1 */
 int vho_con2prim(const vho_grid* g, const double* T, const double* pi, double tau, double* x);
 
+/* residuals y[4] and Jacobian J16 (row-major) of the conserved-to-primitive
+ * system at x = (e,u1,u2,u3); prm = {T00,T10,T20,T30,pi1..pi5,0,tau} */
+void vho_residual(const vho_grid* g, const double* x, const double* prm, double* y, double* J16);
+
 /* Israel-Stewart source for one cell from (e,u,pi,du,tau): out[5] */
 void vho_is_source(const vho_grid* g, double e, const double* u, const double* pi5,
                    const double* du16, double tau, double* out);

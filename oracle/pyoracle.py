@@ -106,7 +106,7 @@ class Oracle:
             for name in ("vho_destroy", "vho_dims", "vho_set_state", "vho_get_state", "vho_step",
                          "vho_stage_terms", "vho_ns_init", "vho_boundary", "vho_fill_tmunu",
                          "vho_max_temp_gev", "vho_last_iterations", "vho_eos", "vho_con2prim",
-                         "vho_is_source"):
+                         "vho_is_source", "vho_residual"):
                 getattr(L, name).argtypes = None
             L.vho_destroy.argtypes = [ctypes.c_void_p]
             L.vho_set_state.argtypes = [ctypes.c_void_p, _dp]
@@ -125,6 +125,7 @@ class Oracle:
             L.vho_con2prim.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, _dp]
             L.vho_con2prim.restype = ctypes.c_int
             L.vho_is_source.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp, _dp, _dp, ctypes.c_double, _dp]
+            L.vho_residual.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
             cls._lib = L
         return cls._lib
 
@@ -176,6 +177,12 @@ class Oracle:
         out = np.zeros(6)
         self.lib().vho_eos(self.h, e, _ptr(out))
         return out
+
+    def residual(self, x, prm):
+        y = np.zeros(4); J = np.zeros(16)
+        self.lib().vho_residual(self.h, _ptr(np.ascontiguousarray(x, dtype=np.float64)),
+                                _ptr(np.ascontiguousarray(prm, dtype=np.float64)), _ptr(y), _ptr(J))
+        return y, J.reshape(4, 4)
 
 
 class RefBuild:

@@ -1,0 +1,113 @@
+"""Generate the golden fixtures of the viscous KT step from the reference's
+own code (its NEWEST5 / TXYZ5 headers compiled by oracle/Makefile into
+oracle/_ref/).  Runs only where the reference tree is present:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+For each compile-time scenario of the reference a seeded smooth viscous
+state is built on the reference's grid (pyoracle.smooth_state, then
+T^{tau mu} from the oracle's closure), and the reference computes:
+  * the stage-1 terms: sources, flux divergence, velocity gradients;
+  * the state after two TVDRK2 steps;
+  * (Milne) the Navier-Stokes initialisation of pi and T^{tau mu};
+  * residuals and Jacobian of the conserved-to-primitive system at random
+    points.
+Outputs are stored at a seeded sample of interior cells (plus per-field
+sums over the whole grid), so that the fixtures stay small.  The CPU tests
+rebuild the same inputs and check the oracle against these numbers.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from pyoracle import Oracle, OracleConfig, RefBuild, smooth_state  # noqa: E402
+
+# reference scenario blocks (oracle/Makefile) and the EOS / transport they compile
+SCENARIOS = {
+    "milne_lbi": dict(etas0=1 / (4 * math.pi), taupi_kind=0, cartesian=False, mirror=False, tau=1.3),
+    "milne_3d": dict(etas0=1 / (4 * math.pi), taupi_kind=0, cartesian=False, mirror=False, tau=1.3),
+    "gubser": dict(etas0=0.2, taupi_kind=1, cartesian=False, mirror=True, tau=1.3),
+    "cart_3d": dict(etas0=0.01 / (4 * math.pi), taupi_kind=0, cartesian=True, mirror=False, tau=1.0),
+}
+TS = 0.01
+SEED = 7
+NSAMPLE = 400
+
+
+def oracle_config(R: RefBuild, sc: dict) -> OracleConfig:
+    return OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=(1 if R.boost_invariant else R.gz - 6),
+                        boost_invariant=R.boost_invariant, cartesian=sc["cartesian"], dx=R.dx, dy=R.dy, dz=R.dz,
+                        eos_kind=0, eos_a=R.factor, etas0=sc["etas0"], etas1=0.0, hbarc=R.gevfm,
+                        taupi_kind=sc["taupi_kind"], gubser_mirror=sc["mirror"])
+
+
+def inputs(R: RefBuild, sc: dict) -> np.ndarray:
+    x, y, z = R.coords()
+    f = smooth_state(x, y, z, sc["tau"], TS, seed=SEED, cartesian=sc["cartesian"])
+    O = Oracle(oracle_config(R, sc))
+    O.set_state(f)
+    O.fill_tmunu(sc["tau"])
+    return O.get_state()
+
+
+def interior(R: RefBuild) -> np.ndarray:
+    idx = np.arange(R.n)
+    i, j, k = idx % R.gx, (idx // R.gx) % R.gy, idx // (R.gx * R.gy)
+    return np.where((i >= R.il) & (i < R.ir) & (j >= R.jl) & (j < R.jr) & (k >= R.kl) & (k < R.kr))[0]
+
+
+def make(variant: str) -> dict:
+    sc = SCENARIOS[variant]
+    R = RefBuild(variant)
+    f = inputs(R, sc)
+    rng = np.random.default_rng(123)
+    cells = np.sort(rng.choice(interior(R), size=min(NSAMPLE, len(interior(R))), replace=False))
+    out = {"cells": cells, "tau": sc["tau"], "ts": TS, "seed": SEED,
+           "dims": np.array([R.gx, R.gy, R.gz, int(R.boost_invariant)]),
+           "consts": np.array([R.dx, R.dy, R.dz, R.factor, R.gevfm])}
+    R.set_state(f)
+    src, res, du = R.stage_terms(sc["tau"], TS)
+    out["src"] = src[:9, cells]
+    out["res"] = res[:9, cells]
+    out["du"] = du[:, cells]
+    R.set_state(f)
+    R.step(sc["tau"], TS)
+    R.step(sc["tau"] + TS, TS)
+    s2 = R.get_state()
+    out["step2"] = s2[:, cells]
+    out["step2_sum"] = s2.sum(axis=1)
+    if not sc["cartesian"]:
+        R.set_state(f)
+        R.ns_init(sc["tau"], TS)
+        ns = R.get_state()
+        out["ns"] = ns[5:14, cells]
+        out["ns_sum"] = ns[5:14].sum(axis=1)
+    # residual / Jacobian at random points near the state of sampled cells
+    xs, ps, ys, Js = [], [], [], []
+    for c in cells[:40]:
+        x = np.array([f[0, c], f[2, c], f[3, c], f[4, c]]) * (1 + 0.01 * rng.standard_normal(4))
+        prm = np.concatenate([f[10:14, c], f[5:10, c], [0.0, sc["tau"]]])
+        y, J = R.residual(x, prm)
+        xs.append(x); ps.append(prm); ys.append(y); Js.append(J)
+    out["res_x"], out["res_p"], out["res_y"], out["res_J"] = map(np.array, (xs, ps, ys, Js))
+    return out
+
+
+def main():
+    for v in SCENARIOS:
+        d = make(v)
+        path = os.path.join(HERE, f"ref_{v}.npz")
+        np.savez_compressed(path, **d)
+        print(path, os.path.getsize(path))
+
+
+if __name__ == "__main__":
+    main()

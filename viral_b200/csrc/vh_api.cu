@@ -256,20 +256,20 @@ static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, dou
   const R inv_h = (R)(1.0 / hh), hr = (R)hh;
   if (dir == 0) {
     using T = Tile<0, R>;
-    block = dim3(T::NA, T::NC);
+    block = dim3(T::NA * T::NC);
     grid = dim3((C.nx + T::NA - 7) / (T::NA - 6), (C.ny + T::NC - 1) / T::NC, nzi);
     sm = sizeof(DirSmem<R, 0>);
     k_dir<R, 0><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
   } else if (dir == 1) {
     using T = Tile<1, R>;
-    block = dim3(T::NC, T::NA);
-    grid = dim3((C.nx + T::NC - 1) / T::NC, (C.ny + T::NA - 7) / (T::NA - 6), nzi);
+    block = dim3(T::NA * T::NC);
+    grid = dim3((C.ny + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, nzi);
     sm = sizeof(DirSmem<R, 1>);
     k_dir<R, 1><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
   } else {
     using T = Tile<2, R>;
-    block = dim3(T::NC, T::NA);
-    grid = dim3((C.nx + T::NC - 1) / T::NC, (C.nz + T::NA - 7) / (T::NA - 6), C.ny);
+    block = dim3(T::NA * T::NC);
+    grid = dim3((C.nz + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, C.ny);
     sm = sizeof(DirSmem<R, 2>);
     k_dir<R, 2><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
   }

@@ -215,6 +215,37 @@ __device__ inline R weno_right(R qm2, R qm1, R qc, R qp1, R qp2) {
   const R q2 = -qm2 + (R)5 * qm1 + (R)2 * qc;
   return (n0 * q0 + n1 * q1 + n2 * q2) / ((R)6 * (n0 + n1 + n2));
 }
+// Both face values of one stencil at once: L at i+1/2 (genWENOL) and R at
+// i-1/2 (genWENOR) share the smoothness indicators and their products.
+template <class R>
+__device__ inline void weno_lr(R qm2, R qm1, R qc, R qp1, R qp2, R& L, R& Rr) {
+  R b0, b1, b2;
+  weno_beta<R>(qm2, qm1, qc, qp1, qp2, b0, b1, b2);
+  const R eps = (R)1e-6;
+  const R e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+  const R E0 = e0 * e0, E1 = e1 * e1, E2 = e2 * e2;
+  const R P12 = E1 * E2, P02 = E0 * E2, P01 = E0 * E1;
+  const R nl0 = (R)0.3 * P12, nl1 = (R)0.6 * P02, nl2 = (R)0.1 * P01;
+  const R nr0 = (R)0.1 * P12, nr1 = nl1, nr2 = (R)0.3 * P01;
+  const R ql0 = (R)2 * qc + (R)5 * qp1 - qp2;
+  const R ql1 = -qm1 + (R)5 * qc + (R)2 * qp1;
+  const R ql2 = (R)2 * qm2 - (R)7 * qm1 + (R)11 * qc;
+  const R qr0 = (R)11 * qc - (R)7 * qp1 + (R)2 * qp2;
+  const R qr1 = (R)2 * qm1 + (R)5 * qc - qp1;
+  const R qr2 = -qm2 + (R)5 * qm1 + (R)2 * qc;
+  const R numl = nl0 * ql0 + nl1 * ql1 + nl2 * ql2, denl = (R)6 * (nl0 + nl1 + nl2);
+  const R numr = nr0 * qr0 + nr1 * qr1 + nr2 * qr2, denr = (R)6 * (nr0 + nr1 + nr2);
+  if (sizeof(R) == 8) {
+    // one reciprocal for both (the product stays far inside double range)
+    const R inv = (R)1 / (denl * denr);
+    L = numl * denr * inv;
+    Rr = numr * denl * inv;
+  } else {
+    L = __fdividef((float)numl, (float)denl);
+    Rr = __fdividef((float)numr, (float)denr);
+  }
+}
+
 // generalized minmod (theta) piecewise-linear face values (utils.h:33-55)
 template <class R>
 __device__ inline R mm3(R a, R b, R c) {

@@ -18,27 +18,25 @@
 
 namespace vh {
 
-// Tile shapes: NA cells along the direction (6 of them halo), NC cells
-// across it.  Along x the warp runs along the direction; along y and eta
-// it runs across (x), so global loads stay coalesced.
+// Tile shapes: NA = 32 cells along the direction (6 of them halo, so 26
+// outputs), NC lines across it.  Loads run x-fastest (coalesced); in the
+// compute phase each warp owns one line and its lanes walk along it.
 template <int DIR, class R>
 struct Tile;
 template <class R>
 struct Tile<0, R> { static constexpr int NA = 32, NC = 4; };
 template <class R>
-struct Tile<1, R> { static constexpr int NA = 22, NC = 8; };
+struct Tile<1, R> { static constexpr int NA = 32, NC = 8; };
 template <class R>
-struct Tile<2, R> { static constexpr int NA = 22, NC = 8; };
+struct Tile<2, R> { static constexpr int NA = 32, NC = 8; };
 
 template <class R, int DIR>
 struct DirSmem {
   static constexpr int NA = Tile<DIR, R>::NA, NC = Tile<DIR, R>::NC;
   static constexpr int TL = NA - 6;
-  static constexpr int NCELL = NA * NC;
-  static constexpr int NFACE = (TL + 1) * NC;
-  R q[19][NCELL];  // 0..8 F^DIR, 9..17 Var, 18 signal speed
-  R u[4][NCELL];   // u^mu for the velocity derivative
-  R h[9][NFACE];   // KT face fluxes
+  static constexpr int LD = NA + 1;  // padded line length (bank spread)
+  R q[19][NC * LD];  // 0..8 F^DIR, 9..17 Var, 18 signal speed
+  R u[4][NC * LD];   // u^mu for the velocity derivative
 };
 
 // Centre flux along DIR, Var and signal speed of one cell
@@ -86,55 +84,59 @@ __device__ inline void cell_terms(const DevCfg& C, R tau, R e, const R* u, const
   for (int l = 0; l < 5; l++) V[4 + l] = p[l];
 }
 
+// Both face states of the stencil centred on the lane's cell: L at the
+// right face, R at the left face (WENO5, or generalized minmod).
 template <class R>
-__device__ inline R face_left(const DevCfg& C, const R* q, int s_m3, int s_m2, int s_m1, int s_0, int s_p1) {
-  // left state at the face between cells -1 and 0 (stencil centred on -1)
-  if (C.recon == 0) return weno_left<R>(q[s_m3], q[s_m2], q[s_m1], q[s_0], q[s_p1]);
-  return mm_left<R>((R)C.mm_theta, q[s_m2], q[s_m1], q[s_0]);
+__device__ inline void recon_lr(const DevCfg& C, const R* q, int s, R& L, R& Rr) {
+  if (C.recon == 0) {
+    weno_lr<R>(q[s - 2], q[s - 1], q[s], q[s + 1], q[s + 2], L, Rr);
+  } else {
+    L = mm_left<R>((R)C.mm_theta, q[s - 1], q[s], q[s + 1]);
+    Rr = mm_right<R>((R)C.mm_theta, q[s - 1], q[s], q[s + 1]);
+  }
 }
+
 template <class R>
-__device__ inline R face_right(const DevCfg& C, const R* q, int s_m2, int s_m1, int s_0, int s_p1, int s_p2) {
-  // right state at the face between cells -1 and 0 (stencil centred on 0)
-  if (C.recon == 0) return weno_right<R>(q[s_m2], q[s_m1], q[s_0], q[s_p1], q[s_p2]);
-  return mm_right<R>((R)C.mm_theta, q[s_m1], q[s_0], q[s_p1]);
-}
+__device__ inline R shfl_dn(R v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+template <class R>
+__device__ inline R shfl_up(R v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 
 template <class R, int DIR>
 __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
     k_dir(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, R h, int first) {
   using S = DirSmem<R, DIR>;
-  constexpr int NA = S::NA, NC = S::NC, TL = S::TL, NT = NA * NC;
+  constexpr int NA = S::NA, NC = S::NC, TL = S::TL, LD = S::LD;
+  static_assert(NA == 32, "one warp per line");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S& sm = *reinterpret_cast<S*>(smem_raw);
   if (*P.status) return;
 
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int tid = threadIdx.x;
   int lo, hi, galong;
   if (DIR == 0) { lo = C.il; hi = C.ir; galong = C.gx; }
   else if (DIR == 1) { lo = C.jl; hi = C.jr; galong = C.gy; }
   else { lo = C.kl; hi = C.kr; galong = C.gz; }
-  const int a0 = lo - NG + (DIR == 0 ? blockIdx.x : blockIdx.y) * TL;  // global along index of local 0
+  const int a0 = lo - NG + blockIdx.x * TL;  // global along index of local 0
   const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)C.gx : (long long)C.gx * C.gy);
 
-  // cross coordinates of local column c
+  // cross coordinates of line c
   auto cross_base = [&](int c, bool& ok) -> long long {
     int i, j, k;
     if (DIR == 0) { i = 0; j = C.jl + blockIdx.y * NC + c; k = C.kl + blockIdx.z; ok = j < C.jr; }
-    else if (DIR == 1) { i = C.il + blockIdx.x * NC + c; j = 0; k = C.kl + blockIdx.z; ok = i < C.ir; }
-    else { i = C.il + blockIdx.x * NC + c; j = C.jl + blockIdx.z; k = 0; ok = i < C.ir; }
+    else if (DIR == 1) { i = C.il + blockIdx.y * NC + c; j = 0; k = C.kl + blockIdx.z; ok = i < C.ir; }
+    else { i = C.il + blockIdx.y * NC + c; j = C.jl + blockIdx.z; k = 0; ok = i < C.ir; }
     return cix(C, i, j, k);
   };
-  auto sidx = [](int a, int c) { return DIR == 0 ? c * NA + a : a * NC + c; };
 
   R* const* set = use_b ? P.B : P.A;
-  // ---- load and per-cell terms
+  // ---- load and per-cell terms (x-fastest thread order: coalesced)
   {
-    const int ta = DIR == 0 ? threadIdx.x : threadIdx.y;
-    const int tc = DIR == 0 ? threadIdx.y : threadIdx.x;
+    const int ta = DIR == 0 ? tid % NA : tid / NC;
+    const int tc = DIR == 0 ? tid / NA : tid % NC;
     bool ok;
     const long long cb = cross_base(tc, ok);
     const int g = a0 + ta;
-    const int s = sidx(ta, tc);
+    const int s = tc * LD + ta;
     R F[9], V[9], spd = 0, uu[4] = {0, 0, 0, 0};
     if (ok && g >= 0 && g < galong) {
       const long long c = cb + (long long)g * stride;
@@ -159,60 +161,52 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
   }
   __syncthreads();
 
-  // ---- KT flux at faces: face f of column c lies between local cells f+2 and f+3
-  for (int idx = tid; idx < S::NFACE; idx += NT) {
-    // consecutive threads take consecutive shared-memory words: along the
-    // direction for x (cells of a column are contiguous), across it else
-    const int f = DIR == 0 ? idx % (TL + 1) : idx / NC;
-    const int c = DIR == 0 ? idx / (TL + 1) : idx % NC;
-    const int a = f + 3;
-    const int g = a0 + a;  // global index of the cell right of the face
-    bool ok;
-    cross_base(c, ok);
-    if (!ok || g > hi) continue;
-    const int sm3 = sidx(a - 3, c), sm2 = sidx(a - 2, c), sm1 = sidx(a - 1, c), s0 = sidx(a, c),
-              sp1 = sidx(a + 1, c), sp2 = sidx(a + 2, c);
-    R amax = 0;
+  // ---- one warp per line: lane a reconstructs both face states of its
+  // stencil; the face right of lane a takes R from lane a + 1
+  const int a = tid & 31, c = tid >> 5;
+  bool ok;
+  const long long cb = cross_base(c, ok);
+  if (!ok) return;  // whole warp: c is uniform in the warp
+  const int g = a0 + a;
+  const int s = c * LD + a;
+  const bool stencil = a >= 2 && a <= NA - 3;  // a-2..a+2 inside the tile
+  // face right of lane a exists for lanes 2..NA-4; it is a needed face when
+  // the cell right of it is in [lo, hi]
+  R amax = 0;
+  {
+    R L = 0, Rr = 0;
+    if (stencil) recon_lr<R>(C, sm.q[18], s, L, Rr);
+    const R Rn = shfl_dn<R>(Rr, 1);
     // the face left of the first interior cell takes no dissipation: its
     // max speed sits in a ghost cell the reference never fills
     // (NEWEST5/hydroKT.h:265-314 vs 435-440)
-    if (g != lo) {
-      R sl = face_left<R>(C, sm.q[18], sm3, sm2, sm1, s0, sp1);
-      R sr = face_right<R>(C, sm.q[18], sm2, sm1, s0, sp1, sp2);
-      amax = fmax(fabs(sl), fabs(sr));
-    }
-#pragma unroll 1
-    for (int l = 0; l < 9; l++) {
-      const R fl = face_left<R>(C, sm.q[l], sm3, sm2, sm1, s0, sp1);
-      const R fr = face_right<R>(C, sm.q[l], sm2, sm1, s0, sp1, sp2);
-      const R vl = face_left<R>(C, sm.q[9 + l], sm3, sm2, sm1, s0, sp1);
-      const R vr = face_right<R>(C, sm.q[9 + l], sm2, sm1, s0, sp1, sp2);
-      sm.h[l][c * (TL + 1) + f] = (R)0.5 * (fl + fr) - (R)0.5 * amax * (vr - vl);
-    }
+    amax = (g + 1 == lo) ? (R)0 : fmax(fabs(L), fabs(Rn));
   }
-  __syncthreads();
-
-  // ---- flux difference and velocity derivative of interior cells
-  for (int idx = tid; idx < TL * NC; idx += NT) {
-    const int a = (DIR == 0 ? idx % TL : idx / NC) + 3;
-    const int c = DIR == 0 ? idx / TL : idx % NC;
-    const int g = a0 + a;
-    bool ok;
-    const long long cb = cross_base(c, ok);
-    if (!ok || g >= hi) continue;
-    const long long cell = cb + (long long)g * stride;
-    const int fr = c * (TL + 1) + (a - 2), fl = c * (TL + 1) + (a - 3);
-#pragma unroll
-    for (int l = 0; l < 9; l++) {
-      const R r = -inv_h * (sm.h[l][fr] - sm.h[l][fl]);
+  const bool out = a >= 3 && a < 3 + TL && g < hi;  // interior cell of this tile
+  const long long cell = cb + (long long)g * stride;
+#pragma unroll 1
+  for (int l = 0; l < 9; l++) {
+    R fl = 0, fr = 0, vl = 0, vr = 0;
+    if (stencil) {
+      recon_lr<R>(C, sm.q[l], s, fl, fr);
+      recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
+    }
+    fr = shfl_dn<R>(fr, 1);
+    vr = shfl_dn<R>(vr, 1);
+    const R H = (R)0.5 * (fl + fr) - (R)0.5 * amax * (vr - vl);  // flux at the right face
+    const R Hl = shfl_up<R>(H, 1);                                // flux at the left face
+    if (out) {
+      const R r = -inv_h * (H - Hl);
       P.res[l][cell] = first ? r : P.res[l][cell] + r;
     }
-    const int sm2 = sidx(a - 2, c), sm1 = sidx(a - 1, c), s0 = sidx(a, c), sp1 = sidx(a + 1, c), sp2 = sidx(a + 2, c);
+  }
+  // velocity derivative along DIR: (L - R)/h of the same stencil (genWENOder)
+  if (out) {
 #pragma unroll
     for (int l = 0; l < 4; l++) {
       const R* q = sm.u[l];
-      const R L = weno_left<R>(q[sm2], q[sm1], q[s0], q[sp1], q[sp2]);
-      const R Rr = weno_right<R>(q[sm2], q[sm1], q[s0], q[sp1], q[sp2]);
+      R L, Rr;
+      weno_lr<R>(q[s - 2], q[s - 1], q[s], q[s + 1], q[s + 2], L, Rr);
       P.du[l * 3 + DIR][cell] = (L - Rr) / h;
     }
   }
@@ -236,7 +230,7 @@ __device__ inline void ghost_put(const DevPtrs<R>& P, R* const* set, long long d
 // root-find and the ghost copy.  STAGE 1 reads set A and writes set B and
 // v1t; STAGE 2 reads A (its own cell), B and v1t and writes A.
 template <class R, int STAGE>
-__global__ void __launch_bounds__(128) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
+__global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
   if (*P.status) return;
   const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

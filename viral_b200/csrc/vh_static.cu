@@ -109,15 +109,15 @@ int launch_dir_static(const DevCfg& C, const DevPtrs<double>& P, int dir, int us
   if (dir == 0) {
     using T = Tile<0, double>;
     dim3 grid((C.nx + T::NA - 7) / (T::NA - 6), (C.ny + T::NC - 1) / T::NC, nzi);
-    k_dir<double, 0><<<grid, dim3(T::NA, T::NC), sizeof(DirSmem<double, 0>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
+    k_dir<double, 0><<<grid, dim3(T::NA * T::NC), sizeof(DirSmem<double, 0>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
   } else if (dir == 1) {
     using T = Tile<1, double>;
-    dim3 grid((C.nx + T::NC - 1) / T::NC, (C.ny + T::NA - 7) / (T::NA - 6), nzi);
-    k_dir<double, 1><<<grid, dim3(T::NC, T::NA), sizeof(DirSmem<double, 1>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
+    dim3 grid((C.ny + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, nzi);
+    k_dir<double, 1><<<grid, dim3(T::NA * T::NC), sizeof(DirSmem<double, 1>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
   } else {
     using T = Tile<2, double>;
-    dim3 grid((C.nx + T::NC - 1) / T::NC, (C.nz + T::NA - 7) / (T::NA - 6), C.ny);
-    k_dir<double, 2><<<grid, dim3(T::NC, T::NA), sizeof(DirSmem<double, 2>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
+    dim3 grid((C.nz + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, C.ny);
+    k_dir<double, 2><<<grid, dim3(T::NA * T::NC), sizeof(DirSmem<double, 2>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
   }
   return cudaGetLastError() == cudaSuccess ? VH_OK : VH_E_CUDA;
 }
