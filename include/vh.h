@@ -178,6 +178,49 @@ int vh_last_iterations(vh_handle* h, long long* iters);
 int vh_step_static(const vh_config* cfg, double* state, const double* eos_dev, double tau, int nsteps,
                    void* stream);
 
+/* ------------------------------------------------------------- batches */
+/* An ensemble of boost-invariant Milne events evolved together by one
+ * persistent kernel over a packed event table (one device pool for all
+ * events).  Every event has its own grid (nx[i] x ny[i]), start time, step
+ * and maximum time; it stops when its maximum temperature falls below
+ * t_freeze_gev or its time reaches tau_max (the reference's main-loop
+ * breaks, NEWEST5/main.cpp:188-205, applied per event), or fails alone
+ * (root-find / causality) while the others continue.  The common physics
+ * (EOS, transport, precision, reconstruction, dx, dy) comes from cfg; its
+ * grid and time fields are ignored. */
+typedef struct vh_batch vh_batch;
+enum { VH_EVENT_RUNNING = 0, VH_EVENT_FROZEN = 1, VH_EVENT_TAUMAX = 2, VH_EVENT_FAILED = 3 };
+int vh_batch_create(const vh_config* cfg, int n_events, const int* nx, const int* ny, const double* tau0,
+                    const double* dtau, const double* tau_max, double t_freeze_gev, vh_batch** out);
+int vh_batch_destroy(vh_batch* b);
+/* rewind every event to its start time and running state (the pool keeps
+ * its contents; re-initialise the events to restart them) */
+int vh_batch_reset(vh_batch* b);
+/* one event's initial profile on its ghost-inclusive grid (as vh_init_profile) */
+int vh_batch_init_event(vh_batch* b, int ev, const double* e, const double* ux, const double* uy,
+                        const double* prevu4, int pi_mode, const double* pi5);
+/* every event from the MC-Glauber generator (vh_profile_glauber with the
+ * event's seed and impact parameter), u = 0, pi = 0; host threads */
+int vh_batch_init_glauber(vh_batch* b, const uint64_t* seeds, const double* bimp, int A, double R, double aws,
+                          double dmin, double sigma_nn, double w, double epeak_gev, double efloor_gev,
+                          int nthreads, int* npart_out);
+/* run until every event has stopped or max_steps steps; device seconds and
+ * whether the launches were replayed from a CUDA graph */
+int vh_batch_run(vh_batch* b, int max_steps, double* seconds, int* graph_used);
+/* per-event time, steps taken and state (VH_EVENT_*) */
+int vh_batch_events(vh_batch* b, double* tau, int* steps, int* state);
+/* one event's 18 canonical fields (doubles, its ghost-inclusive grid) */
+int vh_batch_get_event_state(vh_batch* b, int ev, double* host18);
+/* pick the persistent kernel's tile shape (lines per tile), occupancy,
+ * flux-loop unroll and steps per launch by timing probe_steps steps of each
+ * candidate; cached by device, precision and event-size histogram in
+ * cache_path (NULL: no cache) */
+int vh_batch_autotune(vh_batch* b, const char* cache_path, int probe_steps, double* best_ms_per_step);
+int vh_batch_set_tuning(vh_batch* b, int variant, int steps_per_launch, int use_graph);
+int vh_batch_get_tuning(vh_batch* b, int* variant, int* steps_per_launch, int* lines_per_tile, int* blocks_per_sm,
+                        int* unroll);
+const char* vh_batch_last_error(const vh_batch* b);
+
 /* Message of the last error on this handle (or the last vh_create). */
 const char* vh_last_error(const vh_handle* h);
 

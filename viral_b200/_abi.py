@@ -81,6 +81,24 @@ SIGNATURES = [
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_uint64, _dp,
                                           ctypes.POINTER(ctypes.c_int)]),
+    ("vh_batch_create", ctypes.c_int, [ctypes.POINTER(VhConfig), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp, ctypes.c_double,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    ("vh_batch_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("vh_batch_reset", ctypes.c_int, [ctypes.c_void_p]),
+    ("vh_batch_init_event", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, _dp]),
+    ("vh_batch_init_glauber", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), _dp, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_int)]),
+    ("vh_batch_run", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
+    ("vh_batch_events", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
+    ("vh_batch_get_event_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    ("vh_batch_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, _dp]),
+    ("vh_batch_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("vh_batch_get_tuning", ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 5),
+    ("vh_batch_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
 ]
 
 _lib = None

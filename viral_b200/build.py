@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvh.so")
 
-SOURCES = ["vh_api.cu", "vh_static.cu", "vh_inputs.cpp", "vh_io.cpp"]
+SOURCES = ["vh_api.cu", "vh_static.cu", "vh_batch.cu", "vh_inputs.cpp", "vh_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

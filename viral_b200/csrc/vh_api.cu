@@ -55,17 +55,9 @@ static int fail(vh_handle* h, int code, const std::string& msg) {
 
 template <class R>
 static void set_ptrs(DevPtrs<R>& P, void* base, long long n, unsigned int* status, unsigned long long* iters) {
-  R* b = static_cast<R*>(base);
-  auto f = [&](int q) { return b + (long long)q * n; };
-  P.e = f(0);
-  for (int l = 0; l < 4; l++) P.u[l] = f(1 + l);
-  for (int l = 0; l < 4; l++) P.A[l] = f(10 + l);
-  for (int l = 0; l < 5; l++) P.A[4 + l] = f(5 + l);
-  for (int l = 0; l < 4; l++) P.pu[l] = f(14 + l);
-  for (int l = 0; l < 9; l++) P.B[l] = f(18 + l);
-  for (int l = 0; l < 4; l++) P.v1t[l] = f(27 + l);
-  for (int l = 0; l < 9; l++) P.res[l] = f(31 + l);
-  for (int l = 0; l < 12; l++) P.du[l] = f(40 + l);
+  P.base0 = static_cast<R*>(base);
+  P.base1 = static_cast<R*>(base) + 18 * n;
+  P.stride = n;
   P.status = status;
   P.iters = iters;
 }
@@ -495,7 +487,7 @@ static int debug_terms(vh_handle* h, const DevPtrs<R>& P, double* res, double* s
   k_debug_src<R><<<grid1(n, 128), 128, 0, h->stream>>>(C, P, du16, src9, h->tau);
   VH_CUDA(h, cudaGetLastError());
   std::vector<R> tmp(16 * (size_t)n);
-  VH_CUDA(h, cudaMemcpyAsync(tmp.data(), P.res[0], sizeof(R) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaMemcpyAsync(tmp.data(), P.res(0), sizeof(R) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
   for (long long q = 0; q < 9 * n; q++) res[q] = (double)tmp[q];
   VH_CUDA(h, cudaMemcpyAsync(tmp.data(), src9, sizeof(R) * 9 * n, cudaMemcpyDeviceToHost, h->stream));

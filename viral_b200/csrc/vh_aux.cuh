@@ -13,17 +13,17 @@ __global__ void k_fill_tmunu(DevCfg C, DevPtrs<R> P, double tau) {
   if (c >= C.n) return;
   const R t2 = C.cart ? (R)1 : (R)(tau * tau);
   R u[4], p[5];
-  const R e = P.e[c];
+  const R e = P.e()[c];
 #pragma unroll
-  for (int l = 0; l < 4; l++) u[l] = P.u[l][c];
+  for (int l = 0; l < 4; l++) u[l] = P.u(l)[c];
 #pragma unroll
-  for (int l = 0; l < 5; l++) p[l] = P.A[4 + l][c];
+  for (int l = 0; l < 5; l++) p[l] = P.A(4 + l)[c];
   const R Pp = eos_P<R>(C, e), ep = e + Pp;
   PiDep<R> d = pi_dep<R>(u[0], u[1], u[2], u[3], p, t2);
-  P.A[0][c] = -Pp + ep * (u[0] * u[0]) + d.tt;
-  P.A[1][c] = ep * u[0] * u[1] + d.tx;
-  P.A[2][c] = ep * u[0] * u[2] + d.ty;
-  P.A[3][c] = ep * u[0] * u[3] + d.te;
+  P.A(0)[c] = -Pp + ep * (u[0] * u[0]) + d.tt;
+  P.A(1)[c] = ep * u[0] * u[1] + d.tx;
+  P.A(2)[c] = ep * u[0] * u[2] + d.ty;
+  P.A(3)[c] = ep * u[0] * u[3] + d.te;
 }
 
 // Velocity gradients with the coverage the reference's CalcDer4Vel has
@@ -38,9 +38,9 @@ __global__ void k_du_full(DevCfg C, DevPtrs<R> P, R* du16, double ts) {
   const bool ii = i >= C.il && i < C.ir, jj = j >= C.jl && j < C.jr, kk = k >= C.kl && k < C.kr;
 #pragma unroll 1
   for (int l = 0; l < 4; l++) {
-    const R* u = P.u[l];
+    const R* u = P.u(l);
     R d0 = 0, d1 = 0, d2 = 0, d3 = 0;
-    if (ii && jj && kk) d0 = (u[c] - P.pu[l][c]) / (R)ts;
+    if (ii && jj && kk) d0 = (u[c] - P.pu(l)[c]) / (R)ts;
     if (jj && kk && i >= 2 && i < C.gx - 2) {
       const R L = weno_left<R>(u[c - 2], u[c - 1], u[c], u[c + 1], u[c + 2]);
       const R Rr = weno_right<R>(u[c - 2], u[c - 1], u[c], u[c + 1], u[c + 2]);
@@ -79,9 +79,9 @@ __global__ void k_ns_pi(DevCfg C, DevPtrs<R> P, const R* du16, double tau) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C.n) return;
   R u[4], du[4][4];
-  const R e = P.e[c];
+  const R e = P.e()[c];
 #pragma unroll
-  for (int l = 0; l < 4; l++) u[l] = P.u[l][c];
+  for (int l = 0; l < 4; l++) u[l] = P.u(l)[c];
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -91,11 +91,11 @@ __global__ void k_ns_pi(DevCfg C, DevPtrs<R> P, const R* du16, double tau) {
   transport<R>(C, e, Pp, &eta, &tp);
   R sig[4][4], th, acc[4];
   is_kinematics<R>(C.cart, (R)tau, u, du, sig, th, acc);
-  P.A[4][c] = (R)2 * eta * sig[1][1];
-  P.A[5][c] = (R)2 * eta * sig[2][2];
-  P.A[6][c] = (R)2 * eta * sig[1][2];
-  P.A[7][c] = (R)2 * eta * sig[1][3];
-  P.A[8][c] = (R)2 * eta * sig[2][3];
+  P.A(4)[c] = (R)2 * eta * sig[1][1];
+  P.A(5)[c] = (R)2 * eta * sig[2][2];
+  P.A(6)[c] = (R)2 * eta * sig[1][2];
+  P.A(7)[c] = (R)2 * eta * sig[1][3];
+  P.A(8)[c] = (R)2 * eta * sig[2][3];
 }
 
 // Sources at the current state for the debug dump (interior only).
@@ -107,11 +107,11 @@ __global__ void k_debug_src(DevCfg C, DevPtrs<R> P, const R* du16, R* src9, doub
   for (int l = 0; l < 9; l++) src9[l * C.n + c] = 0;
   if (!(i >= C.il && i < C.ir && j >= C.jl && j < C.jr && k >= C.kl && k < C.kr)) return;
   R u[4], p[5], du[4][4];
-  const R e = P.e[c];
+  const R e = P.e()[c];
 #pragma unroll
-  for (int l = 0; l < 4; l++) u[l] = P.u[l][c];
+  for (int l = 0; l < 4; l++) u[l] = P.u(l)[c];
 #pragma unroll
-  for (int l = 0; l < 5; l++) p[l] = P.A[4 + l][c];
+  for (int l = 0; l < 5; l++) p[l] = P.A(4 + l)[c];
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -144,7 +144,7 @@ __global__ void k_max_temp(DevCfg C, DevPtrs<R> P, unsigned long long* out) {
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long long)gridDim.x * blockDim.x) {
     const int i = C.il + (int)(t % C.nx), j = C.jl + (int)((t / C.nx) % C.ny);
     const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
-    const double T = C.hbarc * (double)eos_T<R>(C, P.e[cix(C, i, j, k)]);
+    const double T = C.hbarc * (double)eos_T<R>(C, P.e()[cix(C, i, j, k)]);
     m = fmax(m, T);
   }
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
@@ -168,7 +168,7 @@ __global__ void k_conserve_part(DevCfg C, DevPtrs<R> P, double tau, double dv, d
     const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
     const long long c = cix(C, i, j, k);
 #pragma unroll
-    for (int l = 0; l < 4; l++) two_sum_add(s[l], cc[l], tf * (double)P.A[l][c] * dv);
+    for (int l = 0; l < 4; l++) two_sum_add(s[l], cc[l], tf * (double)P.A(l)[c] * dv);
   }
   __shared__ double sh[2][4][256];
 #pragma unroll
@@ -182,7 +182,7 @@ __global__ void k_conserve_part(DevCfg C, DevPtrs<R> P, double tau, double dv, d
     part[(l * 2 + 1) * gridDim.x + blockIdx.x] = Cc;
   }
 }
-__global__ void k_conserve_final(const double* part, int nb, double* out4) {
+static __global__ void k_conserve_final(const double* part, int nb, double* out4) {
   const int l = threadIdx.x;
   if (l >= 4) return;
   double S = 0, Cc = 0;
@@ -210,8 +210,8 @@ __global__ void k_cfl(DevCfg C, DevPtrs<R> P, double tau, unsigned long long* ou
         R v = 0;
         if (g >= lo && g < hi) {
           const long long cc = cix(C, i, j, k) + (long long)o * s;
-          const R u0 = P.u[0][cc];
-          v = d == 0 ? P.u[1][cc] / u0 : (d == 1 ? P.u[2][cc] / u0 : (C.cart ? P.u[3][cc] / u0 : (R)tau * P.u[3][cc] / u0));
+          const R u0 = P.u(0)[cc];
+          v = d == 0 ? P.u(1)[cc] / u0 : (d == 1 ? P.u(2)[cc] / u0 : (C.cart ? P.u(3)[cc] / u0 : (R)tau * P.u(3)[cc] / u0));
         }
         q[o + 2] = v;
       }
@@ -227,11 +227,11 @@ __global__ void k_cfl(DevCfg C, DevPtrs<R> P, double tau, unsigned long long* ou
 }
 
 // precision conversion between the canonical double layout and float state
-__global__ void k_d2f(const double* in, float* out, long long n) {
+static __global__ void k_d2f(const double* in, float* out, long long n) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) out[t] = (float)in[t];
 }
-__global__ void k_f2d(const float* in, double* out, long long n) {
+static __global__ void k_f2d(const float* in, double* out, long long n) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) out[t] = (double)in[t];
 }

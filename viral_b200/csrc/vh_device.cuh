@@ -30,19 +30,37 @@ struct DevCfg {
   double mm_theta;
 };
 
-// Device buffers of one event.  All arrays are ghost-inclusive SoA.
+// Device buffers of one event: 52 ghost-inclusive SoA arrays of `stride`
+// cells each.  Fields 0..17 are the canonical state (at base0), fields
+// 18..51 the step's scratch (at base1); an event inside a batch pool is the
+// same view shifted by its cell offset.
+//   0 e, 1..4 u^mu, 5..9 pi (set A), 10..13 T^{tau mu} (set A), 14..17 prevu,
+//   18..26 set B (T^{tau mu} 4, pi 5), 27..30 stage-1 tau T^{tau mu},
+//   31..39 flux-divergence accumulator, 40..51 spatial du[l][1+d] at l*3+d.
 template <class R>
 struct DevPtrs {
-  R* e;          // energy density
-  R* u[4];       // u^tau, u^x, u^y, u^eta
-  R* pu[4];      // previous u
-  R* A[9];       // step-start set: T^{tau mu} (4), pi (5)
-  R* B[9];       // stage-1 set
-  R* v1t[4];     // stage-1 tau T^{tau mu} before division (RK2 needs it)
-  R* res[9];     // flux divergence accumulator
-  R* du[12];     // spatial velocity gradients du[l][1+d] at l*3+d
+  R* base0;
+  R* base1;
+  long long stride;
   unsigned int* status;            // OR of failure bits
   unsigned long long* iters;       // Newton iterations
+  __host__ __device__ R* f(int q) const { return q < 18 ? base0 + (long long)q * stride : base1 + (long long)(q - 18) * stride; }
+  __host__ __device__ R* e() const { return base0; }
+  __host__ __device__ R* u(int l) const { return base0 + (long long)(1 + l) * stride; }
+  __host__ __device__ R* pu(int l) const { return base0 + (long long)(14 + l) * stride; }
+  // conserved set: A (step start) or B (stage 1); l < 4 T^{tau mu}, else pi
+  __host__ __device__ R* A(int l) const { return base0 + (long long)(l < 4 ? 10 + l : l + 1) * stride; }
+  __host__ __device__ R* B(int l) const { return base1 + (long long)l * stride; }
+  __host__ __device__ R* S(int use_b, int l) const { return use_b ? B(l) : A(l); }
+  __host__ __device__ R* v1t(int l) const { return base1 + (long long)(9 + l) * stride; }
+  __host__ __device__ R* res(int l) const { return base1 + (long long)(13 + l) * stride; }
+  __host__ __device__ R* du(int l) const { return base1 + (long long)(22 + l) * stride; }
+  __host__ __device__ DevPtrs shifted(long long off) const {
+    DevPtrs p = *this;
+    p.base0 += off;
+    p.base1 += off;
+    return p;
+  }
 };
 
 enum : unsigned { ST_ROOT = 1u, ST_CAUSAL = 2u, ST_NEGE = 4u };

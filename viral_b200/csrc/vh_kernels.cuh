@@ -30,9 +30,9 @@ struct Tile<1, R> { static constexpr int NA = 32, NC = 8; };
 template <class R>
 struct Tile<2, R> { static constexpr int NA = 32, NC = 8; };
 
-template <class R, int DIR>
+template <class R, int DIR, int NC_ = Tile<DIR, R>::NC>
 struct DirSmem {
-  static constexpr int NA = Tile<DIR, R>::NA, NC = Tile<DIR, R>::NC;
+  static constexpr int NA = Tile<DIR, R>::NA, NC = NC_;
   static constexpr int TL = NA - 6;
   static constexpr int LD = NA + 1;  // padded line length (bank spread)
   R q[19][NC * LD];  // 0..8 F^DIR, 9..17 Var, 18 signal speed
@@ -101,35 +101,32 @@ __device__ inline R shfl_dn(R v, int d) { return __shfl_down_sync(0xffffffffu, v
 template <class R>
 __device__ inline R shfl_up(R v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 
-template <class R, int DIR>
-__global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
-    k_dir(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, R h, int first) {
-  using S = DirSmem<R, DIR>;
-  constexpr int NA = S::NA, NC = S::NC, TL = S::TL, LD = S::LD;
+// One tile of the flux sweep along DIR: tile index bx along the direction,
+// by across it, bz the third axis (interior index).  NC*32 threads.
+template <class R, int DIR, int NC, int UNR = 1>
+__device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, int use_b, R tau, R inv_h, R h,
+                                         int first, int bx, int by, int bz, DirSmem<R, DIR, NC>& sm) {
+  using S = DirSmem<R, DIR, NC>;
+  constexpr int NA = S::NA, TL = S::TL, LD = S::LD;
   static_assert(NA == 32, "one warp per line");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S& sm = *reinterpret_cast<S*>(smem_raw);
-  if (*P.status) return;
-
   const int tid = threadIdx.x;
   int lo, hi, galong;
   if (DIR == 0) { lo = C.il; hi = C.ir; galong = C.gx; }
   else if (DIR == 1) { lo = C.jl; hi = C.jr; galong = C.gy; }
   else { lo = C.kl; hi = C.kr; galong = C.gz; }
-  const int a0 = lo - NG + blockIdx.x * TL;  // global along index of local 0
+  const int a0 = lo - NG + bx * TL;  // global along index of local 0
   const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)C.gx : (long long)C.gx * C.gy);
 
   // cross coordinates of line c
   auto cross_base = [&](int c, bool& ok) -> long long {
     int i, j, k;
-    if (DIR == 0) { i = 0; j = C.jl + blockIdx.y * NC + c; k = C.kl + blockIdx.z; ok = j < C.jr; }
-    else if (DIR == 1) { i = C.il + blockIdx.y * NC + c; j = 0; k = C.kl + blockIdx.z; ok = i < C.ir; }
-    else { i = C.il + blockIdx.y * NC + c; j = C.jl + blockIdx.z; k = 0; ok = i < C.ir; }
+    if (DIR == 0) { i = 0; j = C.jl + by * NC + c; k = C.kl + bz; ok = j < C.jr; }
+    else if (DIR == 1) { i = C.il + by * NC + c; j = 0; k = C.kl + bz; ok = i < C.ir; }
+    else { i = C.il + by * NC + c; j = C.jl + bz; k = 0; ok = i < C.ir; }
     return cix(C, i, j, k);
   };
 
-  R* const* set = use_b ? P.B : P.A;
-  // ---- load and per-cell terms (x-fastest thread order: coalesced)
+    // ---- load and per-cell terms (x-fastest thread order: coalesced)
   {
     const int ta = DIR == 0 ? tid % NA : tid / NC;
     const int tc = DIR == 0 ? tid / NA : tid % NC;
@@ -141,13 +138,13 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
     if (ok && g >= 0 && g < galong) {
       const long long c = cb + (long long)g * stride;
       R p[5], T[4];
-      const R e = P.e[c];
+      const R e = P.e()[c];
 #pragma unroll
-      for (int l = 0; l < 4; l++) uu[l] = P.u[l][c];
+      for (int l = 0; l < 4; l++) uu[l] = P.u(l)[c];
 #pragma unroll
-      for (int l = 0; l < 4; l++) T[l] = set[l][c];
+      for (int l = 0; l < 4; l++) T[l] = P.S(use_b, l)[c];
 #pragma unroll
-      for (int l = 0; l < 5; l++) p[l] = set[4 + l][c];
+      for (int l = 0; l < 5; l++) p[l] = P.S(use_b, 4 + l)[c];
       cell_terms<R, DIR>(C, tau, e, uu, p, T, g >= lo && g < hi, F, V, spd);
     } else {
 #pragma unroll
@@ -166,7 +163,7 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
   const int a = tid & 31, c = tid >> 5;
   bool ok;
   const long long cb = cross_base(c, ok);
-  if (!ok) return;  // whole warp: c is uniform in the warp
+  if (!ok) return;  // whole warp: c is uniform in the warp (no barrier follows)
   const int g = a0 + a;
   const int s = c * LD + a;
   const bool stencil = a >= 2 && a <= NA - 3;  // a-2..a+2 inside the tile
@@ -184,7 +181,7 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
   }
   const bool out = a >= 3 && a < 3 + TL && g < hi;  // interior cell of this tile
   const long long cell = cb + (long long)g * stride;
-#pragma unroll 1
+#pragma unroll UNR
   for (int l = 0; l < 9; l++) {
     R fl = 0, fr = 0, vl = 0, vr = 0;
     if (stencil) {
@@ -197,7 +194,7 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
     const R Hl = shfl_up<R>(H, 1);                                // flux at the left face
     if (out) {
       const R r = -inv_h * (H - Hl);
-      P.res[l][cell] = first ? r : P.res[l][cell] + r;
+      P.res(l)[cell] = first ? r : P.res(l)[cell] + r;
     }
   }
   // velocity derivative along DIR: (L - R)/h of the same stencil (genWENOder)
@@ -207,35 +204,45 @@ __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
       const R* q = sm.u[l];
       R L, Rr;
       weno_lr<R>(q[s - 2], q[s - 1], q[s], q[s + 1], q[s + 2], L, Rr);
-      P.du[l * 3 + DIR][cell] = (L - Rr) / h;
+      P.du(l * 3 + DIR)[cell] = (L - Rr) / h;
     }
   }
 }
 
+template <class R, int DIR>
+__global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
+    k_dir(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, R h, int first) {
+  using S = DirSmem<R, DIR>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (*P.status) return;
+  dir_tile<R, DIR, S::NC>(C, P, use_b, tau, inv_h, h, first, blockIdx.x, blockIdx.y, blockIdx.z,
+                          *reinterpret_cast<S*>(smem_raw));
+}
+
 // Copy one cell's fields into a ghost cell (NEWEST5/boundary.h).
 template <class R>
-__device__ inline void ghost_put(const DevPtrs<R>& P, R* const* set, long long dst, R e, const R* u, const R* pu,
+__device__ inline void ghost_put(const DevPtrs<R>& P, int set_b, long long dst, R e, const R* u, const R* pu,
                                  const R* q9, bool skip_u12) {
-  P.e[dst] = e;
-  P.u[0][dst] = u[0];
-  if (!skip_u12) { P.u[1][dst] = u[1]; P.u[2][dst] = u[2]; }
-  P.u[3][dst] = u[3];
+  P.e()[dst] = e;
+  P.u(0)[dst] = u[0];
+  if (!skip_u12) { P.u(1)[dst] = u[1]; P.u(2)[dst] = u[2]; }
+  P.u(3)[dst] = u[3];
 #pragma unroll
-  for (int l = 0; l < 4; l++) P.pu[l][dst] = pu[l];
+  for (int l = 0; l < 4; l++) P.pu(l)[dst] = pu[l];
 #pragma unroll
-  for (int l = 0; l < 9; l++) set[l][dst] = q9[l];
+  for (int l = 0; l < 9; l++) P.S(set_b, l)[dst] = q9[l];
 }
 
 // One thread per interior cell: du_tau, sources, the RK combination, the
 // root-find and the ghost copy.  STAGE 1 reads set A and writes set B and
 // v1t; STAGE 2 reads A (its own cell), B and v1t and writes A.
+// One interior cell t (0 <= t < nx*ny*nz) of the update; returns the Newton
+// iterations and, at stage 2, the new temperature in GeV in *t_gev.
 template <class R, int STAGE>
-__global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
-  if (*P.status) return;
-  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long my_it = 0;
-  if (t < nint) {
+__device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R>& P, double tau_n, double ts,
+                                                long long t, double* t_gev) {
+  unsigned my_it = 0;
+  {
     const int i = C.il + (int)(t % C.nx);
     const int j = C.jl + (int)((t / C.nx) % C.ny);
     const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
@@ -244,24 +251,24 @@ __global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, doubl
     const R tau_s = (R)(STAGE == 1 ? tau_n : tau1);  // time of the sources
     const bool cart = C.cart;
 
-    R u[4], pu[4], p[5], e = P.e[c];
+    R u[4], pu[4], p[5], e = P.e()[c];
 #pragma unroll
-    for (int l = 0; l < 4; l++) { u[l] = P.u[l][c]; pu[l] = P.pu[l][c]; }
-    R* const* cur = STAGE == 1 ? P.A : P.B;
+    for (int l = 0; l < 4; l++) { u[l] = P.u(l)[c]; pu[l] = P.pu(l)[c]; }
+    const int cur_b = STAGE == 1 ? 0 : 1;  // conserved set read
     R Tc[4];
 #pragma unroll
-    for (int l = 0; l < 4; l++) Tc[l] = cur[l][c];
+    for (int l = 0; l < 4; l++) Tc[l] = P.S(cur_b, l)[c];
 #pragma unroll
-    for (int l = 0; l < 5; l++) p[l] = cur[4 + l][c];
+    for (int l = 0; l < 5; l++) p[l] = P.S(cur_b, 4 + l)[c];
 
     // velocity gradients
     R du[4][4];
 #pragma unroll
     for (int l = 0; l < 4; l++) {
       du[l][0] = (u[l] - pu[l]) / (R)ts;
-      du[l][1] = P.du[l * 3 + 0][c];
-      du[l][2] = P.du[l * 3 + 1][c];
-      du[l][3] = C.bi ? (R)0 : P.du[l * 3 + 2][c];
+      du[l][1] = P.du(l * 3 + 0)[c];
+      du[l][2] = P.du(l * 3 + 1)[c];
+      du[l][3] = C.bi ? (R)0 : P.du(l * 3 + 2)[c];
     }
     // sources (NEWEST5/Source.h:165-191 geometric, 311-433 shear)
     R src[9];
@@ -288,22 +295,22 @@ __global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, doubl
     }
     // RK combination (NEWEST5/time.h:2-140)
     R Vn[9];
-    R* const* out = STAGE == 1 ? P.B : P.A;
+    const int out_b = STAGE == 1 ? 1 : 0;  // conserved set written
     if (STAGE == 1) {
 #pragma unroll
       for (int l = 0; l < 9; l++) {
-        const R L0 = P.res[l][c] + src[l];
+        const R L0 = P.res(l)[c] + src[l];
         const R v0 = l < 4 ? (cart ? Tc[l] : (R)tau_n * Tc[l]) : p[l - 4];
         Vn[l] = v0 + (R)ts * L0;
       }
 #pragma unroll
-      for (int l = 0; l < 4; l++) P.v1t[l][c] = Vn[l];
+      for (int l = 0; l < 4; l++) P.v1t(l)[c] = Vn[l];
     } else {
 #pragma unroll
       for (int l = 0; l < 9; l++) {
-        const R L1 = P.res[l][c] + src[l];
-        const R v0 = l < 4 ? (cart ? P.A[l][c] : (R)tau_n * P.A[l][c]) : P.A[l][c];
-        const R v1 = l < 4 ? P.v1t[l][c] : p[l - 4];
+        const R L1 = P.res(l)[c] + src[l];
+        const R v0 = l < 4 ? (cart ? P.A(l)[c] : (R)tau_n * P.A(l)[c]) : P.A(l)[c];
+        const R v1 = l < 4 ? P.v1t(l)[c] : p[l - 4];
         Vn[l] = (R)0.5 * v0 + (R)0.5 * v1 + (R)0.5 * (R)ts * L1;
       }
     }
@@ -313,11 +320,11 @@ __global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, doubl
 #pragma unroll
     for (int l = 0; l < 5; l++) q9[4 + l] = Vn[4 + l];
 #pragma unroll
-    for (int l = 0; l < 9; l++) out[l][c] = q9[l];
+    for (int l = 0; l < 9; l++) P.S(out_b, l)[c] = q9[l];
     // previous velocity (NEWEST5/time.h:166, stage 1 only)
     if (STAGE == 1) {
 #pragma unroll
-      for (int l = 0; l < 4; l++) { pu[l] = u[l]; P.pu[l][c] = u[l]; }
+      for (int l = 0; l < 4; l++) { pu[l] = u[l]; P.pu(l)[c] = u[l]; }
     }
     // root-find (FP64) with the current primitives as the guess
     double Tt[4], pd[5], x[4] = {(double)e, (double)u[1], (double)u[2], (double)u[3]};
@@ -329,7 +336,7 @@ __global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, doubl
     if (it < 0) {
       atomicOr(P.status, ST_ROOT);
     } else {
-      my_it = (unsigned long long)it;
+      my_it = (unsigned)it;
       const double tt = cart ? 1.0 : tau1;
       const double u0 = sqrt(1 + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] * tt * tt);
       const double vx = x[1] / u0, vy = x[2] / u0, ve = x[3] / u0;
@@ -337,37 +344,48 @@ __global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, doubl
       if (x[0] <= 0) atomicOr(P.status, ST_NEGE);
       e = (R)x[0];
       u[0] = (R)u0; u[1] = (R)x[1]; u[2] = (R)x[2]; u[3] = (R)x[3];
-      P.e[c] = e;
+      P.e()[c] = e;
 #pragma unroll
-      for (int l = 0; l < 4; l++) P.u[l][c] = u[l];
+      for (int l = 0; l < 4; l++) P.u(l)[c] = u[l];
     }
     // ghost copy of boundary cells: faces only, corners untouched
     // (NEWEST5/boundary.h:1-276); Gubser test mirrors u^x,u^y
     const bool mir = C.mirror;
     if (i == C.il)
-      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, m, j, k), e, u, pu, q9, mir);
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out_b, cix(C, m, j, k), e, u, pu, q9, mir);
     if (i == C.ir - 1)
-      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, C.ir + m, j, k), e, u, pu, q9, mir);
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out_b, cix(C, C.ir + m, j, k), e, u, pu, q9, mir);
     if (j == C.jl)
-      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, m, k), e, u, pu, q9, mir);
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out_b, cix(C, i, m, k), e, u, pu, q9, mir);
     if (j == C.jr - 1)
-      for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, C.jr + m, k), e, u, pu, q9, mir);
+      for (int m = 0; m < NG; m++) ghost_put<R>(P, out_b, cix(C, i, C.jr + m, k), e, u, pu, q9, mir);
     if (!C.bi) {
       if (k == C.kl)
-        for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, j, m), e, u, pu, q9, false);
+        for (int m = 0; m < NG; m++) ghost_put<R>(P, out_b, cix(C, i, j, m), e, u, pu, q9, false);
       if (k == C.kr - 1)
-        for (int m = 0; m < NG; m++) ghost_put<R>(P, out, cix(C, i, j, C.kr + m), e, u, pu, q9, false);
+        for (int m = 0; m < NG; m++) ghost_put<R>(P, out_b, cix(C, i, j, C.kr + m), e, u, pu, q9, false);
     }
     if (mir) {
       // ghost m <- cell il + 2 - m on the left, ghost ir + m <- ir - 1 - m on the right
       const int dl = i - C.il, dr = C.ir - 1 - i;
-      if (dl < NG) { long long g = cix(C, C.il - 1 - dl, j, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
-      if (dr < NG) { long long g = cix(C, C.ir + dr, j, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
+      if (dl < NG) { long long g = cix(C, C.il - 1 - dl, j, k); P.u(1)[g] = u[1]; P.u(2)[g] = u[2]; }
+      if (dr < NG) { long long g = cix(C, C.ir + dr, j, k); P.u(1)[g] = u[1]; P.u(2)[g] = u[2]; }
       const int el = j - C.jl, er = C.jr - 1 - j;
-      if (el < NG) { long long g = cix(C, i, C.jl - 1 - el, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
-      if (er < NG) { long long g = cix(C, i, C.jr + er, k); P.u[1][g] = u[1]; P.u[2][g] = u[2]; }
+      if (el < NG) { long long g = cix(C, i, C.jl - 1 - el, k); P.u(1)[g] = u[1]; P.u(2)[g] = u[2]; }
+      if (er < NG) { long long g = cix(C, i, C.jr + er, k); P.u(1)[g] = u[1]; P.u(2)[g] = u[2]; }
     }
+    if (STAGE == 2 && t_gev) *t_gev = C.hbarc * (double)eos_T<R>(C, e);
   }
+  return my_it;
+}
+
+// one thread per interior cell
+template <class R, int STAGE>
+__global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
+  if (*P.status) return;
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long my_it = t < nint ? update_cell<R, STAGE>(C, P, tau_n, ts, t, nullptr) : 0u;
   // one atomic per warp for the iteration counter
   for (int o = 16; o > 0; o >>= 1) my_it += __shfl_down_sync(0xffffffffu, my_it, o);
   if ((threadIdx.x & 31) == 0 && my_it) atomicAdd(P.iters, my_it);

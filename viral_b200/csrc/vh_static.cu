@@ -138,18 +138,9 @@ extern "C" int vh_step_static(const vh_config* cfg, double* state, const double*
 
   DevPtrs<double> P{};
   const long long n = C.n;
-  auto f = [&](int q) { return state + (long long)q * n; };
-  P.e = f(0);
-  for (int l = 0; l < 4; l++) P.u[l] = f(1 + l);
-  for (int l = 0; l < 4; l++) P.A[l] = f(10 + l);
-  for (int l = 0; l < 5; l++) P.A[4 + l] = f(5 + l);
-  for (int l = 0; l < 4; l++) P.pu[l] = f(14 + l);
-  double* work = scratch + kHeaderDoubles;
-  auto w = [&](int q) { return work + (long long)q * n; };
-  for (int l = 0; l < 9; l++) P.B[l] = w(l);
-  for (int l = 0; l < 4; l++) P.v1t[l] = w(9 + l);
-  for (int l = 0; l < 9; l++) P.res[l] = w(13 + l);
-  for (int l = 0; l < 12; l++) P.du[l] = w(22 + l);
+  P.base0 = state;                           // the caller's 18 fields
+  P.base1 = scratch + kHeaderDoubles;        // B, v1t, res, du in the static array
+  P.stride = n;
   P.status = reinterpret_cast<unsigned int*>(scratch);
   P.iters = reinterpret_cast<unsigned long long*>(scratch + 1);
   if (cudaMemsetAsync(scratch, 0, kHeaderDoubles * sizeof(double), s) != cudaSuccess) return VH_E_CUDA;
