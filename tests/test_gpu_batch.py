@@ -42,11 +42,14 @@ def test_batch_matches_single_events(precision, variant):
         tau, nst, st = B.events()
         assert np.all(st == EVENT_RUNNING) and np.all(nst == steps)
         assert np.allclose(tau, cfg.tau0 + steps * cfg.dtau)
+        # FP64: identical up to rounding; mixed: the same FP32 source compiled
+        # into another kernel may fuse multiply-adds differently (ulp level)
+        tol = 1e-13 if precision == A.PREC_FP64 else 1e-5
         for ev, (side, b) in enumerate(zip(SIDES, BIMP)):
             ref = single_event(cfg, side, b, ev, steps)
             got = B.event_state(ev)
             for q in range(14):
-                assert rel_err(got[q], ref[q]) <= 1e-13, (ev, q)
+                assert rel_err(got[q], ref[q]) <= tol, (ev, q)
 
 
 def test_freeze_out_per_event():
