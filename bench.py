@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--tau-end", type=float, default=10.0)
     p.add_argument("--ensemble", type=int, default=0,
                    help="events/s of a batched ensemble of this many boost-invariant events")
+    p.add_argument("--ensemble-precision", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--loop-per-side", type=int, default=2,
                    help="events per grid side for the looped single-event FP64 baseline")
     return p.parse_args()
@@ -389,7 +390,8 @@ def ensemble(args):
     bimp = rng.uniform(0.0, 12.0, size=n)
     tau0, dtau, tau_max, t_fo = 0.6, 0.02, 15.0, 0.15
     max_steps = C.steps_between(tau0, tau_max, dtau)
-    cfg = C.glauber_config(nx=8, ny=8, boost_invariant=True, precision=A.PREC_MIXED)
+    prec = A.PREC_MIXED if args.ensemble_precision == "mixed" else A.PREC_FP64
+    cfg = C.glauber_config(nx=8, ny=8, boost_invariant=True, precision=prec)
     t_init = time.perf_counter()
     B = Batch(cfg, sides, tau0=tau0, dtau=dtau, tau_max=tau_max, t_freeze_gev=t_fo)
     npart = B.init_glauber(seeds=np.arange(n), bimp=bimp)
@@ -406,7 +408,7 @@ def ensemble(args):
     batch_cells_s = float(np.sum(cells * nst)) / sec
     # looped single-event FP64 baseline on a stratified sample
     per_side = {}
-    for side in sides_all:
+    for side in (sides_all if args.loop_per_side > 0 else []):
         ts = []
         for q in range(args.loop_per_side):
             ev = int(np.where(sides == side)[0][q]) if np.sum(sides == side) > q else q
@@ -423,7 +425,7 @@ def ensemble(args):
             ts.append(time.perf_counter() - t0)
             H.close()
         per_side[int(side)] = float(np.mean(ts))
-    loop_seconds = float(sum(per_side[int(s_)] for s_ in sides))
+    loop_seconds = float(sum(per_side[int(s_)] for s_ in sides)) if per_side else float("nan")
     out = {"metric": "events/s", "value": batch_events_s, "unit": "events/s", "n_events": n,
            "batch_seconds": sec, "cell_updates_per_s": batch_cells_s, "graph": graph, "tuning": tuning,
            "autotune_ms_per_step": tune_ms, "init_seconds": t_init,
@@ -431,12 +433,14 @@ def ensemble(args):
            "stopped": {"frozen_out": int(np.sum(st == 1)), "tau_max": int(np.sum(st == 2)),
                        "failed": int(np.sum(st == 3)), "running": int(np.sum(st == 0))},
            "npart_mean": float(np.mean(npart)),
+           "failed_events": [{"event": int(e), "side": int(sides[e]), "b": round(float(bimp[e]), 3),
+                              "steps": int(nst[e])} for e in np.where(st == 3)[0][:64]],
            "loop_fp64": {"events_per_s": n / loop_seconds, "seconds_per_event_by_side": per_side,
                          "sample": f"{args.loop_per_side} events per side, extrapolated by the side counts"},
            "speedup_vs_loop_fp64": loop_seconds / sec, "clocks": clk.summary(),
            "config": {"workload": "glauber ensemble", "sides": [64, 96, 128, 160, 200], "dx_fm": 0.1,
                       "b_fm": [0, 12], "dtau_fm": dtau, "tau0_fm": tau0, "tau_max_fm": tau_max,
-                      "t_freeze_gev": t_fo, "precision": "mixed (batch) / fp64 (loop)"}}
+                      "t_freeze_gev": t_fo, "precision": f"{args.ensemble_precision} (batch) / fp64 (loop)"}}
     print(json.dumps(out), flush=True)
 
 

@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvh.so")
+CHECK_LIB = os.path.join(HERE, "libvh_check.so")
 
 SOURCES = ["vh_api.cu", "vh_static.cu", "vh_batch.cu", "vh_inputs.cpp", "vh_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -26,6 +27,22 @@ def nvcc() -> str:
         if cand and os.path.exists(cand):
             return cand
     raise RuntimeError("nvcc not found")
+
+
+def build_check(verbose: bool = False) -> str:
+    """libvh_check.so: host entry points onto the device arithmetic (tests)."""
+    src = os.path.join(CSRC, "vh_check.cu")
+    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    if os.path.exists(CHECK_LIB) and all(os.path.getmtime(d) <= os.path.getmtime(CHECK_LIB) for d in deps):
+        return CHECK_LIB
+    cmd = [nvcc(), *ARCH, "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"),
+           "-I", CSRC, "-o", CHECK_LIB, src]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed building libvh_check.so")
+    return CHECK_LIB
 
 
 def build(verbose: bool = False, extra: list[str] | None = None) -> str:
@@ -51,4 +68,5 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
 
 if __name__ == "__main__":
     build(verbose="--verbose" in sys.argv)
+    build_check(verbose="--verbose" in sys.argv)
     print(LIB)

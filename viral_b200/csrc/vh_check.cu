@@ -1,0 +1,98 @@
+// Host-side entry points onto the device arithmetic of the step and of its
+// adjoint (the same __host__ __device__ functions the kernels use), for the
+// CPU tests: finite-difference checks of every local adjoint.  Test hooks
+// only: not part of the C ABI in include/vh.h, built as libvh_check.so.
+#include <cmath>
+#include <vector>
+
+#include "vh.h"
+#include "vh_adjoint.cuh"
+
+using namespace vh;
+
+namespace {
+struct HostCfg {
+  DevCfg C{};
+  std::vector<double> td;
+  std::vector<float> tf;
+};
+HostCfg make_cfg(const vh_config* c) {
+  HostCfg h;
+  DevCfg& C = h.C;
+  C.cart = c->coords == VH_COORD_CARTESIAN;
+  C.bi = c->boost_invariant;
+  C.recon = c->recon;
+  C.eos_kind = c->eos_kind;
+  C.eos_a = c->eos_a;
+  C.etas0 = c->etas0; C.etas1 = c->etas1; C.etas_tc = c->etas_tc; C.hbarc = c->hbarc;
+  C.taupi_kind = c->taupi_kind;
+  C.dx = c->dx; C.dy = c->dy; C.dz = c->dz;
+  if (c->eos_kind == VH_EOS_TABLE) {
+    const int n = c->eos_n;
+    h.td.resize(4 * (size_t)n);
+    for (int i = 0; i < n; i++) {
+      h.td[i] = c->eos_e[i]; h.td[n + i] = c->eos_p[i]; h.td[2 * n + i] = c->eos_cs2[i]; h.td[3 * n + i] = c->eos_t[i];
+    }
+    h.tf.assign(h.td.begin(), h.td.end());
+    C.eos_n = n;
+    C.eos_l0 = std::log(c->eos_e[0]);
+    C.eos_idl = (n - 1) / (std::log(c->eos_e[n - 1]) - C.eos_l0);
+    C.eos_d = h.td.data();
+    C.eos_f = h.tf.data();
+  }
+  return h;
+}
+}  // namespace
+
+extern "C" {
+
+void vhc_weno_lr(const double* q, double* L, double* R) { weno_lr<double>(q[0], q[1], q[2], q[3], q[4], *L, *R); }
+void vhc_weno_lr_vjp(const double* q, double Lb, double Rb, double* qb) { weno_lr_vjp<double>(q, Lb, Rb, qb); }
+
+void vhc_cell_q(const vh_config* c, int dir, double tau, const double* x, int interior, double* q) {
+  HostCfg h = make_cfg(c);
+  if (dir == 0) cell_q<double, 0>(h.C, tau, x, interior, q);
+  else cell_q<double, 1>(h.C, tau, x, interior, q);
+}
+void vhc_cell_q_vjp(const vh_config* c, int dir, double tau, const double* x, int interior, const double* qb,
+                    double* xb) {
+  HostCfg h = make_cfg(c);
+  if (dir == 0) cell_q_vjp<double, 0>(h.C, tau, x, interior, qb, xb);
+  else cell_q_vjp<double, 1>(h.C, tau, x, interior, qb, xb);
+}
+void vhc_src2d(const vh_config* c, double tau, double e, const double* u3, const double* p3, const double* du9,
+               double* out4) {
+  HostCfg h = make_cfg(c);
+  src2d<double>(h.C, tau, e, u3, p3, du9, out4);
+}
+void vhc_src2d_vjp(const vh_config* c, double tau, double e, const double* u3, const double* p3, const double* du9,
+                   const double* ob4, double* eb, double* ub3, double* pb3, double* dub9, double* cb2) {
+  HostCfg h = make_cfg(c);
+  src2d_vjp<double>(h.C, tau, e, u3, p3, du9, ob4, *eb, ub3, pb3, dub9, cb2);
+}
+int vhc_con2prim(const vh_config* c, const double* T3, const double* p3, double tau, double* x3) {
+  HostCfg h = make_cfg(c);
+  const double T[4] = {T3[0], T3[1], T3[2], 0.0}, p[5] = {p3[0], p3[1], p3[2], 0.0, 0.0};
+  double x[4] = {x3[0], x3[1], x3[2], 0.0};
+  const int it = con2prim(h.C, T, p, tau, x);
+  x3[0] = x[0]; x3[1] = x[1]; x3[2] = x[2];
+  return it;
+}
+int vhc_c2p_ift_vjp(const vh_config* c, const double* T3, const double* p3, double tau, const double* x3,
+                    const double* xb3, double* Tb3, double* pb3) {
+  HostCfg h = make_cfg(c);
+  return c2p_ift_vjp(h.C, T3, p3, tau, x3, xb3, Tb3, pb3) ? 0 : 1;
+}
+void vhc_obs_cell(const vh_config* c, double e, double u1, double u2, double p1, double p2, double* nd) {
+  HostCfg h = make_cfg(c);
+  obs_cell<double>(h.C, e, u1, u2, p1, p2, nd[0], nd[1]);
+}
+void vhc_obs_cell_vjp(const vh_config* c, double e, double u1, double u2, double N, double D, double* g5) {
+  HostCfg h = make_cfg(c);
+  obs_cell_vjp<double>(h.C, e, u1, u2, N, D, g5[0], g5[1], g5[2], g5[3], g5[4]);
+}
+void vhc_eos_d(const vh_config* c, double e, double* out4) {
+  HostCfg h = make_cfg(c);
+  eos_d<double>(h.C, e, out4[0], out4[1], out4[2], out4[3]);
+}
+}

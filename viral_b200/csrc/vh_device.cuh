@@ -7,6 +7,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// host+device math: the same arithmetic also compiles for host-side checks
+#define VH_HD __host__ __device__
+
 namespace vh {
 
 constexpr int NG = 3;  // ghost layers (NEWEST5/maindef.h:369-371 BORDER)
@@ -65,32 +68,38 @@ struct DevPtrs {
 
 enum : unsigned { ST_ROOT = 1u, ST_CAUSAL = 2u, ST_NEGE = 4u };
 
-__host__ __device__ inline long long cix(const DevCfg& C, int i, int j, int k) {
+__host__ VH_HD inline long long cix(const DevCfg& C, int i, int j, int k) {
   return ((long long)k * C.gy + j) * C.gx + i;
 }
 
 // ------------------------------------------------------------------ EOS
 
 template <class R>
-__device__ inline const R* eos_tab(const DevCfg& C);
+VH_HD inline const R* eos_tab(const DevCfg& C);
 template <>
-__device__ inline const double* eos_tab<double>(const DevCfg& C) { return C.eos_d; }
+VH_HD inline const double* eos_tab<double>(const DevCfg& C) { return C.eos_d; }
 template <>
-__device__ inline const float* eos_tab<float>(const DevCfg& C) { return C.eos_f; }
+VH_HD inline const float* eos_tab<float>(const DevCfg& C) { return C.eos_f; }
 
-__device__ inline double d_log(double x) { return log(x); }
-__device__ inline float d_log(float x) { return __logf(x); }
-__device__ inline double d_sqrt(double x) { return sqrt(x); }
-__device__ inline float d_sqrt(float x) { return sqrtf(x); }
+VH_HD inline double d_log(double x) { return log(x); }
+VH_HD inline float d_log(float x) {
+#ifdef __CUDA_ARCH__
+  return __logf(x);
+#else
+  return logf(x);
+#endif
+}
+VH_HD inline double d_sqrt(double x) { return sqrt(x); }
+VH_HD inline float d_sqrt(float x) { return sqrtf(x); }
 
 // Row i with e_i <= e < e_{i+1}: a log-based guess corrected against the
 // nodes, so the bracket is exact whatever the rounding of log.
 template <class R>
-__device__ inline int eos_row(const DevCfg& C, const R* t, R e) {
+VH_HD inline int eos_row(const DevCfg& C, const R* t, R e) {
   const int n = C.eos_n;
   // a single-precision log is enough for the guess: the loops below make
   // the bracket exact
-  int i = (int)((__logf((float)e) - (float)C.eos_l0) * (float)C.eos_idl);
+  int i = (int)((d_log((float)e) - (float)C.eos_l0) * (float)C.eos_idl);
   i = i < 0 ? 0 : (i > n - 2 ? n - 2 : i);
   while (i > 0 && e < t[i]) i--;
   while (i < n - 2 && e >= t[i + 1]) i++;
@@ -101,7 +110,7 @@ __device__ inline int eos_row(const DevCfg& C, const R* t, R e) {
 // first row P = cs2_0 e and T ~ e^(1/4); above the last row P grows with the
 // last cs2 and T ~ e^(1/4).
 template <class R>
-__device__ inline void eos_table(const DevCfg& C, R e, R* P, R* cs2, R* T) {
+VH_HD inline void eos_table(const DevCfg& C, R e, R* P, R* cs2, R* T) {
   const R* t = eos_tab<R>(C);
   const int n = C.eos_n;
   const R* te = t;
@@ -129,7 +138,7 @@ __device__ inline void eos_table(const DevCfg& C, R e, R* P, R* cs2, R* T) {
 
 // P(e) (NEWEST5/maindef.h:332 EOS)
 template <class R>
-__device__ inline R eos_P(const DevCfg& C, R e) {
+VH_HD inline R eos_P(const DevCfg& C, R e) {
   if (C.eos_kind == 0) return e / (R)3;
   R P, c, T;
   eos_table<R>(C, e, &P, &c, &T);
@@ -137,17 +146,17 @@ __device__ inline R eos_P(const DevCfg& C, R e) {
 }
 // dP/de (NEWEST5/maindef.h:333 DPDE)
 template <class R>
-__device__ inline R eos_cs2(const DevCfg& C, R e) {
+VH_HD inline R eos_cs2(const DevCfg& C, R e) {
   if (C.eos_kind == 0) return (R)1 / (R)3;
   R P, c, T;
   eos_table<R>(C, e, &P, &c, &T);
   return c;
 }
-__device__ inline double conf_T(double x) { return pow(x, 0.25); }
-__device__ inline float conf_T(float x) { return sqrtf(sqrtf(x)); }
+VH_HD inline double conf_T(double x) { return pow(x, 0.25); }
+VH_HD inline float conf_T(float x) { return sqrtf(sqrtf(x)); }
 // T(e) (NEWEST5/maindef.h:335 FT)
 template <class R>
-__device__ inline R eos_T(const DevCfg& C, R e) {
+VH_HD inline R eos_T(const DevCfg& C, R e) {
   if (C.eos_kind == 0) return conf_T(e / (R)C.eos_a);
   R P, c, T;
   eos_table<R>(C, e, &P, &c, &T);
@@ -155,7 +164,7 @@ __device__ inline R eos_T(const DevCfg& C, R e) {
 }
 // eta = (eta/s)(T) s with s = (e+P)/T, and tau_pi (NEWEST5/maindef.h:336-339)
 template <class R>
-__device__ inline void transport(const DevCfg& C, R e, R P, R* eta, R* taupi) {
+VH_HD inline void transport(const DevCfg& C, R e, R P, R* eta, R* taupi) {
   R T = eos_T<R>(C, e);
   R s = (e + P) / T;
   R tg = T * (R)C.hbarc - (R)C.etas_tc;
@@ -173,7 +182,7 @@ struct PiDep {
   R tt, tx, ty, te, ee;
 };
 template <class R>
-__device__ inline PiDep<R> pi_dep(R u0, R u1, R u2, R u3, const R* p, R t2) {
+VH_HD inline PiDep<R> pi_dep(R u0, R u1, R u2, R u3, const R* p, R t2) {
   PiDep<R> d;
   const R iD = (R)1 / (u0 * u0 - t2 * u3 * u3);
   const R iu0 = (R)1 / u0;
@@ -190,7 +199,7 @@ __device__ inline PiDep<R> pi_dep(R u0, R u1, R u2, R u3, const R* p, R t2) {
 // Jiang-Shu WENO5 with p = 2, eps = 1e-6 and linear weights (0.3,0.6,0.1)
 // (NEWEST5/utils.h:57-160).  Evaluation order follows the reference.
 template <class R>
-__device__ inline void weno_beta(R qm2, R qm1, R qc, R qp1, R qp2, R& b0, R& b1, R& b2) {
+VH_HD inline void weno_beta(R qm2, R qm1, R qc, R qp1, R qp2, R& b0, R& b1, R& b2) {
   const R c13 = (R)(13. / 12.);
   R a = qc - (R)2 * qp1 + qp2, c = (R)3 * qc - (R)4 * qp1 + qp2;
   b0 = c13 * (a * a) + (R)0.25 * (c * c);
@@ -207,7 +216,7 @@ __device__ inline void weno_beta(R qm2, R qm1, R qc, R qp1, R qp2, R& b0, R& b1,
 // WENO5 (NEWEST5/utils.h:102-160) up to rounding.
 // value at face i+1/2 from the stencil centred on i (genWENOL)
 template <class R>
-__device__ inline R weno_left(R qm2, R qm1, R qc, R qp1, R qp2) {
+VH_HD inline R weno_left(R qm2, R qm1, R qc, R qp1, R qp2) {
   R b0, b1, b2;
   weno_beta<R>(qm2, qm1, qc, qp1, qp2, b0, b1, b2);
   const R eps = (R)1e-6;
@@ -221,7 +230,7 @@ __device__ inline R weno_left(R qm2, R qm1, R qc, R qp1, R qp2) {
 }
 // value at face i-1/2 from the stencil centred on i (genWENOR)
 template <class R>
-__device__ inline R weno_right(R qm2, R qm1, R qc, R qp1, R qp2) {
+VH_HD inline R weno_right(R qm2, R qm1, R qc, R qp1, R qp2) {
   R b0, b1, b2;
   weno_beta<R>(qm2, qm1, qc, qp1, qp2, b0, b1, b2);
   const R eps = (R)1e-6;
@@ -236,7 +245,7 @@ __device__ inline R weno_right(R qm2, R qm1, R qc, R qp1, R qp2) {
 // Both face values of one stencil at once: L at i+1/2 (genWENOL) and R at
 // i-1/2 (genWENOR) share the smoothness indicators and their products.
 template <class R>
-__device__ inline void weno_lr(R qm2, R qm1, R qc, R qp1, R qp2, R& L, R& Rr) {
+VH_HD inline void weno_lr(R qm2, R qm1, R qc, R qp1, R qp2, R& L, R& Rr) {
   R b0, b1, b2;
   weno_beta<R>(qm2, qm1, qc, qp1, qp2, b0, b1, b2);
   const R eps = (R)1e-6;
@@ -259,14 +268,19 @@ __device__ inline void weno_lr(R qm2, R qm1, R qc, R qp1, R qp2, R& L, R& Rr) {
     L = numl * denr * inv;
     Rr = numr * denl * inv;
   } else {
+#ifdef __CUDA_ARCH__
     L = __fdividef((float)numl, (float)denl);
     Rr = __fdividef((float)numr, (float)denr);
+#else
+    L = (float)numl / (float)denl;
+    Rr = (float)numr / (float)denr;
+#endif
   }
 }
 
 // generalized minmod (theta) piecewise-linear face values (utils.h:33-55)
 template <class R>
-__device__ inline R mm3(R a, R b, R c) {
+VH_HD inline R mm3(R a, R b, R c) {
   if (a * b > (R)0 && b * c > (R)0) {
     R m = fmin(fmin(fabs(a), fabs(b)), fabs(c));
     return a < (R)0 ? -m : m;
@@ -274,11 +288,11 @@ __device__ inline R mm3(R a, R b, R c) {
   return (R)0;
 }
 template <class R>
-__device__ inline R mm_left(R th, R qm1, R qc, R qp1) {
+VH_HD inline R mm_left(R th, R qm1, R qc, R qp1) {
   return qc + (R)0.5 * mm3<R>(th * (qc - qm1), (R)0.5 * (qp1 - qm1), th * (qp1 - qc));
 }
 template <class R>
-__device__ inline R mm_right(R th, R qm1, R qc, R qp1) {
+VH_HD inline R mm_right(R th, R qm1, R qc, R qp1) {
   return qc - (R)0.5 * mm3<R>(th * (qc - qm1), (R)0.5 * (qp1 - qm1), th * (qp1 - qc));
 }
 
@@ -293,7 +307,7 @@ __device__ inline R mm_right(R th, R qm1, R qc, R qp1) {
 // a_b = u^a nabla_a u_b (NEWEST5/Source.h:317-370; Cartesian: no
 // Christoffels, TXYZ5/Source.h:291-335).  du[l][m] = d_m u^l.
 template <class R>
-__device__ inline void is_kinematics(int cart, R tau, const R* u, const R du[4][4], R sig[4][4], R& theta, R acc[4]) {
+VH_HD inline void is_kinematics(int cart, R tau, const R* u, const R du[4][4], R sig[4][4], R& theta, R acc[4]) {
   const R t2 = cart ? (R)1 : tau * tau;
   const R g[4] = {(R)1, (R)-1, (R)-1, -t2};
   const R gi[4] = {(R)1, (R)-1, (R)-1, cart ? (R)-1 : (R)-1 / t2};
@@ -360,7 +374,7 @@ __device__ inline void is_kinematics(int cart, R tau, const R* u, const R du[4][
 }
 
 template <class R>
-__device__ inline void is_source(const DevCfg& C, R tau, R e, const R* u, const R* p, const R du[4][4], R out[5]) {
+VH_HD inline void is_source(const DevCfg& C, R tau, R e, const R* u, const R* p, const R du[4][4], R out[5]) {
   const int cart = C.cart;
   const R t2 = cart ? (R)1 : tau * tau;
   R P = eos_P<R>(C, e), eta, tp;
@@ -396,7 +410,7 @@ __device__ inline void is_source(const DevCfg& C, R tau, R e, const R* u, const 
 
 // P and dP/de together (one table lookup)
 template <class R>
-__device__ inline void eos_P_cs2(const DevCfg& C, R e, R& P, R& cs2) {
+VH_HD inline void eos_P_cs2(const DevCfg& C, R e, R& P, R& cs2) {
   if (C.eos_kind == 0) { P = e / (R)3; cs2 = (R)1 / (R)3; return; }
   R T;
   eos_table<R>(C, e, &P, &cs2, &T);
@@ -405,7 +419,7 @@ __device__ inline void eos_P_cs2(const DevCfg& C, R e, R& P, R& cs2) {
 // -------------------------------------------------------------- con2prim
 // Residuals of T^{tau nu} u_nu = e u^tau for x = (e, u^x, u^y, u^eta) and
 // their Jacobian (NEWEST5/multiroot.h:202-319), in double.
-__device__ inline void c2p_fj(const DevCfg& C, const double* Tt, const double* p, double t2, const double* x,
+VH_HD inline void c2p_fj(const DevCfg& C, const double* Tt, const double* p, double t2, const double* x,
                               double* y, double J[4][4], bool jac) {
   double e = x[0];
   const double u1 = x[1], u2 = x[2], u3 = x[3];
@@ -444,7 +458,7 @@ __device__ inline void c2p_fj(const DevCfg& C, const double* Tt, const double* p
 // Gaussian elimination with partial pivoting on a 4x4 system (in place).
 // Row swaps are written as compile-time-indexed selects so that the matrix
 // stays in registers.
-__device__ inline bool solve4(double A[4][4], double b[4]) {
+VH_HD inline bool solve4(double A[4][4], double b[4]) {
 #pragma unroll
   for (int c = 0; c < 4; c++) {
     int p = c;
@@ -490,7 +504,7 @@ __device__ inline bool solve4(double A[4][4], double b[4]) {
 // result in single precision, stops at rtol = 1e-10.  The Jacobian is
 // formed together with the residual at every trial point, so an accepted
 // full step (the common case) costs one evaluation.
-__device__ inline int con2prim(const DevCfg& C, const double* Tt, const double* p, double tau, double* x,
+VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, double tau, double* x,
                                double rtol = 1e-16) {
   const double t2 = C.cart ? 1.0 : tau * tau;
   double y[4], J[4][4];
