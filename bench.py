@@ -54,6 +54,9 @@ def parse():
     p.add_argument("--ensemble-precision", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--loop-per-side", type=int, default=2,
                    help="events per grid side for the looped single-event FP64 baseline")
+    p.add_argument("--adjoint", action="store_true",
+                   help="adjoint/forward device-time ratio of the eps_p gradient (128x128 Glauber, 330 steps)")
+    p.add_argument("--checkpoint-every", type=int, default=25)
     return p.parse_args()
 
 
@@ -444,6 +447,105 @@ def ensemble(args):
     print(json.dumps(out), flush=True)
 
 
+def adjoint_ratio(args):
+    """Discrete adjoint of the momentum anisotropy eps_p at tau = 7.2 fm/c of
+    the boost-invariant 128x128 MC-Glauber event (dx = 0.1 fm, b = 7 fm, seed
+    0, floor 0.5 GeV/fm^3; 330 steps of 0.02 fm/c from 0.6 fm/c; eta/s =
+    0.08 + 1.0 GeV^-1 max(T - 0.154 GeV, 0)), checkpoints every 25 steps, in
+    FP64 and mixed precision.  The forward is vh_step(330) + vh_eps_p; the
+    adjoint is one vh_adjoint_eps_p call (forward with checkpoints, segment
+    recomputation, reverse steps, gradient export).  Device time from CUDA
+    events on the handle's stream, median of --steps repetitions after
+    --warmup.  The FP64 gradient is also checked against central differences
+    of the FP64 forward (h = 1e-6) along 4 seeded unit directions in e0 and
+    relative perturbations of (c0, c1)."""
+    import numpy as np
+    import torch
+    from viral_b200 import _abi as A
+    from viral_b200 import configs as C
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    nsteps = C.ADJOINT_STEPS
+    res = {}
+    with ClockSampler(dev) as clk:
+        for name, prec in (("fp64", A.PREC_FP64), ("mixed", A.PREC_MIXED)):
+            cfg = C.adjoint_config(128, prec)
+            inp = C.adjoint_inputs(cfg)
+            H = C.make_hydro(cfg, inp)
+            A.check(A.lib().vh_set_stream(H.h, ctypes_void_p(stream.cuda_stream)), H.h)
+
+            def reinit():
+                H.init_profile(inp["tau"], inp["e"], inp["ux"], inp["uy"], inp["ueta"], inp["prevu"],
+                               inp["pi_mode"])
+                torch.cuda.synchronize()
+
+            def timed(fn):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                out = fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1), out
+
+            fwd, adj = [], []
+            for rep in range(args.warmup + args.steps):
+                reinit()
+                tf, eps_f = timed(lambda: (H.step(nsteps), H.eps_p())[1])
+                reinit()
+                ta, out = timed(lambda: H.adjoint_eps_p(nsteps, args.checkpoint_every, want_state=False))
+                if rep >= args.warmup:
+                    fwd.append(tf)
+                    adj.append(ta)
+            phases = H.adjoint_phase_times()
+            res[name] = {"forward_ms": statistics.median(fwd), "adjoint_ms": statistics.median(adj),
+                         "ratio": statistics.median(adj) / statistics.median(fwd), "eps_p": out[0],
+                         "adjoint_phases_ms": {"forward_with_checkpoints": phases[0], "recompute_with_records": phases[1],
+                                               "reverse": phases[2], "rest": phases[3]},
+                         "eps_p_forward": eps_f, "grad_etas": out[3].tolist(),
+                         "grad_e0_norm": float(np.linalg.norm(out[2]))}
+            if name == "fp64":
+                ge, gc = out[2], out[3]
+
+                def eps_of(e0, c):
+                    cfg2 = C.adjoint_config(128, prec, c[0], c[1])
+                    with C.make_hydro(cfg2, dict(inp, e=e0)) as H2:
+                        H2.step(nsteps)
+                        return H2.eps_p()
+
+                g = 134
+                m = np.zeros((g, g), bool)
+                m[3:131, 3:131] = True
+                m = m.reshape(-1)
+                rng = np.random.default_rng(1234)
+                h = 1e-6
+                c = np.array([0.08, 1.0])
+                errs = []
+                for _ in range(4):
+                    v = rng.normal(size=128 * 128)
+                    d = np.zeros_like(inp["e"])
+                    d[m] = v / np.linalg.norm(v)
+                    fd = (eps_of(inp["e"] + h * d, c) - eps_of(inp["e"] - h * d, c)) / (2 * h)
+                    errs.append(abs(float(np.dot(ge, d)) - fd) / abs(fd))
+                cerr = []
+                for k in range(2):
+                    cp = c.copy(); cm = c.copy()
+                    cp[k] *= 1 + h; cm[k] *= 1 - h
+                    fd = (eps_of(inp["e"], cp) - eps_of(inp["e"], cm)) / (2 * h * c[k])
+                    cerr.append(abs(gc[k] - fd) / abs(fd))
+                res[name]["fd_check"] = {"h": h, "e0_unit_directions_rel_err": errs, "c0_c1_rel_err": cerr}
+            H.close()
+    out = {"metric": "adjoint/forward time ratio", "value": res["fp64"]["ratio"], "unit": "x",
+           "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "dtype": "f64", "data": "synthetic (seeded MC-Glauber initial state)", "vs_baseline": None,
+           "mixed_ratio": res["mixed"]["ratio"], "detail": res, "clocks": clk.summary(),
+           "config": {"workload": "glauber_128x128 adjoint", "grid": [128, 128, 1], "b_fm": 7.0, "seed": 0,
+                      "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "tau_fm": [0.6, 7.2],
+                      "eta_over_s": "0.08 + 1.0 max(T - 0.154, 0)", "checkpoint_every": args.checkpoint_every,
+                      "observable": "eps_p"}}
+    print(json.dumps(out), flush=True)
+
+
 def ctypes_void_p(v):
     import ctypes
     return ctypes.c_void_p(v)
@@ -460,6 +562,10 @@ def main():
     if args.ensemble:
         if rank == 0:
             ensemble(args)
+        return
+    if args.adjoint:
+        if rank == 0:
+            adjoint_ratio(args)
         return
     if args.impl == "reference":
         if rank != 0:

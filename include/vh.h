@@ -221,6 +221,41 @@ int vh_batch_get_tuning(vh_batch* b, int* variant, int* steps_per_launch, int* l
                         int* unroll);
 const char* vh_batch_last_error(const vh_batch* b);
 
+/* ------------------------------------------------------------- adjoint
+ * Gradients of a final-time flow observable (no counterpart in the
+ * reference, whose driver only evolves; NEWEST5/time.h:333 is the step that
+ * is differentiated). */
+
+/* Momentum anisotropy of the current state, summed in FP64 over the interior
+ * cells: eps_p = sum(T^xx - T^yy) / sum(T^xx + T^yy), with
+ * T^ij = (e + P) u^i u^j + P delta^ij + pi^ij.  Boost-invariant grids. */
+int vh_eps_p(vh_handle* h, double* eps_p);
+
+/* Discrete adjoint of eps_p after nsteps steps from the current state
+ * (boost-invariant Milne grids, WENO reconstruction, copy boundaries).  Runs
+ * the forward, checkpointing the state every checkpoint_every steps, then the
+ * reverse of every step, re-running each segment from its checkpoint.  The
+ * max-speed and limiter branches are the forward pass's; the root-find is
+ * differentiated through the implicit-function theorem.  Outputs (each may
+ * be NULL):
+ *   eps_p       the observable at the final time;
+ *   grad_state  18 x n doubles, canonical field order: d eps_p / d (initial
+ *               state), every field an independent variable (fields the step
+ *               never reads get 0);
+ *   grad_e      n doubles: d eps_p / d e of vh_init_profile, i.e. with
+ *               T^{tau mu} = (e + P) u^tau u^mu - P g^{tau mu} + pi^{tau mu}
+ *               re-derived from e at fixed u and pi (ghost cells included);
+ *   grad_etas   2 doubles: d eps_p / d (etas0, etas1) of vh_config.
+ * The handle is left at the final state.  In the mixed mode the adjoint runs
+ * in FP32 with the implicit-function solve in FP64. */
+int vh_adjoint_eps_p(vh_handle* h, int nsteps, int checkpoint_every, double* eps_p, double* grad_state,
+                     double* grad_e, double* grad_etas);
+/* Device milliseconds of the last vh_adjoint_eps_p on this handle: [0] the
+ * forward with its checkpoints, [1] the recomputation of the segments with
+ * their records, [2] the reverse steps, [3] the rest (seed, gradient export,
+ * state restore, and the workspace allocation of a first call). */
+int vh_adjoint_phase_times(const vh_handle* h, double* ms4);
+
 /* Message of the last error on this handle (or the last vh_create). */
 const char* vh_last_error(const vh_handle* h);
 

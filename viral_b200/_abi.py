@@ -99,6 +99,9 @@ SIGNATURES = [
     ("vh_batch_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("vh_batch_get_tuning", ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 5),
     ("vh_batch_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("vh_eps_p", ctypes.c_int, [ctypes.c_void_p, _dp]),
+    ("vh_adjoint_eps_p", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]),
+    ("vh_adjoint_phase_times", ctypes.c_int, [ctypes.c_void_p, _dp]),
 ]
 
 _lib = None

@@ -63,6 +63,23 @@ def glauber_inputs(cfg: Config, b=7.0, seed=0, efloor_gev=None):
     return dict(tau=cfg.tau0, e=e, ux=z, uy=z, ueta=z, prevu=None, pi_mode=A.PI_ZERO, npart=npart)
 
 
+# The adjoint workload: boost-invariant 128x128 event, b = 7 fm, seed 0,
+# eta/s(T) = 0.08 + 1.0 GeV^-1 max(T - 0.154 GeV, 0), 330 steps from 0.6 to
+# 7.2 fm/c.  Its floor is 0.5 GeV/fm^3: with 0.04 the near-vacuum edge makes
+# eps_p non-smooth at the 1e-6 scale (central differences with h = 1e-6 miss
+# the derivative by O(1) and reach it only at h <= 1e-9).
+ADJOINT_FLOOR_GEV = 0.5
+ADJOINT_STEPS = 330
+
+
+def adjoint_config(side=128, precision=A.PREC_FP64, c0=0.08, c1=1.0) -> Config:
+    return glauber_config(nx=side, ny=side, boost_invariant=True, precision=precision, etas0=c0, etas1=c1)
+
+
+def adjoint_inputs(cfg: Config, b=7.0, seed=0):
+    return glauber_inputs(cfg, b=b, seed=seed, efloor_gev=ADJOINT_FLOOR_GEV)
+
+
 def make_hydro(cfg: Config, inputs: dict):
     from .hydro import Hydro
     h = Hydro(cfg)

@@ -9,62 +9,13 @@
 #include <vector>
 
 #include "vh.h"
-#include "vh_aux.cuh"
+#include "vh_handle.cuh"
 #include "vh_internal.h"
 
 using namespace vh;
 
-struct vh_handle {
-  vh_config cfg{};
-  DevCfg C{};
-  cudaStream_t stream = nullptr;
-  bool mixed = false;
-  size_t esz = 8;            // bytes per state element
-  void* state = nullptr;     // 18 canonical fields + B(9) + v1t(4) + res(9) + du(12)
-  double* stage = nullptr;   // 18*n doubles: host<->device staging for the mixed path / du16 scratch
-  double* eos_d = nullptr;
-  float* eos_f = nullptr;
-  unsigned int* status = nullptr;
-  unsigned long long* iters = nullptr;
-  unsigned long long* red = nullptr;  // reduction slots
-  double* part = nullptr;              // conservation partial sums
-  int part_blocks = 0;
-  DevPtrs<double> pd{};
-  DevPtrs<float> pf{};
-  std::vector<double> eos_host;  // 4 x eos_n
-  double tau = 0;
-  bool have_state = false;
-  std::string err;
-};
 
 static std::string g_create_err;
-
-#define VH_CUDA(h, call)                                                                        \
-  do {                                                                                          \
-    cudaError_t _e = (call);                                                                    \
-    if (_e != cudaSuccess) {                                                                    \
-      (h)->err = std::string(#call) + ": " + cudaGetErrorString(_e);                            \
-      return VH_E_CUDA;                                                                         \
-    }                                                                                           \
-  } while (0)
-
-static int fail(vh_handle* h, int code, const std::string& msg) {
-  if (h) h->err = msg;
-  return code;
-}
-
-template <class R>
-static void set_ptrs(DevPtrs<R>& P, void* base, long long n, unsigned int* status, unsigned long long* iters) {
-  P.base0 = static_cast<R*>(base);
-  P.base1 = static_cast<R*>(base) + 18 * n;
-  P.stride = n;
-  P.status = status;
-  P.iters = iters;
-}
-static constexpr int kStateArrays = 52;
-
-template <class R>
-static int set_smem_attrs(vh_handle* h);
 
 static int validate(const vh_config* c, std::string& why) {
   if (!c) { why = "null config"; return VH_E_ARG; }
@@ -165,6 +116,7 @@ extern "C" int vh_destroy(vh_handle* h) {
   if (!h) return VH_OK;
   cudaFree(h->state); cudaFree(h->stage); cudaFree(h->eos_d); cudaFree(h->eos_f);
   cudaFree(h->status); cudaFree(h->iters); cudaFree(h->red); cudaFree(h->part);
+  cudaFree(h->adj_buf);
   delete h;
   return VH_OK;
 }
@@ -181,7 +133,6 @@ extern "C" int vh_dims(const vh_handle* h, int* gx, int* gy, int* gz) {
   return VH_OK;
 }
 
-static inline unsigned grid1(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // device canonical doubles (18*n) -> state
 static int import_device(vh_handle* h, const double* dev) {
@@ -238,80 +189,6 @@ extern "C" int vh_get_state(vh_handle* h, double* host) {
   return VH_OK;
 }
 
-template <class R>
-static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, double tau, int first) {
-  const DevCfg& C = h->C;
-  const int nzi = C.kr - C.kl;
-  dim3 grid, block;
-  size_t sm;
-  const double hh = dir == 0 ? C.dx : (dir == 1 ? C.dy : C.dz);
-  const R inv_h = (R)(1.0 / hh), hr = (R)hh;
-  if (dir == 0) {
-    using T = Tile<0, R>;
-    block = dim3(T::NA * T::NC);
-    grid = dim3((C.nx + T::NA - 7) / (T::NA - 6), (C.ny + T::NC - 1) / T::NC, nzi);
-    sm = sizeof(DirSmem<R, 0>);
-    k_dir<R, 0><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
-  } else if (dir == 1) {
-    using T = Tile<1, R>;
-    block = dim3(T::NA * T::NC);
-    grid = dim3((C.ny + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, nzi);
-    sm = sizeof(DirSmem<R, 1>);
-    k_dir<R, 1><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
-  } else {
-    using T = Tile<2, R>;
-    block = dim3(T::NA * T::NC);
-    grid = dim3((C.nz + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, C.ny);
-    sm = sizeof(DirSmem<R, 2>);
-    k_dir<R, 2><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
-  }
-  VH_CUDA(h, cudaGetLastError());
-  return VH_OK;
-}
-
-template <class R>
-static int set_smem_attrs(vh_handle* h) {
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 0>)));
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 1>)));
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 2>)));
-  return VH_OK;
-}
-
-// the flux-divergence part of a stage: every direction into res, du
-template <class R>
-static int stage_rhs(vh_handle* h, const DevPtrs<R>& P, int use_b, double tau) {
-  int r;
-  if ((r = launch_dir<R>(h, P, 0, use_b, tau, 1))) return r;
-  if ((r = launch_dir<R>(h, P, 1, use_b, tau, 0))) return r;
-  if (!h->C.bi && (r = launch_dir<R>(h, P, 2, use_b, tau, 0))) return r;
-  return VH_OK;
-}
-
-template <class R>
-static int step_once(vh_handle* h, const DevPtrs<R>& P) {
-  const DevCfg& C = h->C;
-  const double tau = h->tau, ts = h->cfg.dtau;
-  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
-  int r;
-  if ((r = stage_rhs<R>(h, P, 0, tau))) return r;
-  k_update<R, 1><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
-  VH_CUDA(h, cudaGetLastError());
-  if ((r = stage_rhs<R>(h, P, 1, tau + ts))) return r;
-  k_update<R, 2><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
-  VH_CUDA(h, cudaGetLastError());
-  h->tau = tau + ts;
-  return VH_OK;
-}
-
-static int read_status(vh_handle* h) {
-  unsigned int st = 0;
-  VH_CUDA(h, cudaMemcpyAsync(&st, h->status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
-  VH_CUDA(h, cudaStreamSynchronize(h->stream));
-  if (st & ST_ROOT) return fail(h, VH_E_ROOTFIND, "root-find failed in at least one cell");
-  if (st & ST_NEGE) return fail(h, VH_E_NEG_ENERGY, "non-positive energy density after the root-find");
-  if (st & ST_CAUSAL) return fail(h, VH_E_CAUSALITY, "superluminal velocity after the root-find");
-  return VH_OK;
-}
 
 extern "C" int vh_step(vh_handle* h, int nsteps) {
   if (!h || nsteps < 0) return VH_E_ARG;

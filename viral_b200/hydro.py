@@ -151,6 +151,30 @@ class Hydro:
     def write(self, path: str, layout: int = A.WRITE_XY, every: int = 1):
         self._chk(A.lib().vh_write(self.h, path.encode(), layout, every))
 
+    # ---- observable and its adjoint
+    def eps_p(self) -> float:
+        v = ctypes.c_double()
+        self._chk(A.lib().vh_eps_p(self.h, ctypes.byref(v)))
+        return v.value
+
+    def adjoint_eps_p(self, nsteps: int, checkpoint_every: int = 25, want_state: bool = True):
+        """eps_p after nsteps steps and its gradients: (eps_p, d/d state (18, n)
+        or None, d/d e of init_profile (n,), d/d (etas0, etas1)).  The handle
+        is left at the final state."""
+        v = ctypes.c_double()
+        gs = np.zeros((A.NFIELDS, self.n)) if want_state else None
+        ge = np.zeros(self.n)
+        gc = np.zeros(2)
+        self._chk(A.lib().vh_adjoint_eps_p(self.h, nsteps, checkpoint_every, ctypes.byref(v), A.ptr(gs), A.ptr(ge),
+                                           A.ptr(gc)))
+        return v.value, gs, ge, gc
+
+    def adjoint_phase_times(self) -> np.ndarray:
+        """device ms of the last adjoint: forward, recompute, reverse, rest"""
+        out = np.zeros(4)
+        self._chk(A.lib().vh_adjoint_phase_times(self.h, A.ptr(out)))
+        return out
+
     def debug_stage_terms(self):
         res = np.zeros((9, self.n)); src = np.zeros((9, self.n)); du = np.zeros((16, self.n))
         self._chk(A.lib().vh_debug_stage_terms(self.h, A.ptr(res), A.ptr(src), A.ptr(du)))
