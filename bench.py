@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--adjoint", action="store_true",
                    help="adjoint/forward device-time ratio of the eps_p gradient (128x128 Glauber, 330 steps)")
     p.add_argument("--checkpoint-every", type=int, default=25)
+    p.add_argument("--adjoint-precision", default="both", choices=["both", "fp64", "mixed"])
+    p.add_argument("--adjoint-fd", type=int, default=4,
+                   help="unit directions of the finite-difference check in the adjoint mode (0: none)")
     return p.parse_args()
 
 
@@ -228,6 +231,15 @@ def algorithmic_bytes(cfg, kernel: str) -> float:
     return w * (9 + 12 + 1 + 4 + 4 + 9 + 4 + 4 + 9 + 1 + 4)
 
 
+# DRAM bytes (read + write) per interior cell and launch, from one ncu capture
+# of the 121x121x31 case of the bench event (profiles/step_kernels_*.md),
+# scaled to a full launch by the cells processed
+MEASURED_TRAFFIC_PER_CELL = {
+    ("fp64", "k_dir_x"): 137.0, ("fp64", "k_dir_y"): 220.0, ("fp64", "k_dir_eta"): 249.0,
+    ("fp64", "k_update_stage1"): 465.0,
+}
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -317,7 +329,9 @@ def run_ours(args, rank, world, dist):
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n18 * 8, "d2h_bytes_per_step": n18 * 8,
                     "what": "vh_set_state (pinned host) + vh_step(1) + vh_get_state per step"},
             "roofline": {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "peak_source": peak_kind, "traffic": None,
+                         "frac": ach / peak, "peak_source": peak_kind,
+                         "traffic": (MEASURED_TRAFFIC_PER_CELL[(args.precision, top)] * cells
+                                     if (args.precision, top) in MEASURED_TRAFFIC_PER_CELL else None),
                          "algorithmic_bytes_per_cell": algorithmic_bytes(cfg, top),
                          "kernel_ms_per_launch": per_launch, "kernel_share": share},
         }
@@ -469,7 +483,9 @@ def adjoint_ratio(args):
     nsteps = C.ADJOINT_STEPS
     res = {}
     with ClockSampler(dev) as clk:
-        for name, prec in (("fp64", A.PREC_FP64), ("mixed", A.PREC_MIXED)):
+        modes = [("fp64", A.PREC_FP64), ("mixed", A.PREC_MIXED)]
+        modes = [m_ for m_ in modes if args.adjoint_precision in ("both", m_[0])]
+        for name, prec in modes:
             cfg = C.adjoint_config(128, prec)
             inp = C.adjoint_inputs(cfg)
             H = C.make_hydro(cfg, inp)
@@ -504,7 +520,7 @@ def adjoint_ratio(args):
                                                "reverse": phases[2], "rest": phases[3]},
                          "eps_p_forward": eps_f, "grad_etas": out[3].tolist(),
                          "grad_e0_norm": float(np.linalg.norm(out[2]))}
-            if name == "fp64":
+            if name == "fp64" and args.adjoint_fd > 0:
                 ge, gc = out[2], out[3]
 
                 def eps_of(e0, c):
@@ -521,7 +537,7 @@ def adjoint_ratio(args):
                 h = 1e-6
                 c = np.array([0.08, 1.0])
                 errs = []
-                for _ in range(4):
+                for _ in range(args.adjoint_fd):
                     v = rng.normal(size=128 * 128)
                     d = np.zeros_like(inp["e"])
                     d[m] = v / np.linalg.norm(v)
@@ -535,10 +551,12 @@ def adjoint_ratio(args):
                     cerr.append(abs(gc[k] - fd) / abs(fd))
                 res[name]["fd_check"] = {"h": h, "e0_unit_directions_rel_err": errs, "c0_c1_rel_err": cerr}
             H.close()
-    out = {"metric": "adjoint/forward time ratio", "value": res["fp64"]["ratio"], "unit": "x",
+    first = "fp64" if "fp64" in res else "mixed"
+    out = {"metric": "adjoint/forward time ratio", "value": res[first]["ratio"], "unit": "x",
            "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-           "dtype": "f64", "data": "synthetic (seeded MC-Glauber initial state)", "vs_baseline": None,
-           "mixed_ratio": res["mixed"]["ratio"], "detail": res, "clocks": clk.summary(),
+           "dtype": "f64" if first == "fp64" else "f32 (FP64 implicit-function solve)",
+           "data": "synthetic (seeded MC-Glauber initial state)", "vs_baseline": None,
+           "mixed_ratio": res["mixed"]["ratio"] if "mixed" in res else None, "detail": res, "clocks": clk.summary(),
            "config": {"workload": "glauber_128x128 adjoint", "grid": [128, 128, 1], "b_fm": 7.0, "seed": 0,
                       "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "tau_fm": [0.6, 7.2],
                       "eta_over_s": "0.08 + 1.0 max(T - 0.154, 0)", "checkpoint_every": args.checkpoint_every,
