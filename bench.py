@@ -52,11 +52,15 @@ def parse():
     p.add_argument("--ensemble", type=int, default=0,
                    help="events/s of a batched ensemble of this many boost-invariant events")
     p.add_argument("--ensemble-precision", default="mixed", choices=["fp64", "mixed"])
+    p.add_argument("--ensemble-floor", type=float, default=None,
+                   help="initial energy-density floor of the ensemble events in GeV/fm^3 (default: the workload's)")
     p.add_argument("--loop-per-side", type=int, default=2,
                    help="events per grid side for the looped single-event FP64 baseline")
     p.add_argument("--adjoint", action="store_true",
                    help="adjoint/forward device-time ratio of the eps_p gradient (128x128 Glauber, 330 steps)")
     p.add_argument("--checkpoint-every", type=int, default=25)
+    p.add_argument("--adjoint-steps", type=int, default=0,
+                   help="steps of the adjoint workload (0: its 330 steps to tau = 7.2 fm/c); small values for profiling")
     p.add_argument("--adjoint-precision", default="both", choices=["both", "fp64", "mixed"])
     p.add_argument("--adjoint-fd", type=int, default=4,
                    help="unit directions of the finite-difference check in the adjoint mode (0: none)")
@@ -236,7 +240,9 @@ def algorithmic_bytes(cfg, kernel: str) -> float:
 # scaled to a full launch by the cells processed
 MEASURED_TRAFFIC_PER_CELL = {
     ("fp64", "k_dir_x"): 137.0, ("fp64", "k_dir_y"): 220.0, ("fp64", "k_dir_eta"): 249.0,
-    ("fp64", "k_update_stage1"): 465.0,
+    ("fp64", "k_update_stage1"): 465.0, ("fp64", "k_update_stage2"): 497.0,
+    ("mixed", "k_dir_x"): 61.0, ("mixed", "k_dir_y"): 105.0, ("mixed", "k_dir_eta"): 113.0,
+    ("mixed", "k_update_stage1"): 188.0,
 }
 
 
@@ -411,7 +417,8 @@ def ensemble(args):
     cfg = C.glauber_config(nx=8, ny=8, boost_invariant=True, precision=prec)
     t_init = time.perf_counter()
     B = Batch(cfg, sides, tau0=tau0, dtau=dtau, tau_max=tau_max, t_freeze_gev=t_fo)
-    npart = B.init_glauber(seeds=np.arange(n), bimp=bimp)
+    floor = C.ENSEMBLE_FLOOR_GEV if args.ensemble_floor is None else args.ensemble_floor
+    npart = B.init_glauber(seeds=np.arange(n), bimp=bimp, efloor_gev=floor)
     t_init = time.perf_counter() - t_init
     cache = os.path.join(tempfile.gettempdir(), "vh_batch_tuning.txt")
     tune_ms = B.autotune(cache, probe_steps=16)
@@ -430,7 +437,7 @@ def ensemble(args):
         for q in range(args.loop_per_side):
             ev = int(np.where(sides == side)[0][q]) if np.sum(sides == side) > q else q
             c = C.glauber_config(nx=int(side), ny=int(side), boost_invariant=True)
-            inp = C.glauber_inputs(c, b=float(bimp[ev]), seed=ev)
+            inp = C.glauber_inputs(c, b=float(bimp[ev]), seed=ev, efloor_gev=floor)
             H = C.make_hydro(c, inp)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -457,7 +464,8 @@ def ensemble(args):
            "speedup_vs_loop_fp64": loop_seconds / sec, "clocks": clk.summary(),
            "config": {"workload": "glauber ensemble", "sides": [64, 96, 128, 160, 200], "dx_fm": 0.1,
                       "b_fm": [0, 12], "dtau_fm": dtau, "tau0_fm": tau0, "tau_max_fm": tau_max,
-                      "t_freeze_gev": t_fo, "precision": f"{args.ensemble_precision} (batch) / fp64 (loop)"}}
+                      "t_freeze_gev": t_fo, "floor_gev_fm3": floor,
+                      "precision": f"{args.ensemble_precision} (batch) / fp64 (loop)"}}
     print(json.dumps(out), flush=True)
 
 
@@ -480,7 +488,7 @@ def adjoint_ratio(args):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
-    nsteps = C.ADJOINT_STEPS
+    nsteps = args.adjoint_steps if args.adjoint_steps > 0 else C.ADJOINT_STEPS
     res = {}
     with ClockSampler(dev) as clk:
         modes = [("fp64", A.PREC_FP64), ("mixed", A.PREC_MIXED)]
@@ -558,7 +566,7 @@ def adjoint_ratio(args):
            "data": "synthetic (seeded MC-Glauber initial state)", "vs_baseline": None,
            "mixed_ratio": res["mixed"]["ratio"] if "mixed" in res else None, "detail": res, "clocks": clk.summary(),
            "config": {"workload": "glauber_128x128 adjoint", "grid": [128, 128, 1], "b_fm": 7.0, "seed": 0,
-                      "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "tau_fm": [0.6, 7.2],
+                      "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "tau_fm": [0.6, 0.6 + 0.02 * nsteps],
                       "eta_over_s": "0.08 + 1.0 max(T - 0.154, 0)", "checkpoint_every": args.checkpoint_every,
                       "observable": "eps_p"}}
     print(json.dumps(out), flush=True)

@@ -233,8 +233,10 @@ int vh_eps_p(vh_handle* h, double* eps_p);
 
 /* Discrete adjoint of eps_p after nsteps steps from the current state
  * (boost-invariant Milne grids, WENO reconstruction, copy boundaries).  Runs
- * the forward, checkpointing the state every checkpoint_every steps, then the
- * reverse of every step, re-running each segment from its checkpoint.  The
+ * the forward in segments of checkpoint_every steps (the first segment takes
+ * the remainder), checkpointing the state at each segment start, then the
+ * reverse of every step, re-running each segment from its checkpoint (the
+ * last one is recorded during the forward).  The
  * max-speed and limiter branches are the forward pass's; the root-find is
  * differentiated through the implicit-function theorem.  Outputs (each may
  * be NULL):

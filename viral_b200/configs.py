@@ -53,6 +53,10 @@ def glauber_config(nx=161, ny=161, nz=41, boost_invariant=False, precision=A.PRE
 # the fireball (pi/e > 20, |v| -> 1) until the root-find has no solution
 # before tau = 10 fm/c; the reference enables no regulator for that.
 GLAUBER_FLOOR_GEV = 0.04
+# Floor of the batched-ensemble events (boost-invariant, to tau = 15 fm/c).
+# Of 2048 events, 268 end in a failed root-find (|v| -> 1 at the box edge)
+# with 0.04 GeV/fm^3, 82 with 0.1, 50 with 0.5 (mixed; FP64: 55).
+ENSEMBLE_FLOOR_GEV = 0.5
 
 
 def glauber_inputs(cfg: Config, b=7.0, seed=0, efloor_gev=None):

@@ -293,8 +293,13 @@ struct DirArgs {
 // quantities whose WENO stencils are reversed at the same time, threads per
 // line block, and shared-memory words per line cell
 constexpr int kQP = 4;
-constexpr int kDirThreads = 512;
 constexpr int kDirWords = 55 + 5 * kQP;
+// threads per line block: two blocks per SM keep all the lines of a 128^2
+// grid (256 blocks) resident in one wave at either precision
+template <class R>
+struct DirShape {
+  static constexpr int threads = sizeof(R) == 8 ? 256 : 512;
+};
 
 template <class R>
 __device__ __forceinline__ R sgn(R x) { return (R)((x > (R)0) - (x < (R)0)); }
@@ -429,7 +434,7 @@ __device__ __forceinline__ void adj_line(const DirArgs<R>& a, int line, R* sm) {
 
 // blockIdx.y = direction, blockIdx.x = line
 template <class R>
-__global__ void __launch_bounds__(kDirThreads) k_adj_dir(DirArgs<R> a) {
+__global__ void __launch_bounds__(DirShape<R>::threads, 2) k_adj_dir(DirArgs<R> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
   if (blockIdx.y == 0) {
@@ -576,18 +581,15 @@ int record_step(vh_handle* h, const DevPtrs<R>& P, R* xrec, R* yrec) {
   const DevCfg& C = h->C;
   const size_t nb = (size_t)C.n * sizeof(R);
   const double tau = h->tau, ts = h->cfg.dtau;
-  const long long nint = (long long)C.nx * C.ny;
   cudaStream_t st = h->stream;
   int r;
   VH_CUDA(h, cudaMemcpyAsync(xrec, P.base0, 18 * nb, cudaMemcpyDeviceToDevice, st));
   if ((r = stage_rhs<R>(h, P, 0, tau))) return r;
-  k_update<R, 1><<<grid1(nint, 128), 128, 0, st>>>(C, P, tau, ts);
-  VH_CUDA(h, cudaGetLastError());
+  if ((r = stage_update<R, 1>(h, P, tau, ts))) return r;
   VH_CUDA(h, cudaMemcpyAsync(yrec, P.base0, 5 * nb, cudaMemcpyDeviceToDevice, st));
   VH_CUDA(h, cudaMemcpyAsync(yrec + 5 * C.n, P.base1, 9 * nb, cudaMemcpyDeviceToDevice, st));
   if ((r = stage_rhs<R>(h, P, 1, tau + ts))) return r;
-  k_update<R, 2><<<grid1(nint, 128), 128, 0, st>>>(C, P, tau, ts);
-  VH_CUDA(h, cudaGetLastError());
+  if ((r = stage_update<R, 2>(h, P, tau, ts))) return r;
   h->tau = tau + ts;
   return VH_OK;
 }
@@ -622,7 +624,11 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
   cudaStream_t st = h->stream;
   const int nseg = (nsteps + every - 1) / every;
   const int seg_len = std::min(every, nsteps);
-  const int last0 = (nseg - 1) * every;  // first step of the last segment
+  // segments: the first takes the remainder, the others `every` steps each,
+  // so the last one (recorded during the forward) is a full segment
+  const int first = nsteps - (nseg - 1) * every;
+  auto seg_start = [&](int k) { return k == 0 ? 0 : first + (k - 1) * every; };
+  const int last0 = seg_start(nseg - 1);  // first step of the last segment
 
   // ---- workspace
   Carve cv;
@@ -676,15 +682,17 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
   int t_start, t_fwd, t_end;
   VH_CUDA(h, clk.mark(st, &t_start));
 
-  // ---- forward: checkpoints every `every` steps; the last segment is
+  // ---- forward: a checkpoint at every segment start; the last segment is
   // recorded as it runs, so it is not recomputed
   const double ts = h->cfg.dtau;
   std::vector<double> taus(nsteps + 1);
   R* state = P.base0;
   int r;
   for (int s = 0; s < nsteps; s++) {
-    if (s % every == 0)
-      VH_CUDA(h, cudaMemcpyAsync(ck + (size_t)(s / every) * 18 * n, state, 18 * nb, cudaMemcpyDeviceToDevice, st));
+    if (s == 0 || (s >= first && (s - first) % every == 0)) {
+      const int k = s == 0 ? 0 : (s - first) / every + 1;
+      VH_CUDA(h, cudaMemcpyAsync(ck + (size_t)k * 18 * n, state, 18 * nb, cudaMemcpyDeviceToDevice, st));
+    }
     taus[s] = h->tau;
     if (s >= last0) r = record_step<R>(h, P, Xr + (size_t)(s - last0) * 18 * n, Yr + (size_t)(s - last0) * kRecY * n);
     else r = step_once<R>(h, P);
@@ -719,13 +727,13 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
   DirArgs<R> d{};
   d.C = C; d.n = n; d.resb = resb; d.dub = dub;
   const int G = std::max(C.gx, C.gy);
-  const int dthreads = kDirThreads;
+  const int dthreads = DirShape<R>::threads;
   const dim3 dgrid(std::max(C.nx, C.ny), 2);
 
   // ---- reverse, one segment at a time
   std::vector<int> seg_marks;
   for (int seg = nseg - 1; seg >= 0; seg--) {
-    const int s0 = seg * every, m = std::min(nsteps, s0 + every) - s0;
+    const int s0 = seg_start(seg), m = (seg + 1 < nseg ? seg_start(seg + 1) : nsteps) - s0;
     int t0, t1, t2;
     VH_CUDA(h, clk.mark(st, &t0));
     if (seg != nseg - 1) {

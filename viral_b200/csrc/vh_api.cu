@@ -207,7 +207,6 @@ extern "C" int vh_step(vh_handle* h, int nsteps) {
 template <class R>
 static int timed_steps(vh_handle* h, const DevPtrs<R>& P, int nsteps, double* out) {
   const DevCfg& C = h->C;
-  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
   cudaEvent_t ev[2];
   VH_CUDA(h, cudaEventCreate(&ev[0]));
   VH_CUDA(h, cudaEventCreate(&ev[1]));
@@ -232,10 +231,7 @@ static int timed_steps(vh_handle* h, const DevPtrs<R>& P, int nsteps, double* ou
         r = timed(d, [&]() { return launch_dir<R>(h, P, d, stage, t, d == 0); });
       if (r) break;
       r = timed(3 + stage, [&]() -> int {
-        if (stage == 0) k_update<R, 1><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
-        else k_update<R, 2><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
-        VH_CUDA(h, cudaGetLastError());
-        return VH_OK;
+        return stage == 0 ? stage_update<R, 1>(h, P, tau, ts) : stage_update<R, 2>(h, P, tau, ts);
       });
     }
     h->tau = tau + ts;

@@ -116,18 +116,25 @@ static int stage_rhs(vh_handle* h, const DevPtrs<R>& P, int use_b, double tau) {
   return VH_OK;
 }
 
+// the update part of a stage (sources, RK, root-find, ghosts): k_update,
+// one thread per interior cell
+template <class R, int STAGE>
+static int stage_update(vh_handle* h, const DevPtrs<R>& P, double tau, double ts) {
+  const DevCfg& C = h->C;
+  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
+  k_update<R, STAGE><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
+  VH_CUDA(h, cudaGetLastError());
+  return VH_OK;
+}
+
 template <class R>
 static int step_once(vh_handle* h, const DevPtrs<R>& P) {
-  const DevCfg& C = h->C;
   const double tau = h->tau, ts = h->cfg.dtau;
-  const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
   int r;
   if ((r = stage_rhs<R>(h, P, 0, tau))) return r;
-  k_update<R, 1><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
-  VH_CUDA(h, cudaGetLastError());
+  if ((r = stage_update<R, 1>(h, P, tau, ts))) return r;
   if ((r = stage_rhs<R>(h, P, 1, tau + ts))) return r;
-  k_update<R, 2><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
-  VH_CUDA(h, cudaGetLastError());
+  if ((r = stage_update<R, 2>(h, P, tau, ts))) return r;
   h->tau = tau + ts;
   return VH_OK;
 }

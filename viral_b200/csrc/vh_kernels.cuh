@@ -233,20 +233,32 @@ __device__ inline void ghost_put(const DevPtrs<R>& P, int set_b, long long dst, 
   for (int l = 0; l < 9; l++) P.S(set_b, l)[dst] = q9[l];
 }
 
-// One thread per interior cell: du_tau, sources, the RK combination, the
-// root-find and the ghost copy.  STAGE 1 reads set A and writes set B and
-// v1t; STAGE 2 reads A (its own cell), B and v1t and writes A.
-// One interior cell t (0 <= t < nx*ny*nz) of the update; returns the Newton
-// iterations and, at stage 2, the new temperature in GeV in *t_gev.
+// The update of one interior cell, in two parts: rk_cell (du_tau, sources,
+// the RK combination, prevu) and root_cell (the root-find and the ghost
+// copy).  STAGE 1 reads set A and writes set B and v1t; STAGE 2 reads A (its
+// own cell), B and v1t and writes A.
+struct CellAt {
+  int i, j, k;
+  long long c;
+};
+__device__ __forceinline__ CellAt cell_at(const DevCfg& C, long long t) {
+  CellAt x;
+  x.i = C.il + (int)(t % C.nx);
+  x.j = C.jl + (int)((t / C.nx) % C.ny);
+  x.k = C.kl + (int)(t / ((long long)C.nx * C.ny));
+  x.c = cix(C, x.i, x.j, x.k);
+  return x;
+}
+
+// Sources and RK combination of cell x: stores the new conserved set (q9,
+// also returned) and, at stage 1, v1t and prevu; returns e, u and prevu for
+// the root-find.
 template <class R, int STAGE>
-__device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R>& P, double tau_n, double ts,
-                                                long long t, double* t_gev) {
-  unsigned my_it = 0;
+__device__ __forceinline__ void rk_cell(const DevCfg& C, const DevPtrs<R>& P, double tau_n, double ts, const CellAt& x,
+                                        R& e_out, R* u_out, R* pu_out, R* q9) {
   {
-    const int i = C.il + (int)(t % C.nx);
-    const int j = C.jl + (int)((t / C.nx) % C.ny);
-    const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
-    const long long c = cix(C, i, j, k);
+    const int k = x.k;
+    const long long c = x.c;
     const double tau1 = tau_n + ts;
     const R tau_s = (R)(STAGE == 1 ? tau_n : tau1);  // time of the sources
     const bool cart = C.cart;
@@ -314,7 +326,6 @@ __device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R
         Vn[l] = (R)0.5 * v0 + (R)0.5 * v1 + (R)0.5 * (R)ts * L1;
       }
     }
-    R q9[9];
 #pragma unroll
     for (int l = 0; l < 4; l++) q9[l] = cart ? Vn[l] : Vn[l] / (R)tau1;
 #pragma unroll
@@ -326,6 +337,25 @@ __device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R
 #pragma unroll
       for (int l = 0; l < 4; l++) { pu[l] = u[l]; P.pu(l)[c] = u[l]; }
     }
+#pragma unroll
+    for (int l = 0; l < 4; l++) { u_out[l] = u[l]; pu_out[l] = pu[l]; }
+    e_out = e;
+  }
+}
+
+// Root-find (FP64) of cell x from its new conserved set q9 with (e, u) as the
+// guess, then the ghost copy; returns the Newton iterations and, at stage 2,
+// the new temperature in GeV in *t_gev.
+template <class R, int STAGE>
+__device__ __forceinline__ unsigned root_cell(const DevCfg& C, const DevPtrs<R>& P, double tau_n, double ts,
+                                              const CellAt& at, R e, R* u, const R* pu, const R* q9, double* t_gev) {
+  unsigned my_it = 0;
+  {
+    const int i = at.i, j = at.j, k = at.k;
+    const long long c = at.c;
+    const double tau1 = tau_n + ts;
+    const bool cart = C.cart;
+    const int out_b = STAGE == 1 ? 1 : 0;  // conserved set written
     // root-find (FP64) with the current primitives as the guess
     double Tt[4], pd[5], x[4] = {(double)e, (double)u[1], (double)u[2], (double)u[3]};
 #pragma unroll
@@ -377,6 +407,16 @@ __device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R
     if (STAGE == 2 && t_gev) *t_gev = C.hbarc * (double)eos_T<R>(C, e);
   }
   return my_it;
+}
+
+// One interior cell t (0 <= t < nx*ny*nz) of the update, both parts.
+template <class R, int STAGE>
+__device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R>& P, double tau_n, double ts,
+                                                long long t, double* t_gev) {
+  const CellAt x = cell_at(C, t);
+  R e, u[4], pu[4], q9[9];
+  rk_cell<R, STAGE>(C, P, tau_n, ts, x, e, u, pu, q9);
+  return root_cell<R, STAGE>(C, P, tau_n, ts, x, e, u, pu, q9, t_gev);
 }
 
 // one thread per interior cell
