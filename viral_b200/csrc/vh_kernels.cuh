@@ -181,6 +181,11 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   }
   const bool out = a >= 3 && a < 3 + TL && g < hi;  // interior cell of this tile
   const long long cell = cb + (long long)g * stride;
+  // the divergence accumulated by the previous sweeps: loaded before the
+  // flux loop so that the loads overlap the reconstruction
+  R racc[9];
+#pragma unroll
+  for (int l = 0; l < 9; l++) racc[l] = (!first && out) ? P.res(l)[cell] : (R)0;
 #pragma unroll UNR
   for (int l = 0; l < 9; l++) {
     R fl = 0, fr = 0, vl = 0, vr = 0;
@@ -194,7 +199,7 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
     const R Hl = shfl_up<R>(H, 1);                                // flux at the left face
     if (out) {
       const R r = -inv_h * (H - Hl);
-      P.res(l)[cell] = first ? r : P.res(l)[cell] + r;
+      P.res(l)[cell] = first ? r : racc[l] + r;
     }
   }
   // velocity derivative along DIR: (L - R)/h of the same stencil (genWENOder)
