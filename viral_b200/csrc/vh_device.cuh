@@ -162,7 +162,27 @@ VH_HD inline R eos_T(const DevCfg& C, R e) {
   eos_table<R>(C, e, &P, &c, &T);
   return T;
 }
-// eta = (eta/s)(T) s with s = (e+P)/T, and tau_pi (NEWEST5/maindef.h:336-339)
+// P, c_s^2 and T of one state (one table lookup)
+template <class R>
+VH_HD inline void eos_all(const DevCfg& C, R e, R& P, R& cs2, R& T) {
+  if (C.eos_kind == 0) {
+    P = e / (R)3;
+    cs2 = (R)1 / (R)3;
+    T = conf_T(e / (R)C.eos_a);
+    return;
+  }
+  eos_table<R>(C, e, &P, &cs2, &T);
+}
+// eta = (eta/s)(T) s with s = (e+P)/T, and tau_pi (NEWEST5/maindef.h:336-339),
+// from a known temperature
+template <class R>
+VH_HD inline void transport_T(const DevCfg& C, R e, R P, R T, R* eta, R* taupi) {
+  R s = (e + P) / T;
+  R tg = T * (R)C.hbarc - (R)C.etas_tc;
+  R etas = (R)C.etas0 + (R)C.etas1 * (tg > (R)0 ? tg : (R)0);
+  *eta = etas * s;
+  *taupi = (C.taupi_kind == 1) ? (R)5 * (*eta) / (e + P) : (R)1.5 * ((*eta) / P);
+}
 template <class R>
 VH_HD inline void transport(const DevCfg& C, R e, R P, R* eta, R* taupi) {
   R T = eos_T<R>(C, e);
@@ -373,12 +393,14 @@ VH_HD inline void is_kinematics(int cart, R tau, const R* u, const R du[4][4], R
   }
 }
 
+// the shear source with P(e) and T(e) already known
 template <class R>
-VH_HD inline void is_source(const DevCfg& C, R tau, R e, const R* u, const R* p, const R du[4][4], R out[5]) {
+VH_HD inline void is_source_PT(const DevCfg& C, R tau, R e, R P, R T, const R* u, const R* p, const R du[4][4],
+                               R out[5]) {
   const int cart = C.cart;
   const R t2 = cart ? (R)1 : tau * tau;
-  R P = eos_P<R>(C, e), eta, tp;
-  transport<R>(C, e, P, &eta, &tp);
+  R eta, tp;
+  transport_T<R>(C, e, P, T, &eta, &tp);
   PiDep<R> d = pi_dep<R>(u[0], u[1], u[2], u[3], p, t2);
   R pi[4][4] = {{d.tt, d.tx, d.ty, d.te}, {d.tx, p[0], p[2], p[3]}, {d.ty, p[2], p[1], p[4]}, {d.te, p[3], p[4], d.ee}};
   R sig[4][4], th, acc[4];
@@ -406,6 +428,13 @@ VH_HD inline void is_source(const DevCfg& C, R tau, R e, const R* u, const R* p,
     }
     out[q] = (rhs - chr) * iu0 + pi[m][v] * divv;
   }
+}
+
+template <class R>
+VH_HD inline void is_source(const DevCfg& C, R tau, R e, const R* u, const R* p, const R du[4][4], R out[5]) {
+  R P, cs2, T;
+  eos_all<R>(C, e, P, cs2, T);
+  is_source_PT<R>(C, tau, e, P, T, u, p, du, out);
 }
 
 // P and dP/de together (one table lookup)
@@ -509,7 +538,9 @@ VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, do
   const double t2 = C.cart ? 1.0 : tau * tau;
   double y[4], J[4][4];
   c2p_fj(C, Tt, p, t2, x, y, J, true);
-  double phi = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+  // squared residual norms: the step control compares and divides squares,
+  // so no square root is taken per trial point
+  double phi = y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3];
   int it = 0;
   while (it < 100) {
     it++;
@@ -522,9 +553,9 @@ VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, do
       for (int i = 0; i < 4; i++) xt[i] = x[i] + t * st[i];
       c2p_fj(C, Tt, p, t2, xt, y, J, true);
       if (!(isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && isfinite(y[3]))) return -1;
-      phi1 = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+      phi1 = y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3];
       if (phi1 <= phi || phi == 0.0) { ok = true; break; }
-      double r = (phi1 * phi1) / (phi * phi);
+      const double r = phi1 / phi;
       t *= (sqrt(1.0 + 6.0 * r) - 1.0) / (3.0 * r);
     }
     if (!ok) return -1;
@@ -540,8 +571,8 @@ VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, do
   }
   // an iterate that is not a root is a failure (the reference keeps it
   // silently after 100 iterations): residual above 1e-8 of |T^{tau mu}|
-  const double scale = fabs(Tt[0]) + fabs(Tt[1]) + fabs(Tt[2]) + fabs(Tt[3]);
-  if (!(phi <= 1e-8 * scale)) return -1;
+  const double scale = 1e-8 * (fabs(Tt[0]) + fabs(Tt[1]) + fabs(Tt[2]) + fabs(Tt[3]));
+  if (!(phi <= scale * scale)) return -1;
   return it;
 }
 

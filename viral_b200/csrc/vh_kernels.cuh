@@ -290,7 +290,8 @@ __device__ __forceinline__ void rk_cell(const DevCfg& C, const DevPtrs<R>& P, do
     // sources (NEWEST5/Source.h:165-191 geometric, 311-433 shear)
     R src[9];
     {
-      const R Pp = eos_P<R>(C, e);
+      R Pp, cs2, Te;
+      eos_all<R>(C, e, Pp, cs2, Te);
       if (cart) {
         src[0] = src[1] = src[2] = src[3] = 0;
       } else {
@@ -303,7 +304,7 @@ __device__ __forceinline__ void rk_cell(const DevCfg& C, const DevPtrs<R>& P, do
         src[3] = -(R)2 * (d.te + ep * u[0] * u[3]);
       }
       R s5[5];
-      is_source<R>(C, tau_s, e, u, p, du, s5);
+      is_source_PT<R>(C, tau_s, e, Pp, Te, u, p, du, s5);
       // TXYZ5/Source.h:268-270: the Cartesian 3+1D shear source skips the
       // last three interior z layers
       if (cart && !C.bi && (k - C.kl) >= C.nz - NG) s5[0] = s5[1] = s5[2] = s5[3] = s5[4] = 0;
@@ -424,9 +425,10 @@ __device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R
   return root_cell<R, STAGE>(C, P, tau_n, ts, x, e, u, pu, q9, t_gev);
 }
 
-// one thread per interior cell
+// one thread per interior cell; 6 blocks per SM (80 registers: the spills
+// cost less than the latency the extra warps hide, measured)
 template <class R, int STAGE>
-__global__ void __launch_bounds__(128, 4) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
+__global__ void __launch_bounds__(128, 6) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
   if (*P.status) return;
   const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
