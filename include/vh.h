@@ -107,6 +107,13 @@ int vh_get_state(vh_handle* h, double* host);
 /* The same with device pointers to 18 x G doubles (no host copies). */
 int vh_set_state_device(vh_handle* h, const double* dev, double tau);
 int vh_get_state_device(vh_handle* h, double* dev);
+/* Primitive fields of every ghost-inclusive cell, as the reference's cell
+ * holds them (NEWEST5/maindef.h:392-466: En, P, Temp, u[4], and pi with its
+ * dependent components A1..A5, maindef.h:497-501): e, P, T (n doubles each),
+ * u^mu (4 x n) and pi^{mu nu} (10 x n, contravariant, in the order tt, tx,
+ * ty, t-eta, xx, xy, x-eta, yy, y-eta, eta-eta), in fm units.  Any pointer
+ * may be NULL. */
+int vh_get_primitive(vh_handle* h, double* e, double* P, double* T, double* u4, double* pi10);
 
 /* Initialise from a profile (the reference's init(tau, ts) with a scenario,
  * NEWEST5/init.h:556-704): e, u^x, u^y, u^eta on the ghost-inclusive grid

@@ -1,0 +1,75 @@
+"""The C++ host driver against the Python path over the same C ABI: the
+snapshots it writes (the reference's file names and layouts) are the bytes
+vh_write gives after the same steps; and vh_get_primitive returns the state's
+primitive fields with the dependent pi components consistent."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from viral_b200 import _abi as A
+from viral_b200 import build
+from viral_b200 import configs as C
+
+pytestmark = pytest.mark.gpu
+
+
+def run_driver(args, tmp):
+    out = os.path.join(tmp, "res")
+    r = subprocess.run([build.build_driver(), *args, "--out", out, "--quiet"], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    return out
+
+
+def test_gubser_snapshots_match_the_python_path(tmp_path):
+    steps = 6
+    out = run_driver(["--scenario", "gubser", "--nx", "33", "--ny", "33", "--steps", str(steps),
+                      "--print-every", "0.03"], str(tmp_path))
+    names = sorted(os.listdir(out))
+    assert names == ["tau1.000fm.bin", "tau1.010fm.bin", "tau1.030fm.bin", "tau1.060fm.bin"], names
+    cfg = C.gubser_config(nx=33, ny=33)
+    with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:
+        H.step(steps)
+        mine = os.path.join(str(tmp_path), "py.bin")
+        H.write(mine, A.WRITE_XY, 1)
+    assert open(mine, "rb").read() == open(os.path.join(out, "tau1.060fm.bin"), "rb").read()
+
+
+def test_glauber_snapshot_matches_the_python_path(tmp_path):
+    steps = 5
+    out = run_driver(["--scenario", "glauber", "--nx", "40", "--ny", "40", "--steps", str(steps), "--b", "6",
+                      "--seed", "3", "--every", "2", "--print-every", "0.1"], str(tmp_path))
+    cfg = C.glauber_config(nx=40, ny=40, boost_invariant=True)
+    with C.make_hydro(cfg, C.glauber_inputs(cfg, b=6.0, seed=3)) as H:
+        H.step(steps)
+        mine = os.path.join(str(tmp_path), "py.bin")
+        H.write(mine, A.WRITE_XY, 2)
+    assert open(mine, "rb").read() == open(os.path.join(out, "tau0.700fm.bin"), "rb").read()
+
+
+def test_get_primitive():
+    cfg = C.gubser_config(nx=21, ny=21)
+    with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:
+        H.step(3)
+        tau = H.tau
+        s = H.get_state()
+        p = H.get_primitive()
+    assert np.array_equal(p["e"], s[0]) and np.array_equal(p["u"], s[1:5])
+    assert np.allclose(p["P"], s[0] / 3, rtol=1e-15)
+    assert np.allclose(p["T"], (s[0] / cfg.eos_a) ** 0.25, rtol=1e-14)
+    pi = p["pi"]
+    assert np.array_equal(pi[4], s[5]) and np.array_equal(pi[7], s[6]) and np.array_equal(pi[5], s[7])
+    # transversality u_mu pi^{mu nu} = 0 and tracelessness g_{mu nu} pi^{mu nu} = 0, metric diag(1,-1,-1,-tau^2)
+    u = p["u"]
+    g = np.array([1.0, -1.0, -1.0, -tau * tau])
+    full = np.zeros((4, 4, pi.shape[1]))
+    idx = {(0, 0): 0, (0, 1): 1, (0, 2): 2, (0, 3): 3, (1, 1): 4, (1, 2): 5, (1, 3): 6, (2, 2): 7, (2, 3): 8, (3, 3): 9}
+    for (a, b), q in idx.items():
+        full[a, b] = pi[q]
+        full[b, a] = pi[q]
+    scale = np.abs(pi).max()
+    for nu in range(4):
+        assert np.abs(sum(g[m] * u[m] * full[m, nu] for m in range(4))).max() <= 1e-12 * scale
+    assert np.abs(sum(g[m] * full[m, m] for m in range(4))).max() <= 1e-12 * scale

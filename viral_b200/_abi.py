@@ -57,6 +57,7 @@ SIGNATURES = [
     ("vh_get_state", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("vh_set_state_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]),
     ("vh_get_state_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("vh_get_primitive", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     ("vh_init_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, _dp]),
     ("vh_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("vh_get_time", ctypes.c_int, [ctypes.c_void_p, _dp]),

@@ -45,6 +45,25 @@ def build_check(verbose: bool = False) -> str:
     return CHECK_LIB
 
 
+DRIVER = os.path.join(HERE, "vh_run")
+
+
+def build_driver(verbose: bool = False) -> str:
+    """vh_run: the C++ host driver (the reference's main loop over the C ABI)."""
+    src = os.path.join(HERE, "host", "vh_run.cpp")
+    deps = [src, LIB, os.path.join(ROOT, "include", "vh.h")]
+    if os.path.exists(DRIVER) and all(os.path.getmtime(d) <= os.path.getmtime(DRIVER) for d in deps):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), src, "-L", HERE, "-lvh",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+    if r.returncode != 0:
+        raise RuntimeError("g++ failed building vh_run")
+    return DRIVER
+
+
 def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "vh.h")]
@@ -69,4 +88,5 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
 if __name__ == "__main__":
     build(verbose="--verbose" in sys.argv)
     build_check(verbose="--verbose" in sys.argv)
+    build_driver(verbose="--verbose" in sys.argv)
     print(LIB)

@@ -303,6 +303,24 @@ extern "C" int vh_init_profile(vh_handle* h, double tau, const double* e, const 
   return VH_OK;
 }
 
+extern "C" int vh_get_primitive(vh_handle* h, double* e, double* P, double* T, double* u4, double* pi10) {
+  if (!h) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  const long long n = h->C.n;
+  double* buf = h->stage;  // 18 x n doubles; 17 are used
+  if (h->mixed) k_primitive<float><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pf, h->tau, buf);
+  else k_primitive<double><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pd, h->tau, buf);
+  VH_CUDA(h, cudaGetLastError());
+  const size_t nb = sizeof(double) * (size_t)n;
+  if (e) VH_CUDA(h, cudaMemcpyAsync(e, buf, nb, cudaMemcpyDeviceToHost, h->stream));
+  if (P) VH_CUDA(h, cudaMemcpyAsync(P, buf + n, nb, cudaMemcpyDeviceToHost, h->stream));
+  if (T) VH_CUDA(h, cudaMemcpyAsync(T, buf + 2 * n, nb, cudaMemcpyDeviceToHost, h->stream));
+  if (u4) VH_CUDA(h, cudaMemcpyAsync(u4, buf + 3 * n, 4 * nb, cudaMemcpyDeviceToHost, h->stream));
+  if (pi10) VH_CUDA(h, cudaMemcpyAsync(pi10, buf + 7 * n, 10 * nb, cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VH_OK;
+}
+
 extern "C" int vh_max_temperature(vh_handle* h, double* tmax_gev) {
   if (!h || !tmax_gev) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");

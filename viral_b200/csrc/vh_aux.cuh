@@ -26,6 +26,35 @@ __global__ void k_fill_tmunu(DevCfg C, DevPtrs<R> P, double tau) {
   P.A(3)[c] = ep * u[0] * u[3] + d.te;
 }
 
+// Primitive fields of every cell into 17 x n doubles: e, P, T, u^mu (4) and
+// the ten pi^{mu nu} (tt, tx, ty, te, xx, xy, xe, yy, ye, ee), the dependent
+// components by transversality and tracelessness (the reference cell's En, P,
+// Temp, u[4] and pi; NEWEST5/maindef.h:392-466, 497-501).
+template <class R>
+__global__ void k_primitive(DevCfg C, DevPtrs<R> P, double tau, double* out) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = C.n;
+  if (c >= n) return;
+  const R t2 = C.cart ? (R)1 : (R)(tau * tau);
+  R u[4], p[5];
+  const R e = P.e()[c];
+#pragma unroll
+  for (int l = 0; l < 4; l++) u[l] = P.u(l)[c];
+#pragma unroll
+  for (int l = 0; l < 5; l++) p[l] = P.A(4 + l)[c];
+  R Pp, cs2, T;
+  eos_all<R>(C, e, Pp, cs2, T);
+  const PiDep<R> d = pi_dep<R>(u[0], u[1], u[2], u[3], p, t2);
+  out[c] = (double)e;
+  out[n + c] = (double)Pp;
+  out[2 * n + c] = (double)T;
+#pragma unroll
+  for (int l = 0; l < 4; l++) out[(3 + l) * n + c] = (double)u[l];
+  const R pi10[10] = {d.tt, d.tx, d.ty, d.te, p[0], p[2], p[3], p[1], p[4], d.ee};
+#pragma unroll
+  for (int l = 0; l < 10; l++) out[(7 + l) * n + c] = (double)pi10[l];
+}
+
 // Velocity gradients with the coverage the reference's CalcDer4Vel has
 // (NEWEST5/Source.h:3-101): d_tau on the interior; d_x for i in [2, gx-3]
 // on interior (j,k); d_y likewise; d_eta for every k on interior (i,j) with

@@ -107,6 +107,13 @@ class Hydro:
         self._chk(A.lib().vh_get_state(self.h, A.ptr(f)))
         return f
 
+    def get_primitive(self) -> dict:
+        """e, P, T (n,), u (4, n), pi (10, n: tt tx ty te xx xy xe yy ye ee)"""
+        e, P, T = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        u, pi = np.zeros((4, self.n)), np.zeros((10, self.n))
+        self._chk(A.lib().vh_get_primitive(self.h, A.ptr(e), A.ptr(P), A.ptr(T), A.ptr(u), A.ptr(pi)))
+        return dict(e=e, P=P, T=T, u=u, pi=pi)
+
     def init_profile(self, tau, e, ux, uy, ueta=None, prevu=None, pi_mode=A.PI_ZERO, pi5=None):
         c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
         self._chk(A.lib().vh_init_profile(self.h, tau, A.ptr(c(e)), A.ptr(c(ux)), A.ptr(c(uy)), A.ptr(c(ueta)),
