@@ -239,10 +239,10 @@ def algorithmic_bytes(cfg, kernel: str) -> float:
 # of the 121x121x31 case of the bench event (profiles/step_kernels_*.md),
 # scaled to a full launch by the cells processed
 MEASURED_TRAFFIC_PER_CELL = {
-    ("fp64", "k_dir_x"): 137.0, ("fp64", "k_dir_y"): 220.0, ("fp64", "k_dir_eta"): 249.0,
-    ("fp64", "k_update_stage1"): 465.0, ("fp64", "k_update_stage2"): 497.0,
-    ("mixed", "k_dir_x"): 61.0, ("mixed", "k_dir_y"): 105.0, ("mixed", "k_dir_eta"): 113.0,
-    ("mixed", "k_update_stage1"): 188.0,
+    ("fp64", "k_dir_x"): 150.0, ("fp64", "k_dir_y"): 239.0, ("fp64", "k_dir_eta"): 261.0,
+    ("fp64", "k_update_stage2"): 651.0,
+    ("mixed", "k_dir_x"): 63.0, ("mixed", "k_dir_y"): 104.0, ("mixed", "k_dir_eta"): 114.0,
+    ("mixed", "k_update_stage2"): 223.0,
 }
 
 
