@@ -2,7 +2,7 @@
 own code (its NEWEST5 / TXYZ5 headers compiled by oracle/Makefile into
 oracle/_ref/).  Runs only where the reference tree is present:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [scenario ...]
 
 For each compile-time scenario of the reference a seeded smooth viscous
 state is built on the reference's grid (pyoracle.smooth_state, then
@@ -13,7 +13,9 @@ T^{tau mu} from the oracle's closure), and the reference computes:
   * residuals and Jacobian of the conserved-to-primitive system at random
     points.
 Outputs are stored at a seeded sample of interior cells (plus per-field
-sums over the whole grid), so that the fixtures stay small.  The CPU tests
+sums over the whole grid), so that the fixtures stay small.  A fifth
+fixture, cart_3d_shock, is the reference's own Cartesian scenario (the
+shock tube of its default TXYZ5 block) after 20 steps.  The CPU tests
 rebuild the same inputs and check the oracle against these numbers.
 """
 from __future__ import annotations
@@ -101,9 +103,47 @@ def make(variant: str) -> dict:
     return out
 
 
+SHOCK_STEPS = 20
+
+
+def shock_tube_state(R: RefBuild) -> np.ndarray:
+    """TXYZ5's default initial state (TXYZ5/init.h:151-210): e = 16 fm^-4 for
+    z < 0 and 1 fm^-4 for z >= 0, at rest, pi = 0, prevu = u, T^{tau mu}
+    from the closure."""
+    sc = SCENARIOS["cart_3d"]
+    x, y, z = R.coords()
+    f = np.zeros((18, R.n))
+    f[0] = np.where(z < 0, 16.0, 1.0)
+    f[1] = 1.0
+    f[14] = 1.0
+    O = Oracle(oracle_config(R, sc))
+    O.set_state(f)
+    O.fill_tmunu(0.0)
+    return O.get_state()
+
+
+def make_shock() -> dict:
+    """The reference's Cartesian shock tube (its default TXYZ5 block),
+    SHOCK_STEPS steps of dt = 0.01 from t = 0."""
+    R = RefBuild("cart_3d")
+    f = shock_tube_state(R)
+    R.set_state(f)
+    t = 0.0
+    for _ in range(SHOCK_STEPS):
+        R.step(t, TS)
+        t += TS
+    s = R.get_state()
+    cells = interior(R)
+    return {"cells": cells, "t": t, "ts": TS, "steps": SHOCK_STEPS,
+            "dims": np.array([R.gx, R.gy, R.gz, int(R.boost_invariant)]),
+            "consts": np.array([R.dx, R.dy, R.dz, R.factor, R.gevfm]),
+            "state": s[:14, cells], "state_sum": s.sum(axis=1)}
+
+
 def main():
-    for v in SCENARIOS:
-        d = make(v)
+    which = sys.argv[1:] or list(SCENARIOS) + ["cart_3d_shock"]
+    for v in which:
+        d = make_shock() if v == "cart_3d_shock" else make(v)
         path = os.path.join(HERE, f"ref_{v}.npz")
         np.savez_compressed(path, **d)
         print(path, os.path.getsize(path))

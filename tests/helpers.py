@@ -69,3 +69,29 @@ def smooth_inputs(cfg: Config, tau: float, seed: int, amp: float = 1.0) -> np.nd
     O.set_state(f)
     O.fill_tmunu(tau)
     return O.get_state()
+
+
+def shock_tube_fixture():
+    """The Cartesian shock tube of the reference's default TXYZ5 block
+    (TXYZ5/init.h:151-210: e = 16 fm^-4 for z < 0, 1 fm^-4 for z >= 0, at
+    rest, pi = 0) and the reference's state after 20 steps, as stored in
+    tests/golden/ref_cart_3d_shock.npz.  Returns (fixture, OracleConfig,
+    initial 18-field state)."""
+    import math
+    import os
+
+    from pyoracle import Oracle, OracleConfig, grid_coords
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_cart_3d_shock.npz"))
+    gx, gy, gz, bi = (int(v) for v in g["dims"])
+    dx, dy, dz, factor, gevfm = (float(v) for v in g["consts"])
+    cfg = OracleConfig(nx=gx - 6, ny=gy - 6, nz=gz - 6, boost_invariant=False, cartesian=True, dx=dx, dy=dy, dz=dz,
+                       eos_kind=0, eos_a=factor, etas0=0.01 / (4 * math.pi), hbarc=gevfm, taupi_kind=0)
+    x, y, z = grid_coords(gx, gy, gz, dx, dy, dz, False)
+    f = np.zeros((18, gx * gy * gz))
+    f[0] = np.where(z < 0, 16.0, 1.0)
+    f[1] = 1.0
+    f[14] = 1.0
+    O = Oracle(cfg)
+    O.set_state(f)
+    O.fill_tmunu(0.0)
+    return g, cfg, O.get_state()

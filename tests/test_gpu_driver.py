@@ -73,3 +73,17 @@ def test_get_primitive():
     for nu in range(4):
         assert np.abs(sum(g[m] * u[m] * full[m, nu] for m in range(4))).max() <= 1e-12 * scale
     assert np.abs(sum(g[m] * full[m, m] for m in range(4))).max() <= 1e-12 * scale
+
+
+def test_shock_tube_scenario_matches_the_reference(tmp_path):
+    """vh_run --scenario shocktube, 20 steps: the full-grid snapshot holds the
+    reference's own state of its Cartesian default block"""
+    from helpers import shock_tube_fixture
+    g, ocfg, f = shock_tube_fixture()
+    out = run_driver(["--scenario", "shocktube", "--steps", "20", "--print-every", "0.2"], str(tmp_path))
+    snap = np.fromfile(os.path.join(out, "tau0.200fm.bin"), dtype=np.float64).reshape(-1, 12)
+    nx, ny, nz = ocfg.nx, ocfg.ny, ocfg.nz
+    # records x outer, y, then z inner; fixture cells are interior cells in (k, j, i) order
+    e = snap[:, 0].reshape(nx, ny, nz).transpose(2, 1, 0).ravel()
+    ref = g["state"][0]
+    assert np.max(np.abs(e - ref)) <= 1e-10 * np.max(np.abs(ref))

@@ -101,3 +101,23 @@ def test_con2prim_residuals(variant):
         scale = np.max(np.abs(p[:4])) * max(1.0, np.max(np.abs(x)))
         assert np.max(np.abs(yo - y)) <= 1e-13 * scale
         assert np.max(np.abs(Jo - J)) <= 1e-13 * max(1.0, np.max(np.abs(J)))
+
+
+def test_cartesian_shock_tube():
+    """The reference's own Cartesian scenario: the oracle runs the shock tube
+    20 steps and reproduces the reference's state at every interior cell"""
+    from helpers import shock_tube_fixture
+    g, cfg, f = shock_tube_fixture()
+    O = Oracle(cfg)
+    O.set_state(f)
+    t = 0.0
+    for _ in range(int(g["steps"])):
+        assert O.step(t, float(g["ts"])) == 0
+        t += float(g["ts"])
+    s = O.get_state()
+    c = g["cells"]
+    for grp in GROUPS:
+        grp = [q for q in grp if q < 14]
+        if grp:
+            assert scaled_err(s[grp][:, c], g["state"][grp]) <= TOL, grp
+    assert np.allclose(s.sum(axis=1)[:14], g["state_sum"][:14], rtol=1e-12, atol=1e-9)

@@ -14,6 +14,10 @@
 //              eta/s 0.08, tau_pi = 1.5 eta/P, tau0 0.6, dtau 0.02;
 //              stops when max T < 120 MeV (main.cpp:201-204, GINIT block)
 //   glauber3d  the same on a 3+1D Milne grid (default 161x161x41, d eta 0.25)
+//   shocktube  the Cartesian default block of TXYZ5 (TXYZ5/maindef.h:35-63,
+//              init.h:151-210): 10x10x101 cells of 0.1 fm, t0 = 0, dt 0.01,
+//              e = 16 fm^-4 for z < 0 and 1 fm^-4 for z >= 0 at rest,
+//              conformal EOS with 42.25 degrees of freedom, eta/s 0.01/(4 pi)
 // Every run also stops at tau > 25.3 fm/c (main.cpp:211) or --tau-end.
 // Snapshots use the reference's names and layouts (res/tau%2.3ffm.bin, one xy
 // plane on boost-invariant grids, the full grid otherwise).
@@ -50,7 +54,7 @@ struct Options {
 
 void usage() {
   std::printf(
-      "usage: vh_run [--scenario gubser|glauber|glauber3d] [--nx N --ny N --nz N]\n"
+      "usage: vh_run [--scenario gubser|glauber|glauber3d|shocktube] [--nx N --ny N --nz N]\n"
       "              [--precision fp64|mixed] [--steps N] [--tau-end T] [--print-every T]\n"
       "              [--out DIR] [--every FREQ] [--b B] [--seed S] [--floor E_GeV_fm3] [--quiet]\n");
 }
@@ -86,7 +90,7 @@ bool parse(int argc, char** argv, Options& o) {
     else if (a == "--quiet") o.quiet = true;
     else { std::fprintf(stderr, "vh_run: unknown option %s\n", a.c_str()); usage(); return false; }
   }
-  if (o.scenario != "gubser" && o.scenario != "glauber" && o.scenario != "glauber3d") {
+  if (o.scenario != "gubser" && o.scenario != "glauber" && o.scenario != "glauber3d" && o.scenario != "shocktube") {
     std::fprintf(stderr, "vh_run: unknown scenario %s\n", o.scenario.c_str());
     return false;
   }
@@ -104,6 +108,7 @@ int main(int argc, char** argv) {
   Options o;
   if (!parse(argc, argv, o)) return 2;
   const bool gubser = o.scenario == "gubser", three_d = o.scenario == "glauber3d";
+  const bool shock = o.scenario == "shocktube";
 
   vh_config c;
   std::memset(&c, 0, sizeof c);
@@ -113,7 +118,14 @@ int main(int argc, char** argv) {
   c.minmod_theta = 1.1;
   c.hbarc = kHbarc;
   std::vector<double> eos_e, eos_p, eos_c, eos_t;
-  if (gubser) {
+  if (shock) {
+    c.coords = VH_COORD_CARTESIAN;
+    c.nx = o.nx ? o.nx : 10; c.ny = o.ny ? o.ny : 10; c.nz = o.nz ? o.nz : 101; c.boost_invariant = 0;
+    c.dx = c.dy = c.dz = 0.1; c.tau0 = 0.0; c.dtau = 0.01;
+    c.eos_kind = VH_EOS_CONFORMAL; c.eos_a = 3 * 42.25 * M_PI * M_PI / 90;
+    c.hbarc = 0.1973;
+    c.etas0 = 0.01 / (4 * M_PI); c.etas_tc = 0.154; c.taupi_kind = VH_TAUPI_15_ETA_OVER_P;
+  } else if (gubser) {
     c.nx = o.nx ? o.nx : 129; c.ny = o.ny ? o.ny : 129; c.nz = 1; c.boost_invariant = 1;
     c.dx = c.dy = 0.1; c.dz = 1.0; c.tau0 = 1.0; c.dtau = 0.01;
     c.eos_kind = VH_EOS_CONFORMAL; c.eos_a = kAqgp;
@@ -139,7 +151,15 @@ int main(int argc, char** argv) {
   const size_t n = (size_t)gx * gy * gz;
   std::vector<double> e(n), ux(n, 0.0), uy(n, 0.0), prevu(4 * n);
   int r;
-  if (gubser) {
+  if (shock) {
+    // cell centres z = -(nz/2) dz + (k - 3) dz, as the reference centres one rank
+    for (int k = 0; k < gz; k++)
+      for (size_t q = 0; q < (size_t)gx * gy; q++) {
+        const double z = -((c.nz / 2) * c.dz) + (k - VH_NGHOST) * c.dz;
+        e[(size_t)k * gx * gy + q] = z < 0 ? 16.0 : 1.0;
+      }
+    r = vh_init_profile(h, c.tau0, e.data(), ux.data(), uy.data(), nullptr, nullptr, VH_PI_ZERO, nullptr);
+  } else if (gubser) {
     r = vh_profile_gubser(c.nx, c.ny, c.dx, c.dy, 1.0, c.tau0, c.dtau, 0.6, c.eos_a, kHbarc, e.data(), ux.data(),
                           uy.data(), prevu.data());
     if (!r) r = vh_init_profile(h, c.tau0, e.data(), ux.data(), uy.data(), nullptr, prevu.data(), VH_PI_NS, nullptr);
@@ -185,7 +205,7 @@ int main(int argc, char** argv) {
     if (std::fabs(tau - (c.tau0 + ts)) < 1e-6 && (r = write(tau))) { status = fail("vh_write", h, r); break; }
     l++;
     if (gubser && tau > 9) break;             // main.cpp:196-199
-    if (!gubser && tmax_mev < 120) break;     // main.cpp:201-204
+    if (!gubser && !shock && tmax_mev < 120) break;  // main.cpp:201-204
     if (tau > o.tau_end) break;                // main.cpp:211
     if (o.max_steps > 0 && l > o.max_steps) break;
   }
