@@ -60,8 +60,9 @@ enum { VH_EOS_CONFORMAL = 0, VH_EOS_TABLE = 1 };
 enum { VH_TAUPI_15_ETA_OVER_P = 0, VH_TAUPI_5_ETA_OVER_EPP = 1 };
 /* initial pi: given, zero, or Navier-Stokes (NEWEST5/Source.h:535-630) */
 enum { VH_PI_GIVEN = 0, VH_PI_ZERO = 1, VH_PI_NS = 2 };
-/* snapshot layouts of NEWEST5/write.h: one xy plane, or the full grid */
-enum { VH_WRITE_XY = 0, VH_WRITE_FULL = 1 };
+/* snapshot layouts: NEWEST5/write.h's 12 doubles per cell for one xy plane
+ * or the full grid, and NEWEST10/write.h's 17 (full pi^{mu nu}) likewise */
+enum { VH_WRITE_XY = 0, VH_WRITE_FULL = 1, VH_WRITE_XY17 = 2, VH_WRITE_FULL17 = 3 };
 
 typedef struct {
   int coords;           /* VH_COORD_* (NEWEST5 Milne, TXYZ5 Cartesian) */
@@ -148,6 +149,22 @@ int vh_cfl(vh_handle* h, double* max_speed, double* dtau_suggest);
  * eta slice (VH_WRITE_FULL, NEWEST5/write.h:225-290); `every` keeps every
  * n-th cell as the reference's FREQ. */
 int vh_write(vh_handle* h, const char* path, int layout, int every);
+/* VH_WRITE_XY17 / VH_WRITE_FULL17: the same two layouts with 17 doubles per
+ * cell (e, T, P, v^x, v^y, v^eta, the ten pi^{mu nu} in the order tt, tx, ty,
+ * t-eta, xx, xy, x-eta, yy, y-eta, eta-eta, Pi), NEWEST10/write.h:51-115 and
+ * its WriteResults. */
+
+/* Initial profile from the ASCII files of the ideal-hydro driver
+ * (NEWideal/init.h:296-345): eps_path, vx_path and vy_path hold nx*ny
+ * whitespace-separated numbers each, x fastest, for the interior cells of a
+ * boost-invariant grid.  Writes e, u^x, u^y on the ghost-inclusive grid
+ * ((nx+6)*(ny+6) doubles each; u = v / sqrt(1 - v^2)) with the reference's
+ * floor: every cell below 0.01 (the ghost cells included) gets min/10, min
+ * being the smallest interior value above 1e-5 in magnitude (100 if none is
+ * smaller); *min_out receives it (may be NULL).  VH_E_ARG when a file cannot
+ * be read or holds fewer than nx*ny numbers. */
+int vh_read_ideal_profile(const char* eps_path, const char* vx_path, const char* vy_path, int nx, int ny,
+                          double* e, double* ux, double* uy, double* min_out);
 
 /* Stage-1 terms for tests: the flux divergence res[9*G], sources src[9*G]
  * and velocity gradients du[16*G] at the current state (the reference's

@@ -87,3 +87,33 @@ def test_shock_tube_scenario_matches_the_reference(tmp_path):
     e = snap[:, 0].reshape(nx, ny, nz).transpose(2, 1, 0).ravel()
     ref = g["state"][0]
     assert np.max(np.abs(e - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("every", [1, 2])
+def test_seventeen_variable_snapshots(tmp_path, every):
+    """VH_WRITE_XY17 / VH_WRITE_FULL17 (NEWEST10/write.h): e, T, P, v, the ten
+    pi^{mu nu} and Pi per cell, x outer, y, then eta"""
+    cfg = C.glauber_config(nx=12, ny=10, nz=8, boost_invariant=False)
+    with C.make_hydro(cfg, C.glauber_inputs(cfg, b=4.0, seed=1)) as H:
+        H.step(3)
+        s = H.get_state()
+        p = H.get_primitive()
+        xy = os.path.join(str(tmp_path), "xy.bin")
+        full = os.path.join(str(tmp_path), "full.bin")
+        H.write(xy, A.WRITE_XY17, every)
+        H.write(full, A.WRITE_FULL17, every)
+    gx, gy, gz = cfg.gdims()
+    n = gx * gy * gz
+
+    def rec(i, j, k):
+        c = (k * gy + j) * gx + i
+        u0 = s[1, c]
+        return [s[0, c], p["T"][c], p["P"][c], s[2, c] / u0, s[3, c] / u0, s[4, c] / u0, *p["pi"][:, c], 0.0]
+
+    want_xy = [rec(i, j, (gz - 1) // 2) for i in range(3, 3 + cfg.nx, every) for j in range(3, 3 + cfg.ny, every)]
+    got_xy = np.fromfile(xy, dtype=np.float64).reshape(-1, 17)
+    assert np.array_equal(got_xy, np.array(want_xy))
+    want_full = [rec(i, j, k) for i in range(3, 3 + cfg.nx, every) for j in range(3, 3 + cfg.ny, every)
+                 for k in range(3, 3 + cfg.nz)]
+    got_full = np.fromfile(full, dtype=np.float64).reshape(-1, 17)
+    assert np.array_equal(got_full, np.array(want_full))

@@ -27,7 +27,7 @@ RECON_WENO5, RECON_MINMOD = 0, 1
 EOS_CONFORMAL, EOS_TABLE = 0, 1
 TAUPI_15_ETA_OVER_P, TAUPI_5_ETA_OVER_EPP = 0, 1
 PI_GIVEN, PI_ZERO, PI_NS = 0, 1, 2
-WRITE_XY, WRITE_FULL = 0, 1
+WRITE_XY, WRITE_FULL, WRITE_XY17, WRITE_FULL17 = 0, 1, 2, 3
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -100,6 +100,8 @@ SIGNATURES = [
     ("vh_batch_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("vh_batch_get_tuning", ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 5),
     ("vh_batch_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("vh_read_ideal_profile", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                             ctypes.c_int, _dp, _dp, _dp, _dp]),
     ("vh_eps_p", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("vh_adjoint_eps_p", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]),
     ("vh_adjoint_phase_times", ctypes.c_int, [ctypes.c_void_p, _dp]),

@@ -40,7 +40,10 @@ struct HostEos {
 }  // namespace
 
 extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
-  if (!h || !path || every < 1 || (layout != VH_WRITE_XY && layout != VH_WRITE_FULL)) return VH_E_ARG;
+  if (!h || !path || every < 1 || layout < VH_WRITE_XY || layout > VH_WRITE_FULL17) return VH_E_ARG;
+  const bool v17 = layout == VH_WRITE_XY17 || layout == VH_WRITE_FULL17;
+  const int NV = v17 ? 17 : 12;
+  if (v17) layout = layout == VH_WRITE_XY17 ? VH_WRITE_XY : VH_WRITE_FULL;
   vh_config cfg;
   std::vector<double> tab;
   int r = vh_internal_config(h, &cfg, &tab);
@@ -50,6 +53,12 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
   const long long n = (long long)gx * gy * gz;
   std::vector<double> f(18 * (size_t)n);
   if ((r = vh_get_state(h, f.data()))) return r;
+  // the 17-variable records take T, P and the full pi^{mu nu} from the device
+  std::vector<double> pT, pP, pi10;
+  if (v17) {
+    pT.resize(n); pP.resize(n); pi10.resize(10 * (size_t)n);
+    if ((r = vh_get_primitive(h, nullptr, pP.data(), pT.data(), nullptr, pi10.data()))) return r;
+  }
   HostEos eos;
   eos.kind = cfg.eos_kind;
   eos.a = cfg.eos_a;
@@ -71,10 +80,17 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
     o[3] = f[2 * n + c] / u0;
     o[4] = f[3 * n + c] / u0;
     o[5] = f[4 * n + c] / u0;
+    if (v17) {
+      o[1] = pT[c];
+      o[2] = pP[c];
+      for (int l = 0; l < 10; l++) o[6 + l] = pi10[(size_t)l * n + c];
+      o[16] = 0.0;  // bulk pressure is not evolved
+      return;
+    }
     for (int l = 0; l < 5; l++) o[6 + l] = f[(5 + l) * n + c];
     o[11] = 0.0;  // bulk pressure is not evolved
   };
-  const size_t R = 12 * sizeof(double);
+  const size_t R = NV * sizeof(double);
   std::vector<unsigned char> file;
   auto put = [&](size_t off, const double* src, size_t ndouble) {
     const size_t bytes = ndouble * sizeof(double);
@@ -86,21 +102,21 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
     // offset (gi/FREQ * (ny/FREQ)) records, central eta slice k0
     const int k0 = bi ? 0 : (gz - 1) / 2;
     const int ypts = ny / every;
-    const size_t chunk = (size_t)(12 * ny) / every;
-    std::vector<double> buf(12 * (size_t)(ny / every + 2), 0.0);
+    const size_t chunk = (size_t)(NV * ny) / every;
+    std::vector<double> buf(NV * (size_t)(ny / every + 2), 0.0);
     for (int i = 3; i < 3 + nx; i += every) {
       const int gi = i - 3;
-      for (int j = 3, jj = 0; j < 3 + ny; j += every, jj++) rec(i, j, k0, &buf[12 * (size_t)jj]);
+      for (int j = 3, jj = 0; j < 3 + ny; j += every, jj++) rec(i, j, k0, &buf[NV * (size_t)jj]);
       put((size_t)(gi / every) * ypts * R, buf.data(), chunk);
     }
   } else {
     // NEWEST5/write.h:204-290: per (x,y) column the eta records, at offset
     // (gi/FREQ * ypts * zpts + gj/FREQ * zpts) records
     const int ypts = ny / every, zpts = nzi;
-    std::vector<double> buf(12 * (size_t)nzi);
+    std::vector<double> buf(NV * (size_t)nzi);
     for (int i = 3; i < 3 + nx; i += every)
       for (int j = 3; j < 3 + ny; j += every) {
-        for (int k = kl, kk = 0; k < kl + nzi; k++, kk++) rec(i, j, k, &buf[12 * (size_t)kk]);
+        for (int k = kl, kk = 0; k < kl + nzi; k++, kk++) rec(i, j, k, &buf[NV * (size_t)kk]);
         put(((size_t)((i - 3) / every) * ypts * zpts + (size_t)((j - 3) / every) * zpts) * R, buf.data(), buf.size());
       }
   }
@@ -109,4 +125,44 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
   const size_t w = std::fwrite(file.data(), 1, file.size(), fp);
   std::fclose(fp);
   return w == file.size() ? VH_OK : VH_E_ARG;
+}
+
+// NEWideal/init.h:296-345: interior values read row by row (x fastest),
+// v -> u, and the floor applied over the whole grid.
+extern "C" int vh_read_ideal_profile(const char* eps_path, const char* vx_path, const char* vy_path, int nx, int ny,
+                                     double* e, double* ux, double* uy, double* min_out) {
+  if (!eps_path || !vx_path || !vy_path || !e || !ux || !uy || nx < 1 || ny < 1) return VH_E_ARG;
+  FILE* fe = std::fopen(eps_path, "r");
+  FILE* fx = std::fopen(vx_path, "r");
+  FILE* fy = std::fopen(vy_path, "r");
+  auto close_all = [&]() {
+    if (fe) std::fclose(fe);
+    if (fx) std::fclose(fx);
+    if (fy) std::fclose(fy);
+  };
+  if (!fe || !fx || !fy) { close_all(); return VH_E_ARG; }
+  const int gx = nx + 6, gy = ny + 6;
+  const size_t n = (size_t)gx * gy;
+  std::vector<double> vx(n, 0.0), vy(n, 0.0);
+  for (size_t c = 0; c < n; c++) e[c] = 0.0;
+  double mn = 100;
+  for (int j = 3; j < 3 + ny; j++)
+    for (int i = 3; i < 3 + nx; i++) {
+      const size_t c = (size_t)j * gx + i;
+      if (std::fscanf(fe, "%lf", &e[c]) != 1 || std::fscanf(fx, "%lf", &vx[c]) != 1 ||
+          std::fscanf(fy, "%lf", &vy[c]) != 1) {
+        close_all();
+        return VH_E_ARG;
+      }
+      if (e[c] < mn && std::fabs(e[c]) > 1e-5) mn = e[c];
+    }
+  close_all();
+  for (size_t c = 0; c < n; c++) {
+    if (e[c] < 0.01) e[c] = mn / 10;
+    const double g = 1.0 / std::sqrt(1.0 - vx[c] * vx[c] - vy[c] * vy[c]);
+    ux[c] = g * vx[c];
+    uy[c] = g * vy[c];
+  }
+  if (min_out) *min_out = mn;
+  return VH_OK;
 }

@@ -197,6 +197,17 @@ def eos_table_synthetic(n=2000, emin=1e-3, emax=500.0, a=A_QGP, hbarc=HBARC) -> 
     return t
 
 
+def read_ideal_profile(eps_path: str, vx_path: str, vy_path: str, nx: int, ny: int):
+    """e, u^x, u^y on the ghost-inclusive (nx+6)x(ny+6) grid from the ideal
+    driver's ASCII files, and the floor's min (vh_read_ideal_profile)."""
+    g = (nx + 6) * (ny + 6)
+    e, ux, uy = np.zeros(g), np.zeros(g), np.zeros(g)
+    mn = ctypes.c_double()
+    A.check(A.lib().vh_read_ideal_profile(eps_path.encode(), vx_path.encode(), vy_path.encode(), nx, ny, A.ptr(e),
+                                          A.ptr(ux), A.ptr(uy), ctypes.byref(mn)))
+    return e, ux, uy, mn.value
+
+
 def profile_gubser(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, t0_gev=0.6, a=A_QGP, hbarc=HBARC):
     gx, gy = nx + 6, ny + 6
     e = np.zeros(gx * gy); ux = np.zeros_like(e); uy = np.zeros_like(e); pu = np.zeros(4 * gx * gy)
