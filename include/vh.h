@@ -116,6 +116,25 @@ int vh_get_state_device(vh_handle* h, double* dev);
  * may be NULL. */
 int vh_get_primitive(vh_handle* h, double* e, double* P, double* T, double* u4, double* pi10);
 
+/* Landau matching (NEWEST5/ginit.h:521-656, FindVar): for each of n cells
+ * the timelike eigenvector u^mu (u_mu u^mu = 1) of T^mu_nu and its
+ * eigenvalue e, from the contravariant T^{mu nu} given as 10 x n doubles
+ * (tt, tx, ty, t-eta, xx, xy, x-eta, yy, y-eta, eta-eta) at time tau (Milne
+ * metric diag(1,-1,-1,-tau^2); Cartesian when cartesian != 0).  Outputs e
+ * (n) and u (4 x n); *nfail (may be NULL) counts the cells without a
+ * timelike eigenpair (where the reference exits).  Runs on the current GPU;
+ * the arrays are host memory. */
+int vh_landau_match(const double* tmunu10, long long n, double tau, int cartesian, double* e, double* u4,
+                    long long* nfail);
+/* Initial state from T^{mu nu} on the handle's ghost-inclusive grid (10 x n
+ * host doubles as above), as the reference's Glasma initialisation builds it
+ * (NEWEST5/ginit.h:658-1052): Landau matching, P(e) from the EOS, the five
+ * evolved components of pi^{mu nu} = T^{mu nu} - (e+P) u^mu u^nu + P g^{mu nu}
+ * (the trace part, a bulk pressure, is not evolved and is dropped),
+ * prevu = u, T^{tau mu} from (e, u, pi).  VH_E_ROOTFIND, with *nfail > 0,
+ * when some cell has no timelike eigenpair. */
+int vh_init_tmunu(vh_handle* h, double tau, const double* tmunu10, long long* nfail);
+
 /* Initialise from a profile (the reference's init(tau, ts) with a scenario,
  * NEWEST5/init.h:556-704): e, u^x, u^y, u^eta on the ghost-inclusive grid
  * (u^tau from normalisation), optional previous velocity prevu (4 fields;

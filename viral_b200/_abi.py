@@ -58,6 +58,9 @@ SIGNATURES = [
     ("vh_set_state_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]),
     ("vh_get_state_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("vh_get_primitive", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]),
+    ("vh_landau_match", ctypes.c_int, [_dp, ctypes.c_longlong, ctypes.c_double, ctypes.c_int, _dp, _dp,
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+    ("vh_init_tmunu", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("vh_init_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, _dp]),
     ("vh_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("vh_get_time", ctypes.c_int, [ctypes.c_void_p, _dp]),

@@ -321,6 +321,68 @@ extern "C" int vh_get_primitive(vh_handle* h, double* e, double* P, double* T, d
   return VH_OK;
 }
 
+extern "C" int vh_landau_match(const double* tmunu10, long long n, double tau, int cartesian, double* e, double* u4,
+                               long long* nfail) {
+  if (!tmunu10 || !e || !u4 || n < 1 || (!cartesian && !(tau > 0))) return VH_E_ARG;
+  double* d = nullptr;
+  unsigned long long* cnt = nullptr;
+  const size_t nb = sizeof(double) * (size_t)n;
+  if (cudaMalloc(&d, 15 * nb) != cudaSuccess) {
+    g_create_err = "vh_landau_match: device buffers";
+    return VH_E_NOMEM;
+  }
+  if (cudaMalloc(&cnt, sizeof(unsigned long long)) != cudaSuccess) {
+    cudaFree(d);
+    g_create_err = "vh_landau_match: device buffers";
+    return VH_E_NOMEM;
+  }
+  unsigned long long bad = 0;
+  cudaError_t err = cudaMemcpy(d, tmunu10, 10 * nb, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemset(cnt, 0, sizeof(bad));
+  if (err == cudaSuccess) {
+    k_landau<double><<<grid1(n, 128), 128>>>(n, tau, cartesian, d, d + 10 * n, d + 11 * n, cnt);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMemcpy(e, d + 10 * n, nb, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess) err = cudaMemcpy(u4, d + 11 * n, 4 * nb, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess) err = cudaMemcpy(&bad, cnt, sizeof(bad), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  cudaFree(cnt);
+  if (err != cudaSuccess) {
+    g_create_err = std::string("vh_landau_match: ") + cudaGetErrorString(err);
+    return VH_E_CUDA;
+  }
+  if (nfail) *nfail = (long long)bad;
+  return VH_OK;
+}
+
+extern "C" int vh_init_tmunu(vh_handle* h, double tau, const double* tmunu10, long long* nfail) {
+  if (!h || !tmunu10) return VH_E_ARG;
+  if (!h->C.cart && !(tau > 0)) return fail(h, VH_E_ARG, "Milne tau must be positive");
+  const long long n = h->C.n;
+  double* buf = h->stage;  // 18 x n doubles; the tensor takes 10
+  VH_CUDA(h, cudaMemcpyAsync(buf, tmunu10, 10 * sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+  VH_CUDA(h, cudaMemsetAsync(h->red, 0, sizeof(unsigned long long), h->stream));
+  if (h->mixed) {
+    k_init_tmunu<float><<<grid1(n, 128), 128, 0, h->stream>>>(h->C, h->pf, tau, buf, h->red);
+    k_fill_tmunu<float><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pf, tau);
+  } else {
+    k_init_tmunu<double><<<grid1(n, 128), 128, 0, h->stream>>>(h->C, h->pd, tau, buf, h->red);
+    k_fill_tmunu<double><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pd, tau);
+  }
+  VH_CUDA(h, cudaGetLastError());
+  unsigned long long bad = 0;
+  VH_CUDA(h, cudaMemcpyAsync(&bad, h->red, sizeof(bad), cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(unsigned int), h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->tau = tau;
+  h->have_state = true;
+  if (nfail) *nfail = (long long)bad;
+  if (bad) return fail(h, VH_E_ROOTFIND, "Landau matching found no timelike eigenvector in " + std::to_string(bad) +
+                                             " cell(s)");
+  return VH_OK;
+}
+
 extern "C" int vh_max_temperature(vh_handle* h, double* tmax_gev) {
   if (!h || !tmax_gev) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");

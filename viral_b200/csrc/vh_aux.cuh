@@ -55,6 +55,109 @@ __global__ void k_primitive(DevCfg C, DevPtrs<R> P, double tau, double* out) {
   for (int l = 0; l < 10; l++) out[(7 + l) * n + c] = (double)pi10[l];
 }
 
+// Landau matching of one cell (NEWEST5/ginit.h:521-656): the timelike
+// eigenvector u of T^mu_nu = T^{mu a} g_{a nu} and its eigenvalue e.  The
+// reference takes all four eigenpairs from GSL and keeps the one real pair
+// with |v| < 1; here Rayleigh-quotient iteration starts from the flow of
+// energy u ~ T^{tau mu} (the timelike pair is the one it reaches for any
+// tensor with e > |p_i|), with the 4x4 solves of the root-find.  Returns
+// false when the iteration leaves the light cone or does not converge.
+VH_HD inline bool landau_cell(const double* T10, double tau, bool cart, double& e, double* u) {
+  const double t2 = cart ? 1.0 : tau * tau;
+  const double g[4] = {1.0, -1.0, -1.0, -t2};
+  const int I[4][4] = {{0, 1, 2, 3}, {1, 4, 5, 6}, {2, 5, 7, 8}, {3, 6, 8, 9}};
+  double M[4][4];
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) M[a][b] = T10[I[a][b]] * g[b];
+  auto lnorm = [&](const double* x) { return x[0] * x[0] - x[1] * x[1] - x[2] * x[2] - t2 * x[3] * x[3]; };
+  auto rayleigh = [&](const double* x) {
+    double s = 0;
+    for (int a = 0; a < 4; a++) {
+      double r = 0;
+      for (int b = 0; b < 4; b++) r += M[a][b] * x[b];
+      s += g[a] * x[a] * r;
+    }
+    return s;
+  };
+  double x[4] = {T10[0], T10[1], T10[2], T10[3]};
+  double nn = lnorm(x);
+  if (!(nn > 0) || !(x[0] > 0)) { x[0] = 1; x[1] = x[2] = x[3] = 0; nn = 1; }
+  const double in = 1.0 / sqrt(nn);
+  for (int a = 0; a < 4; a++) u[a] = x[a] * in;
+  double sig = rayleigh(u);
+  bool conv = false;
+  for (int it = 0; it < 60 && !conv; it++) {
+    double A[4][4], y[4] = {u[0], u[1], u[2], u[3]};
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++) A[a][b] = M[a][b] - (a == b ? sig : 0.0);
+    if (!solve4(A, y)) { conv = true; break; }  // sig is an eigenvalue to working precision
+    const double ny = lnorm(y);
+    if (!(ny > 0)) return false;
+    const double s = (y[0] > 0 ? 1.0 : -1.0) / sqrt(ny);
+    double d = 0;
+    for (int a = 0; a < 4; a++) {
+      const double v = y[a] * s;
+      d = fmax(d, fabs(v - u[a]));
+      u[a] = v;
+    }
+    sig = rayleigh(u);
+    if (d <= 1e-15 * fabs(u[0])) conv = true;
+  }
+  if (!conv) return false;
+  // the pair must be an eigenpair: |M u - e u| small against e u^tau
+  double res = 0;
+  for (int a = 0; a < 4; a++) {
+    double r = -sig * u[a];
+    for (int b = 0; b < 4; b++) r += M[a][b] * u[b];
+    res = fmax(res, fabs(r));
+  }
+  e = sig;
+  return u[0] >= 1.0 && e > 0 && res <= 1e-10 * fabs(e) * u[0];
+}
+
+template <class R>
+__global__ void k_landau(long long n, double tau, int cart, const double* T10, double* e, double* u4,
+                         unsigned long long* nfail) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double t[10], ee = 0, u[4] = {1, 0, 0, 0};
+#pragma unroll
+  for (int l = 0; l < 10; l++) t[l] = T10[(long long)l * n + c];
+  if (!landau_cell(t, tau, cart != 0, ee, u)) atomicAdd(nfail, 1ull);
+  e[c] = ee;
+#pragma unroll
+  for (int l = 0; l < 4; l++) u4[(long long)l * n + c] = u[l];
+}
+
+// Initial state from T^{mu nu} on every cell: Landau matching, then
+// pi^{mu nu} = T^{mu nu} - (e + P) u^mu u^nu + P g^{mu nu} (its five evolved
+// components), prevu = u; T^{tau mu} follows from k_fill_tmunu.
+template <class R>
+__global__ void k_init_tmunu(DevCfg C, DevPtrs<R> P, double tau, const double* T10, unsigned long long* nfail) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = C.n;
+  if (c >= n) return;
+  double t[10], e = 0, u[4] = {1, 0, 0, 0};
+#pragma unroll
+  for (int l = 0; l < 10; l++) t[l] = T10[(long long)l * n + c];
+  if (!landau_cell(t, tau, C.cart, e, u)) atomicAdd(nfail, 1ull);
+  double Pp, cs2, Te;
+  eos_all<double>(C, e, Pp, cs2, Te);
+  const double t2 = C.cart ? 1.0 : tau * tau;
+  // evolved components xx, yy, xy, x-eta, y-eta at T10 indices 4, 7, 5, 6, 8
+  const int q[5] = {4, 7, 5, 6, 8}, a5[5] = {1, 2, 1, 1, 2}, b5[5] = {1, 2, 2, 3, 3};
+  const double gi[4] = {1.0, -1.0, -1.0, -1.0 / t2};
+  P.e()[c] = (R)e;
+#pragma unroll
+  for (int l = 0; l < 4; l++) { P.u(l)[c] = (R)u[l]; P.pu(l)[c] = (R)u[l]; }
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const int a = a5[k], b = b5[k];
+    const double pi = t[q[k]] - (e + Pp) * u[a] * u[b] + (a == b ? Pp * gi[a] : 0.0);
+    P.A(4 + k)[c] = (R)pi;
+  }
+}
+
 // Velocity gradients with the coverage the reference's CalcDer4Vel has
 // (NEWEST5/Source.h:3-101): d_tau on the interior; d_x for i in [2, gx-3]
 // on interior (j,k); d_y likewise; d_eta for every k on interior (i,j) with

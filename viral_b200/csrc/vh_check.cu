@@ -7,6 +7,7 @@
 
 #include "vh.h"
 #include "vh_adjoint.cuh"
+#include "vh_aux.cuh"
 
 using namespace vh;
 
@@ -90,6 +91,9 @@ void vhc_obs_cell(const vh_config* c, double e, double u1, double u2, double p1,
 void vhc_obs_cell_vjp(const vh_config* c, double e, double u1, double u2, double N, double D, double* g5) {
   HostCfg h = make_cfg(c);
   obs_cell_vjp<double>(h.C, e, u1, u2, N, D, g5[0], g5[1], g5[2], g5[3], g5[4]);
+}
+int vhc_landau(const double* T10, double tau, int cart, double* e, double* u4) {
+  return landau_cell(T10, tau, cart != 0, *e, u4) ? 1 : 0;
 }
 void vhc_eos_d(const vh_config* c, double e, double* out4) {
   HostCfg h = make_cfg(c);

@@ -114,6 +114,14 @@ class Hydro:
         self._chk(A.lib().vh_get_primitive(self.h, A.ptr(e), A.ptr(P), A.ptr(T), A.ptr(u), A.ptr(pi)))
         return dict(e=e, P=P, T=T, u=u, pi=pi)
 
+    def init_tmunu(self, tau: float, tmunu10: np.ndarray) -> int:
+        """state from T^{mu nu} (10, n) by Landau matching; returns the cells
+        without a timelike eigenpair (raises when there are any)"""
+        t = np.ascontiguousarray(tmunu10, dtype=np.float64).reshape(10, self.n)
+        nf = ctypes.c_longlong()
+        self._chk(A.lib().vh_init_tmunu(self.h, tau, A.ptr(t), ctypes.byref(nf)))
+        return nf.value
+
     def init_profile(self, tau, e, ux, uy, ueta=None, prevu=None, pi_mode=A.PI_ZERO, pi5=None):
         c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
         self._chk(A.lib().vh_init_profile(self.h, tau, A.ptr(c(e)), A.ptr(c(ux)), A.ptr(c(uy)), A.ptr(c(ueta)),
@@ -195,6 +203,17 @@ def eos_table_synthetic(n=2000, emin=1e-3, emax=500.0, a=A_QGP, hbarc=HBARC) -> 
     A.check(A.lib().vh_eos_table_synthetic(n, emin, emax, a, hbarc, A.ptr(t[0]), A.ptr(t[1]), A.ptr(t[2]),
                                            A.ptr(t[3])))
     return t
+
+
+def landau_match(tmunu10: np.ndarray, tau: float, cartesian: bool = False):
+    """e (n,), u (4, n) and the failure count of the Landau matching of
+    T^{mu nu} (10, n) on the GPU (vh_landau_match)"""
+    t = np.ascontiguousarray(tmunu10, dtype=np.float64)
+    n = t.shape[1]
+    e, u = np.zeros(n), np.zeros((4, n))
+    nf = ctypes.c_longlong()
+    A.check(A.lib().vh_landau_match(A.ptr(t), n, tau, int(cartesian), A.ptr(e), A.ptr(u), ctypes.byref(nf)))
+    return e, u, nf.value
 
 
 def read_ideal_profile(eps_path: str, vx_path: str, vy_path: str, nx: int, ny: int):
