@@ -240,9 +240,9 @@ def algorithmic_bytes(cfg, kernel: str) -> float:
 # scaled to a full launch by the cells processed
 MEASURED_TRAFFIC_PER_CELL = {
     ("fp64", "k_dir_x"): 150.0, ("fp64", "k_dir_y"): 239.0, ("fp64", "k_dir_eta"): 261.0,
-    ("fp64", "k_update_stage2"): 651.0,
+    ("fp64", "k_update_stage1"): 663.0, ("fp64", "k_update_stage2"): 651.0,
     ("mixed", "k_dir_x"): 63.0, ("mixed", "k_dir_y"): 104.0, ("mixed", "k_dir_eta"): 114.0,
-    ("mixed", "k_update_stage2"): 223.0,
+    ("mixed", "k_update_stage1"): 200.0, ("mixed", "k_update_stage2"): 223.0,
 }
 
 

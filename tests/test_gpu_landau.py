@@ -69,8 +69,12 @@ def test_init_tmunu_round_trip(which):
         assert H2.init_tmunu(tau, T) == 0
         s2 = H2.get_state()
         assert abs(H2.tau - tau) < 1e-15
+    # interior cells (the Gubser test's mirrored ghosts hold a u^tau that is
+    # not the normalisation of their u^x, u^y: no fluid tensor there)
+    from helpers import interior_mask
+    m = interior_mask(cfg)
     for grp in ((0,), (1, 2, 3, 4), (5, 6, 7, 8, 9), (10, 11, 12, 13)):
-        scale = max(np.max(np.abs(s[q])) for q in grp)
+        scale = max(np.max(np.abs(s[q][m])) for q in grp)
         for q in grp:
-            assert np.max(np.abs(s2[q] - s[q])) <= 1e-11 * scale, q
+            assert np.max(np.abs(s2[q][m] - s[q][m])) <= 1e-11 * scale, q
     assert np.array_equal(s2[14:18], s2[1:5])  # prevu = u
