@@ -420,13 +420,21 @@ def ensemble(args):
     floor = C.ENSEMBLE_FLOOR_GEV if args.ensemble_floor is None else args.ensemble_floor
     npart = B.init_glauber(seeds=np.arange(n), bimp=bimp, efloor_gev=floor)
     t_init = time.perf_counter() - t_init
+    _, ecc2_initial = B.observables()
     cache = os.path.join(tempfile.gettempdir(), "vh_batch_tuning.txt")
     tune_ms = B.autotune(cache, probe_steps=16)
     tuning = B.tuning()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         sec, graph = B.run(max_steps)
     tau, nst, st = B.events()
+    eps_p_final, _ = B.observables()
     B.close()
+    okev = st != 3
+    observables = {"eps2_initial_mean": float(np.mean(ecc2_initial)),
+                   "eps_p_final_mean": float(np.mean(eps_p_final[okev])),
+                   "corr_eps2_eps_p": float(np.corrcoef(ecc2_initial[okev], eps_p_final[okev])[0, 1]),
+                   "what": "eccentricity of the initial energy density and momentum anisotropy where each event "
+                           "stopped (failed events excluded), vh_batch_observables"}
     cells = (sides.astype(np.int64) ** 2)
     batch_events_s = n / sec
     batch_cells_s = float(np.sum(cells * nst)) / sec
@@ -456,7 +464,7 @@ def ensemble(args):
            "steps": {"mean": float(np.mean(nst)), "min": int(nst.min()), "max": int(nst.max())},
            "stopped": {"frozen_out": int(np.sum(st == 1)), "tau_max": int(np.sum(st == 2)),
                        "failed": int(np.sum(st == 3)), "running": int(np.sum(st == 0))},
-           "npart_mean": float(np.mean(npart)),
+           "npart_mean": float(np.mean(npart)), "observables": observables,
            "failed_events": [{"event": int(e), "side": int(sides[e]), "b": round(float(bimp[e]), 3),
                               "steps": int(nst[e])} for e in np.where(st == 3)[0][:64]],
            "loop_fp64": {"events_per_s": n / loop_seconds, "seconds_per_event_by_side": per_side,

@@ -262,6 +262,12 @@ int vh_batch_autotune(vh_batch* b, const char* cache_path, int probe_steps, doub
 int vh_batch_set_tuning(vh_batch* b, int variant, int steps_per_launch, int use_graph);
 int vh_batch_get_tuning(vh_batch* b, int* variant, int* steps_per_launch, int* lines_per_tile, int* blocks_per_sm,
                         int* unroll);
+/* Per-event observables of the events' current states (no counterpart in
+ * the reference, which only evolves): the momentum anisotropy eps_p (as
+ * vh_eps_p) and the eccentricity of the energy density about its centre,
+ * eps_2 = sqrt((<y^2> - <x^2>)^2 + 4 <xy>^2) / (<x^2> + <y^2>); n doubles
+ * each, either may be NULL. */
+int vh_batch_observables(vh_batch* b, double* eps_p, double* ecc2);
 const char* vh_batch_last_error(const vh_batch* b);
 
 /* ------------------------------------------------------------- adjoint

@@ -119,3 +119,34 @@ def test_autotune_picks_a_compiled_variant(tmp_path):
         # a second tuning with the same key reads the cache
         assert B.autotune(cache, probe_steps=8) < 0
         assert "=" in open(cache).read()
+
+
+def test_per_event_observables():
+    """eps_p of every batched event equals vh_eps_p of the same event stepped
+    alone; eps_2 equals the energy-density eccentricity of its state"""
+    cfg = C.glauber_config(nx=8, ny=8, boost_invariant=True)
+    sides, bimp = [30, 41, 26], [6.0, 9.0, 3.0]
+    steps = 10
+    with Batch(cfg, sides, tau0=cfg.tau0, dtau=cfg.dtau, tau_max=100.0, t_freeze_gev=0.0) as B:
+        B.init_glauber(seeds=[4, 5, 6], bimp=bimp)
+        ep0, e20 = B.observables()
+        B.run(steps)
+        ep, e2 = B.observables()
+        states = [B.event_state(ev) for ev in range(3)]
+    for ev, (side, b) in enumerate(zip(sides, bimp)):
+        c = C.glauber_config(nx=side, ny=side, boost_invariant=True)
+        with C.make_hydro(c, C.glauber_inputs(c, b=b, seed=4 + ev)) as H:
+            assert abs(H.eps_p() - ep0[ev]) <= 1e-12 * max(abs(ep0[ev]), 1e-3)
+            H.step(steps)
+            assert abs(H.eps_p() - ep[ev]) <= 1e-12 * max(abs(ep[ev]), 1e-3)
+        g = side + 6
+        e = states[ev][0].reshape(g, g)[3:3 + side, 3:3 + side]
+        yy, xx = np.meshgrid(np.arange(side) * 0.1, np.arange(side) * 0.1, indexing="ij")
+        E = e.sum()
+        xm, ym = (e * xx).sum() / E, (e * yy).sum() / E
+        sxx = (e * xx * xx).sum() / E - xm * xm
+        syy = (e * yy * yy).sum() / E - ym * ym
+        sxy = (e * xx * yy).sum() / E - xm * ym
+        want = np.sqrt((syy - sxx) ** 2 + 4 * sxy ** 2) / (sxx + syy)
+        assert abs(e2[ev] - want) <= 1e-10 * want
+    assert np.all(np.abs(ep0) < 1e-12)  # at rest with pi = 0: T^xx = T^yy = P

@@ -83,6 +83,13 @@ class Batch:
         _chk(A.lib().vh_batch_get_event_state(self.h, ev, A.ptr(f)), self.h)
         return f
 
+    def observables(self):
+        """per-event momentum anisotropy eps_p and eccentricity eps_2 of the
+        current states"""
+        ep, e2 = np.zeros(self.n), np.zeros(self.n)
+        _chk(A.lib().vh_batch_observables(self.h, A.ptr(ep), A.ptr(e2)), self.h)
+        return ep, e2
+
     def autotune(self, cache_path=None, probe_steps=16) -> float:
         ms = ctypes.c_double()
         _chk(A.lib().vh_batch_autotune(self.h, cache_path.encode() if cache_path else None, probe_steps,

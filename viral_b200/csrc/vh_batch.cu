@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "vh.h"
+#include "vh_adjoint.cuh"
 #include "vh_aux.cuh"
 
 using namespace vh;
@@ -701,6 +702,70 @@ extern "C" int vh_batch_autotune(vh_batch* b, const char* cache_path, int probe_
   if (cache_path && best < 1e300) {
     std::ofstream out(cache_path, std::ios::app);
     out << key.str() << "=" << best_v << "," << best_s << "\n";
+  }
+  return VH_OK;
+}
+
+// Per-event observables of the current states, one block per event, FP64
+// sums in a fixed order: the momentum anisotropy
+// eps_p = sum(T^xx - T^yy) / sum(T^xx + T^yy) and the eccentricity of the
+// energy density about its centre,
+// eps_2 = sqrt((<y^2> - <x^2>)^2 + 4 <xy>^2) / (<x^2> + <y^2>).
+template <class R>
+__global__ void __launch_bounds__(256) k_batch_obs(DevCfg C0, DevPtrs<R> pool, const long long* off, const int* nx,
+                                                   const int* ny, double* out) {
+  const int ev = blockIdx.x;
+  const DevCfg C = event_cfg(C0, nx[ev], ny[ev]);
+  const DevPtrs<R> P = pool.shifted(off[ev]);
+  const long long nint = (long long)C.nx * C.ny;
+  double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // N, D, sum e, e x, e y, e x^2, e y^2, e x y
+  for (long long t = threadIdx.x; t < nint; t += blockDim.x) {
+    const int i = (int)(t % C.nx), j = (int)(t / C.nx);
+    const long long c = cix(C, C.il + i, C.jl + j, 0);
+    const R e = P.e()[c];
+    double num, den;
+    obs_cell<R>(C, e, P.u(1)[c], P.u(2)[c], P.A(4)[c], P.A(5)[c], num, den);
+    const double x = i * C.dx, y = j * C.dy, ed = (double)e;
+    s[0] += num; s[1] += den; s[2] += ed; s[3] += ed * x; s[4] += ed * y;
+    s[5] += ed * x * x; s[6] += ed * y * y; s[7] += ed * x * y;
+  }
+  __shared__ double sh[8][256];
+#pragma unroll
+  for (int q = 0; q < 8; q++) sh[q][threadIdx.x] = s[q];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+#pragma unroll
+      for (int q = 0; q < 8; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double E = sh[2][0], xm = sh[3][0] / E, ym = sh[4][0] / E;
+    const double xx = sh[5][0] / E - xm * xm, yy = sh[6][0] / E - ym * ym, xy = sh[7][0] / E - xm * ym;
+    out[2 * ev] = sh[0][0] / sh[1][0];
+    out[2 * ev + 1] = sqrt((yy - xx) * (yy - xx) + 4 * xy * xy) / (xx + yy);
+  }
+}
+
+extern "C" int vh_batch_observables(vh_batch* b, double* eps_p, double* ecc2) {
+  if (!b) return VH_E_ARG;
+  double* d = nullptr;
+  VB_CUDA(b, cudaMalloc(&d, sizeof(double) * 2 * b->n));
+  if (b->mixed)
+    k_batch_obs<float><<<b->n, 256>>>(b->C0, pool_ptrs<float>(b), b->d_off, b->d_nx, b->d_ny, d);
+  else
+    k_batch_obs<double><<<b->n, 256>>>(b->C0, pool_ptrs<double>(b), b->d_off, b->d_nx, b->d_ny, d);
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> h(2 * (size_t)b->n);
+  if (e == cudaSuccess) e = cudaMemcpy(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    b->err = std::string("vh_batch_observables: ") + cudaGetErrorString(e);
+    return VH_E_CUDA;
+  }
+  for (int ev = 0; ev < b->n; ev++) {
+    if (eps_p) eps_p[ev] = h[2 * ev];
+    if (ecc2) ecc2[ev] = h[2 * ev + 1];
   }
   return VH_OK;
 }
