@@ -56,7 +56,9 @@ class Batch:
                                          pi_mode, A.ptr(c(pi5))), self.h)
 
     def init_glauber(self, seeds, bimp, A_nuc=208, R=6.62, aws=0.546, dmin=0.4, sigma_nn=6.4, w=0.5,
-                     epeak_gev=40.0, efloor_gev=0.04, nthreads=0):
+                     epeak_gev=40.0, efloor_gev=None, nthreads=0):
+        if efloor_gev is None:
+            from .configs import GLAUBER_FLOOR_GEV as efloor_gev
         s = np.ascontiguousarray(seeds, dtype=np.uint64)
         b = np.ascontiguousarray(bimp, dtype=np.float64)
         npart = np.zeros(self.n, dtype=np.int32)

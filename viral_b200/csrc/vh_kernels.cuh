@@ -96,6 +96,80 @@ __device__ inline void recon_lr(const DevCfg& C, const R* q, int s, R& L, R& Rr)
   }
 }
 
+// Paired FP32 arithmetic (sm_100's f32x2 add/mul/fma: one instruction for
+// two lanes of a 64-bit register pair).  The FP32 sweeps reconstruct the
+// flux F^l and the conserved variable V^l of a face together, so the WENO5
+// arithmetic of the pair runs at half the instruction count; each lane
+// rounds as the scalar operation would.
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float a, float b) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ F2 f2s(float a) { return f2(a, a); }
+__device__ __forceinline__ void f2u(F2 x, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+}
+__device__ __forceinline__ F2 add2(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+// weno_lr for two quantities at once (same formulas as weno_beta/weno_lr)
+__device__ __forceinline__ void weno_lr2(F2 qm2, F2 qm1, F2 qc, F2 qp1, F2 qp2, F2& L, F2& Rr) {
+  const F2 c13 = f2s((float)(13. / 12.)), q4 = f2s(0.25f), two = f2s(2.f), m2 = f2s(-2.f), three = f2s(3.f),
+           m4 = f2s(-4.f), five = f2s(5.f), m7 = f2s(-7.f), eleven = f2s(11.f), eps = f2s(1e-6f);
+  F2 a = add2(fma2(m2, qp1, qc), qp2), c = add2(fma2(m4, qp1, mul2(three, qc)), qp2);
+  const F2 b0 = fma2(c13, mul2(a, a), mul2(q4, mul2(c, c)));
+  a = add2(fma2(m2, qc, qm1), qp1);
+  c = sub2(qm1, qp1);
+  const F2 b1 = fma2(c13, mul2(a, a), mul2(q4, mul2(c, c)));
+  a = add2(fma2(m2, qm1, qm2), qc);
+  c = fma2(three, qc, fma2(m4, qm1, qm2));
+  const F2 b2 = fma2(c13, mul2(a, a), mul2(q4, mul2(c, c)));
+  const F2 e0 = add2(eps, b0), e1 = add2(eps, b1), e2 = add2(eps, b2);
+  const F2 E0 = mul2(e0, e0), E1 = mul2(e1, e1), E2 = mul2(e2, e2);
+  const F2 P12 = mul2(E1, E2), P02 = mul2(E0, E2), P01 = mul2(E0, E1);
+  const F2 nl0 = mul2(f2s(0.3f), P12), nl1 = mul2(f2s(0.6f), P02), nl2 = mul2(f2s(0.1f), P01);
+  const F2 nr0 = mul2(f2s(0.1f), P12), nr2 = mul2(f2s(0.3f), P01);
+  const F2 ql0 = sub2(fma2(five, qp1, mul2(two, qc)), qp2);
+  const F2 ql1 = fma2(two, qp1, fma2(five, qc, sub2(f2s(0.f), qm1)));
+  const F2 ql2 = fma2(eleven, qc, fma2(m7, qm1, mul2(two, qm2)));
+  const F2 qr0 = fma2(two, qp2, fma2(m7, qp1, mul2(eleven, qc)));
+  const F2 qr1 = sub2(fma2(five, qc, mul2(two, qm1)), qp1);
+  const F2 qr2 = fma2(two, qc, fma2(five, qm1, sub2(f2s(0.f), qm2)));
+  const F2 numl = fma2(nl2, ql2, fma2(nl1, ql1, mul2(nl0, ql0)));
+  const F2 numr = fma2(nr2, qr2, fma2(nl1, qr1, mul2(nr0, qr0)));
+  const F2 six = f2s(6.f);
+  const F2 denl = mul2(six, add2(add2(nl0, nl1), nl2)), denr = mul2(six, add2(add2(nr0, nl1), nr2));
+  float a0, a1, d0, d1;
+  f2u(numl, a0, a1);
+  f2u(denl, d0, d1);
+  L = f2(__fdividef(a0, d0), __fdividef(a1, d1));
+  f2u(numr, a0, a1);
+  f2u(denr, d0, d1);
+  Rr = f2(__fdividef(a0, d0), __fdividef(a1, d1));
+}
+
 template <class R>
 __device__ inline R shfl_dn(R v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 template <class R>
@@ -190,8 +264,27 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   for (int l = 0; l < 9; l++) {
     R fl = 0, fr = 0, vl = 0, vr = 0;
     if (stencil) {
-      recon_lr<R>(C, sm.q[l], s, fl, fr);
-      recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
+      if constexpr (sizeof(R) == 4) {
+        if (C.recon == 0) {
+          // F^l and V^l of the stencil reconstructed as one pair
+          const float* qa = reinterpret_cast<const float*>(sm.q[l]);
+          const float* qb = reinterpret_cast<const float*>(sm.q[9 + l]);
+          F2 L2, R2;
+          weno_lr2(f2(qa[s - 2], qb[s - 2]), f2(qa[s - 1], qb[s - 1]), f2(qa[s], qb[s]), f2(qa[s + 1], qb[s + 1]),
+                   f2(qa[s + 2], qb[s + 2]), L2, R2);
+          float a, b;
+          f2u(L2, a, b);
+          fl = a; vl = b;
+          f2u(R2, a, b);
+          fr = a; vr = b;
+        } else {
+          recon_lr<R>(C, sm.q[l], s, fl, fr);
+          recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
+        }
+      } else {
+        recon_lr<R>(C, sm.q[l], s, fl, fr);
+        recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
+      }
     }
     fr = shfl_dn<R>(fr, 1);
     vr = shfl_dn<R>(vr, 1);

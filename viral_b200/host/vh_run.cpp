@@ -48,7 +48,7 @@ struct Options {
   std::string out;          // snapshot directory ("" = no snapshots)
   double b = 7.0;
   unsigned long long seed = 0;
-  double floor_gev = 0.04;
+  double floor_gev = 0.2;    // GeV/fm^3, the library workloads' Glauber floor
   bool quiet = false;
 };
 
