@@ -40,9 +40,12 @@ def test_landau_match_reports_failures():
 
 
 def tmunu_of(p, tau, cart=False):
+    """the fluid tensor of (e, P, u, pi), with u^tau the normalisation of the
+    spatial u (the Gubser test's mirrored ghost cells store another u^tau)"""
     t2 = 1.0 if cart else tau * tau
     gi = [1.0, -1.0, -1.0, -1.0 / t2]
-    u = p["u"]
+    u = p["u"].copy()
+    u[0] = np.sqrt(1 + u[1] ** 2 + u[2] ** 2 + t2 * u[3] ** 2)
     out = np.zeros((10, u.shape[1]))
     for q, (a, b) in enumerate(IDX):
         out[q] = (p["e"] + p["P"]) * u[a] * u[b] + p["pi"][q] - (p["P"] * gi[a] if a == b else 0.0)

@@ -524,15 +524,18 @@ VH_HD inline bool solve4(double A[4][4], double b[4]) {
   return true;
 }
 
-// Newton with norm-reducing step control and the reference's stopping rule
-// (|dx_i| < 1e-16 |x_i| or dx_i = 0 for all i, at most 100 iterations;
-// NEWEST5/multiroot.h:389-422).  A step that raises |f| is shortened by
-// t = (sqrt(1+6r)-1)/(3r), r = |f_new|^2/|f_old|^2, at most 64 times.
-// Returns the iteration count, or -1 on failure.
-// rtol = 1e-16 is the reference's rule; the mixed step, which stores the
-// result in single precision, stops at rtol = 1e-10.  The Jacobian is
-// formed together with the residual at every trial point, so an accepted
-// full step (the common case) costs one evaluation.
+// Newton with norm-reducing step control and the reference's form of
+// stopping rule (|dx_i| < rtol |x_i| or dx_i = 0 for all i, at most 100
+// iterations; NEWEST5/multiroot.h:389-422, where rtol = 1e-16).  A step that
+// raises |f| is shortened by t = (sqrt(1+6r)-1)/(3r), r = |f_new|^2/|f_old|^2,
+// at most 64 times.  Returns the iteration count, or -1 on failure.
+// The step stops at rtol = 1e-13 in FP64 and 1e-10 in the mixed mode (which
+// stores the result in single precision).  Newton converges quadratically,
+// so an iterate reached by a step below 1e-13 relative is the root to
+// rounding; the reference's 1e-16 mostly waits for steps that round to zero
+// (about 1.5 more iterations per cell, and warps wait for their slowest
+// cell).  The Jacobian is formed together with the residual at every trial
+// point, so an accepted full step (the common case) costs one evaluation.
 VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, double tau, double* x,
                                double rtol = 1e-16) {
   const double t2 = C.cart ? 1.0 : tau * tau;

@@ -461,7 +461,7 @@ __device__ __forceinline__ unsigned root_cell(const DevCfg& C, const DevPtrs<R>&
     for (int l = 0; l < 4; l++) Tt[l] = (double)q9[l];
 #pragma unroll
     for (int l = 0; l < 5; l++) pd[l] = (double)q9[4 + l];
-    const int it = con2prim(C, Tt, pd, tau1, x, sizeof(R) == 4 ? 1e-10 : 1e-16);
+    const int it = con2prim(C, Tt, pd, tau1, x, sizeof(R) == 4 ? 1e-10 : 1e-13);
     if (it < 0) {
       atomicOr(P.status, ST_ROOT);
     } else {
