@@ -67,14 +67,17 @@ def test_init_tmunu_round_trip(which):
         tau = H.tau
         s = H.get_state()
         p = H.get_primitive()
+    # ghost cells get the ideal-fluid tensor of their (e, u): the Gubser
+    # test's corner ghosts keep a pi that no fluid tensor has
+    from helpers import interior_mask
+    p["pi"][:, ~interior_mask(cfg)] = 0.0
     T = tmunu_of(p, tau)
     with Hydro(cfg) as H2:
         assert H2.init_tmunu(tau, T) == 0
         s2 = H2.get_state()
         assert abs(H2.tau - tau) < 1e-15
     # interior cells (the Gubser test's mirrored ghosts hold a u^tau that is
-    # not the normalisation of their u^x, u^y: no fluid tensor there)
-    from helpers import interior_mask
+    # not the normalisation of their u^x, u^y)
     m = interior_mask(cfg)
     for grp in ((0,), (1, 2, 3, 4), (5, 6, 7, 8, 9), (10, 11, 12, 13)):
         scale = max(np.max(np.abs(s[q][m])) for q in grp)

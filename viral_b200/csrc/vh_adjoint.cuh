@@ -71,22 +71,26 @@ VH_HD inline void weno_lr_vjp(const R* q, R Lbar, R Rbar, R* qbar) {
                    (R)2 * q[0] - (R)7 * q[1] + (R)11 * q[2]};
   const R qr[3] = {(R)11 * q[2] - (R)7 * q[3] + (R)2 * q[4], (R)2 * q[1] + (R)5 * q[2] - q[3],
                    -q[0] + (R)5 * q[1] + (R)2 * q[2]};
+  // five reciprocals instead of a division per use
+  const R iE[3] = {(R)1 / E[0], (R)1 / E[1], (R)1 / E[2]};
   R al[3], ar[3], sl = 0, sr = 0;
-  for (int k = 0; k < 3; k++) { al[k] = dl[k] / E[k]; ar[k] = dr[k] / E[k]; sl += al[k]; sr += ar[k]; }
+  for (int k = 0; k < 3; k++) { al[k] = dl[k] * iE[k]; ar[k] = dr[k] * iE[k]; sl += al[k]; sr += ar[k]; }
+  const R isl = (R)1 / sl, isr = (R)1 / sr;
   R wl[3], wr[3];
-  for (int k = 0; k < 3; k++) { wl[k] = al[k] / sl; wr[k] = ar[k] / sr; }
+  for (int k = 0; k < 3; k++) { wl[k] = al[k] * isl; wr[k] = ar[k] * isr; }
   // candidates
+  const R L6 = Lbar * ((R)1 / (R)6), R6 = Rbar * ((R)1 / (R)6);
   R qlb[3], qrb[3], wlb[3], wrb[3];
   for (int k = 0; k < 3; k++) {
-    qlb[k] = wl[k] * Lbar / (R)6; qrb[k] = wr[k] * Rbar / (R)6;
-    wlb[k] = ql[k] * Lbar / (R)6; wrb[k] = qr[k] * Rbar / (R)6;
+    qlb[k] = wl[k] * L6; qrb[k] = wr[k] * R6;
+    wlb[k] = ql[k] * L6; wrb[k] = qr[k] * R6;
   }
   R swl = 0, swr = 0;
   for (int k = 0; k < 3; k++) { swl += wl[k] * wlb[k]; swr += wr[k] * wrb[k]; }
   R eb[3];
   for (int k = 0; k < 3; k++) {
-    const R alb = (wlb[k] - swl) / sl, arb = (wrb[k] - swr) / sr;
-    const R Eb = -(alb * al[k] + arb * ar[k]) / E[k];
+    const R alb = (wlb[k] - swl) * isl, arb = (wrb[k] - swr) * isr;
+    const R Eb = -(alb * al[k] + arb * ar[k]) * iE[k];
     eb[k] = Eb * (R)2 * e[k];  // d(e^2) and e = eps + beta: betabar = Ebar 2 e
   }
   const R a0b = eb[0] * (R)2 * c13 * a0, g0b = eb[0] * (R)0.5 * g0;
@@ -204,18 +208,21 @@ VH_HD inline void src2d_vjp(const DevCfg& C, R tau, R e, const R* u3v, const R* 
   // ---- forward recompute
   R P, dP, T, dT;
   eos_d<R>(C, e, P, dP, T, dT);
-  const R s = (e + P) / T;
+  const R iT = (R)1 / T, iep = (R)1 / (e + P), iP = (R)1 / P;
+  const R s = (e + P) * iT;
   const R tg = T * (R)C.hbarc - (R)C.etas_tc;
   const bool kink = tg > (R)0;
   const R etas = (R)C.etas0 + (R)C.etas1 * (kink ? tg : (R)0);
   const R eta = etas * s;
-  const R tp = C.taupi_kind == 1 ? (R)5 * eta / (e + P) : (R)1.5 * (eta / P);
+  const R tp = C.taupi_kind == 1 ? (R)5 * eta * iep : (R)1.5 * (eta * iP);
+  const R itp = (R)1 / tp;
   const R u0 = u[0], u1 = u[1], u2 = u[2];
+  const R iu0 = (R)1 / u0, iD = iu0 * iu0, it2 = (R)1 / t2;
   const R p1 = p3v[0], p2 = p3v[1], p3 = p3v[2];
   const R D = u0 * u0;
   const R Q = u1 * u1 * p1 + (R)2 * u1 * u2 * p3 + u2 * u2 * p2;
-  const R ptt = Q / D, pee = (Q - D * (p1 + p2)) / (t2 * D);
-  const R ptx = (p1 * u1 + p3 * u2) / u0, pty = (p3 * u1 + p2 * u2) / u0;
+  const R ptt = Q * iD, pee = (Q - D * (p1 + p2)) * it2 * iD;
+  const R ptx = (p1 * u1 + p3 * u2) * iu0, pty = (p3 * u1 + p2 * u2) * iu0;
   R pi[4][4] = {{ptt, ptx, pty, 0}, {ptx, p1, p3, 0}, {pty, p3, p2, 0}, {0, 0, 0, pee}};
   R Dm[4][4];
   for (int l = 0; l < 4; l++)
@@ -257,7 +264,7 @@ VH_HD inline void src2d_vjp(const DevCfg& C, R tau, R e, const R* u3v, const R* 
   R pa[4];
   for (int v = 0; v < 4; v++) pa[v] = pi[v][0] * acc4[0] + pi[v][1] * acc4[1] + pi[v][2] * acc4[2] + pi[v][3] * acc4[3];
   R divv = 0;
-  for (int i = 1; i < 3; i++) divv += du9[i * 3 + i] / u0 - u[i] * du9[i] / (u0 * u0);
+  for (int i = 1; i < 3; i++) divv += du9[i * 3 + i] * iu0 - u[i] * du9[i] * iD;
 
   // ---- reverse
   R u0b = 0, u1b = 0, u2b = 0, p1b = 0, p2b = 0, p3b = 0, Pb = 0, etab = 0, tpb = 0, thb = 0, divvb = 0;
@@ -271,25 +278,25 @@ VH_HD inline void src2d_vjp(const DevCfg& C, R tau, R e, const R* u3v, const R* 
     const R o = ob[1 + q];
     if (o == (R)0) continue;
     const int m = MU[q], v = NU[q];
-    const R rhs = -(pi[m][v] - (R)2 * eta * sig[m][v]) / tp - ((R)4 / (R)3) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
-    const R rb = o / u0;
-    u0b -= o * rhs / (u0 * u0);
+    const R rhs = -(pi[m][v] - (R)2 * eta * sig[m][v]) * itp - ((R)4 / (R)3) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
+    const R rb = o * iu0;
+    u0b -= o * rhs * iD;
     pib[m][v] += o * divv;
     divvb += o * pi[m][v];
-    pib[m][v] += -rb / tp - ((R)4 / (R)3) * th * rb;
-    sigb[m][v] += (R)2 * eta * rb / tp;
-    etab += (R)2 * sig[m][v] * rb / tp;
-    tpb += (pi[m][v] - (R)2 * eta * sig[m][v]) * rb / (tp * tp);
+    pib[m][v] += -rb * itp - ((R)4 / (R)3) * th * rb;
+    sigb[m][v] += (R)2 * eta * rb * itp;
+    etab += (R)2 * sig[m][v] * rb * itp;
+    tpb += (pi[m][v] - (R)2 * eta * sig[m][v]) * rb * (itp * itp);
     thb += -((R)4 / (R)3) * pi[m][v] * rb;
     ub[m] -= pa[v] * rb; pab[v] -= u[m] * rb;
     ub[v] -= pa[m] * rb; pab[m] -= u[v] * rb;
   }
   // divv = sum_i du[i][i]/u0 - u_i du[0][i]/u0^2
   for (int i = 1; i < 3; i++) {
-    dub[i * 3 + i] += divvb / u0;
-    u0b += divvb * (-du9[i * 3 + i] / (u0 * u0) + (R)2 * u[i] * du9[i] / (u0 * u0 * u0));
-    ub[i] -= divvb * du9[i] / (u0 * u0);
-    dub[i] -= divvb * u[i] / (u0 * u0);
+    dub[i * 3 + i] += divvb * iu0;
+    u0b += divvb * (-du9[i * 3 + i] * iD + (R)2 * u[i] * du9[i] * iD * iu0);
+    ub[i] -= divvb * du9[i] * iD;
+    dub[i] -= divvb * u[i] * iD;
   }
   // pa[v] = sum_b pi[v][b] acc[b]
   for (int v = 0; v < 4; v++)
@@ -336,31 +343,31 @@ VH_HD inline void src2d_vjp(const DevCfg& C, R tau, R e, const R* u3v, const R* 
   p1b += pib[1][1]; p2b += pib[2][2]; p3b += pib[1][2] + pib[2][1];
   const R peeb = pib[3][3];
   // ptt = Q/D, pee = (Q - D (p1+p2))/(t2 D), D = u0^2
-  const R Qb = pttb / D + peeb / (t2 * D);
-  const R Db = -pttb * ptt / D + peeb * (-(p1 + p2) / (t2 * D) - pee / D);
-  p1b -= peeb / t2; p2b -= peeb / t2;
+  const R Qb = pttb * iD + peeb * it2 * iD;
+  const R Db = -pttb * ptt * iD + peeb * (-(p1 + p2) * it2 * iD - pee * iD);
+  p1b -= peeb * it2; p2b -= peeb * it2;
   ub[0] += (R)2 * u0 * Db;
   p1b += Qb * u1 * u1; p2b += Qb * u2 * u2; p3b += Qb * (R)2 * u1 * u2;
   ub[1] += Qb * ((R)2 * u1 * p1 + (R)2 * u2 * p3);
   ub[2] += Qb * ((R)2 * u1 * p3 + (R)2 * u2 * p2);
   // ptx = (p1 u1 + p3 u2)/u0, pty = (p3 u1 + p2 u2)/u0
-  p1b += ptxb * u1 / u0; p3b += ptxb * u2 / u0; ub[1] += ptxb * p1 / u0; ub[2] += ptxb * p3 / u0; ub[0] -= ptxb * ptx / u0;
-  p3b += ptyb * u1 / u0; p2b += ptyb * u2 / u0; ub[1] += ptyb * p3 / u0; ub[2] += ptyb * p2 / u0; ub[0] -= ptyb * pty / u0;
+  p1b += ptxb * u1 * iu0; p3b += ptxb * u2 * iu0; ub[1] += ptxb * p1 * iu0; ub[2] += ptxb * p3 * iu0; ub[0] -= ptxb * ptx * iu0;
+  p3b += ptyb * u1 * iu0; p2b += ptyb * u2 * iu0; ub[1] += ptyb * p3 * iu0; ub[2] += ptyb * p2 * iu0; ub[0] -= ptyb * pty * iu0;
   // transport: eta = etas s, s = (e+P)/T, etas = c0 + c1 max(T hbarc - tc, 0), tp
   R eb_ = 0, Tb = 0;
   if (C.taupi_kind == 1) {
-    etab += tpb * (R)5 / (e + P);
-    const R eppb = -tpb * (R)5 * eta / ((e + P) * (e + P));
+    etab += tpb * (R)5 * iep;
+    const R eppb = -tpb * (R)5 * eta * (iep * iep);
     eb_ += eppb; Pb += eppb;
   } else {
-    etab += tpb * (R)1.5 / P;
-    Pb -= tpb * (R)1.5 * eta / (P * P);
+    etab += tpb * (R)1.5 * iP;
+    Pb -= tpb * (R)1.5 * eta * (iP * iP);
   }
   const R etasb = etab * s, sb = etab * etas;
   cb[0] += etasb;
   cb[1] += etasb * (kink ? tg : (R)0);
   if (kink) Tb += etasb * (R)C.etas1 * (R)C.hbarc;
-  eb_ += sb / T; Pb += sb / T; Tb -= sb * s / T;
+  eb_ += sb * iT; Pb += sb * iT; Tb -= sb * s * iT;
   eb_ += Pb * dP + Tb * dT;
   eb += eb_;
   ub3[0] += ub[0] + u0b;
