@@ -115,3 +115,12 @@ def test_no_timelike_eigenvector(L):
     ee = ctypes.c_double(); uu = np.zeros(4)
     assert L.vhc_landau(T10.ctypes.data_as(_dp), 1.0, 1, ctypes.byref(ee), uu.ctypes.data_as(_dp)) == 0
     assert find_var(T10, 1.0, True) == []
+
+
+def test_fluid_at_rest(L):
+    """u = 0 exactly: the matching must not fail on u^tau rounding below 1"""
+    for e in (0.3, 12.0, 150.0):
+        T10 = np.array([e, 0, 0, 0, e / 3, 0, 0, e / 3, 0, e / 3 / 1.7 ** 2])
+        ee = ctypes.c_double(); uu = np.zeros(4)
+        assert L.vhc_landau(T10.ctypes.data_as(_dp), 1.7, 0, ctypes.byref(ee), uu.ctypes.data_as(_dp)) == 1
+        assert abs(ee.value - e) <= 1e-14 * e and abs(uu[0] - 1) <= 1e-15 and np.all(uu[1:] == 0)

@@ -112,7 +112,9 @@ VH_HD inline bool landau_cell(const double* T10, double tau, bool cart, double& 
     res = fmax(res, fabs(r));
   }
   e = sig;
-  return u[0] >= 1.0 && e > 0 && res <= 1e-10 * fabs(e) * u[0];
+  // timelike and future-directed by construction (positive norm, u^tau > 0;
+  // at rest u^tau can round to 1 - 1 ulp)
+  return u[0] > 0 && e > 0 && res <= 1e-10 * fabs(e) * u[0];
 }
 
 template <class R>

@@ -298,6 +298,42 @@ VH_HD inline void weno_lr(R qm2, R qm1, R qc, R qp1, R qp2, R& L, R& Rr) {
   }
 }
 
+// weno_lr of two quantities in FP64 with one reciprocal for the four face
+// values (the product of the four denominators stays inside double range:
+// each lies between about 6e-24 and 1e40 for |q| below 1e4)
+VH_HD inline void weno_lr_pair(const double* a, const double* b, double& La, double& Ra, double& Lb, double& Rb) {
+  double num[4], den[4];
+  const double* q[2] = {a, b};
+  for (int m = 0; m < 2; m++) {
+    const double qm2 = q[m][0], qm1 = q[m][1], qc = q[m][2], qp1 = q[m][3], qp2 = q[m][4];
+    double b0, b1, b2;
+    weno_beta<double>(qm2, qm1, qc, qp1, qp2, b0, b1, b2);
+    const double eps = 1e-6;
+    const double e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+    const double E0 = e0 * e0, E1 = e1 * e1, E2 = e2 * e2;
+    const double P12 = E1 * E2, P02 = E0 * E2, P01 = E0 * E1;
+    const double nl0 = 0.3 * P12, nl1 = 0.6 * P02, nl2 = 0.1 * P01;
+    const double nr0 = 0.1 * P12, nr1 = nl1, nr2 = 0.3 * P01;
+    const double ql0 = 2 * qc + 5 * qp1 - qp2;
+    const double ql1 = -qm1 + 5 * qc + 2 * qp1;
+    const double ql2 = 2 * qm2 - 7 * qm1 + 11 * qc;
+    const double qr0 = 11 * qc - 7 * qp1 + 2 * qp2;
+    const double qr1 = 2 * qm1 + 5 * qc - qp1;
+    const double qr2 = -qm2 + 5 * qm1 + 2 * qc;
+    num[2 * m] = nl0 * ql0 + nl1 * ql1 + nl2 * ql2;
+    den[2 * m] = 6 * (nl0 + nl1 + nl2);
+    num[2 * m + 1] = nr0 * qr0 + nr1 * qr1 + nr2 * qr2;
+    den[2 * m + 1] = 6 * (nr0 + nr1 + nr2);
+  }
+  const double d01 = den[0] * den[1], d23 = den[2] * den[3];
+  const double inv = 1.0 / (d01 * d23);
+  const double i01 = d23 * inv, i23 = d01 * inv;  // 1/(den0 den1), 1/(den2 den3)
+  La = num[0] * den[1] * i01;
+  Ra = num[1] * den[0] * i01;
+  Lb = num[2] * den[3] * i23;
+  Rb = num[3] * den[2] * i23;
+}
+
 // generalized minmod (theta) piecewise-linear face values (utils.h:33-55)
 template <class R>
 VH_HD inline R mm3(R a, R b, R c) {

@@ -281,6 +281,14 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
           recon_lr<R>(C, sm.q[l], s, fl, fr);
           recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
         }
+      } else if (C.recon == 0) {
+        // F^l and V^l with one reciprocal between them
+        const double* qa = reinterpret_cast<const double*>(sm.q[l]) + s - 2;
+        const double* qb = reinterpret_cast<const double*>(sm.q[9 + l]) + s - 2;
+        double a_[5] = {qa[0], qa[1], qa[2], qa[3], qa[4]}, b_[5] = {qb[0], qb[1], qb[2], qb[3], qb[4]};
+        double flx, frx, vlx, vrx;
+        weno_lr_pair(a_, b_, flx, frx, vlx, vrx);
+        fl = flx; fr = frx; vl = vlx; vr = vrx;
       } else {
         recon_lr<R>(C, sm.q[l], s, fl, fr);
         recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
@@ -302,7 +310,7 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
       const R* q = sm.u[l];
       R L, Rr;
       weno_lr<R>(q[s - 2], q[s - 1], q[s], q[s + 1], q[s + 2], L, Rr);
-      P.du(l * 3 + DIR)[cell] = (L - Rr) / h;
+      P.du(l * 3 + DIR)[cell] = (L - Rr) * inv_h;
     }
   }
 }
@@ -375,7 +383,7 @@ __device__ __forceinline__ void rk_cell(const DevCfg& C, const DevPtrs<R>& P, do
     R du[4][4];
 #pragma unroll
     for (int l = 0; l < 4; l++) {
-      du[l][0] = (u[l] - pu[l]) / (R)ts;
+      du[l][0] = (u[l] - pu[l]) * (R)(1.0 / ts);
       du[l][1] = P.du(l * 3 + 0)[c];
       du[l][2] = P.du(l * 3 + 1)[c];
       du[l][3] = C.bi ? (R)0 : P.du(l * 3 + 2)[c];
@@ -426,7 +434,7 @@ __device__ __forceinline__ void rk_cell(const DevCfg& C, const DevPtrs<R>& P, do
       }
     }
 #pragma unroll
-    for (int l = 0; l < 4; l++) q9[l] = cart ? Vn[l] : Vn[l] / (R)tau1;
+    for (int l = 0; l < 4; l++) q9[l] = cart ? Vn[l] : Vn[l] * (R)(1.0 / tau1);
 #pragma unroll
     for (int l = 0; l < 5; l++) q9[4 + l] = Vn[4 + l];
 #pragma unroll
