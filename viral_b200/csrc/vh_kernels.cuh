@@ -306,11 +306,21 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   // velocity derivative along DIR: (L - R)/h of the same stencil (genWENOder)
   if (out) {
 #pragma unroll
-    for (int l = 0; l < 4; l++) {
-      const R* q = sm.u[l];
-      R L, Rr;
-      weno_lr<R>(q[s - 2], q[s - 1], q[s], q[s + 1], q[s + 2], L, Rr);
-      P.du(l * 3 + DIR)[cell] = (L - Rr) * inv_h;
+    for (int l = 0; l < 4; l += 2) {
+      const R* qa = sm.u[l] + s - 2;
+      const R* qb = sm.u[l + 1] + s - 2;
+      R La, Ra, Lb, Rb;
+      if constexpr (sizeof(R) == 4) {
+        F2 L2, R2;
+        weno_lr2(f2(qa[0], qb[0]), f2(qa[1], qb[1]), f2(qa[2], qb[2]), f2(qa[3], qb[3]), f2(qa[4], qb[4]), L2, R2);
+        f2u(L2, La, Lb);
+        f2u(R2, Ra, Rb);
+      } else {
+        const double a_[5] = {qa[0], qa[1], qa[2], qa[3], qa[4]}, b_[5] = {qb[0], qb[1], qb[2], qb[3], qb[4]};
+        weno_lr_pair(a_, b_, La, Ra, Lb, Rb);
+      }
+      P.du(l * 3 + DIR)[cell] = (La - Ra) * inv_h;
+      P.du((l + 1) * 3 + DIR)[cell] = (Lb - Rb) * inv_h;
     }
   }
 }
