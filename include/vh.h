@@ -173,6 +173,16 @@ int vh_write(vh_handle* h, const char* path, int layout, int every);
  * t-eta, xx, xy, x-eta, yy, y-eta, eta-eta, Pi), NEWEST10/write.h:51-115 and
  * its WriteResults. */
 
+/* Restart files.  vh_save_checkpoint writes the grid, tau and the 18
+ * canonical fields of every cell (ghosts and the previous velocity
+ * included); vh_load_checkpoint restores them into a handle of the same grid
+ * (coordinates, nx, ny, nz, boost invariance, dx, dy, dz; VH_E_ARG
+ * otherwise) and sets *tau_out (may be NULL).  A run resumed from a file of
+ * its own precision continues bit for bit; the handle's dtau applies.  The
+ * reference has no restart state (its snapshots are output only). */
+int vh_save_checkpoint(vh_handle* h, const char* path);
+int vh_load_checkpoint(vh_handle* h, const char* path, double* tau_out);
+
 /* Initial profile from the ASCII files of the ideal-hydro driver
  * (NEWideal/init.h:296-345): eps_path, vx_path and vy_path hold nx*ny
  * whitespace-separated numbers each, x fastest, for the interior cells of a
@@ -268,6 +278,12 @@ int vh_batch_get_tuning(vh_batch* b, int* variant, int* steps_per_launch, int* l
  * eps_2 = sqrt((<y^2> - <x^2>)^2 + 4 <xy>^2) / (<x^2> + <y^2>); n doubles
  * each, either may be NULL. */
 int vh_batch_observables(vh_batch* b, double* eps_p, double* ecc2);
+/* Self-test of the bounded grid barrier of the persistent kernel: a launch of
+ * two blocks where absent_blocks (0 or 1) never arrive.  With one absent, the
+ * waiting block gives up after its spin limit (2^20 polls) and the call
+ * returns VH_E_TIMEOUT, as vh_batch_run does when a barrier times out; the
+ * context stays usable.  *seconds (may be NULL) receives the launch's time. */
+int vh_batch_barrier_selftest(int absent_blocks, double* seconds);
 const char* vh_batch_last_error(const vh_batch* b);
 
 /* ------------------------------------------------------------- adjoint

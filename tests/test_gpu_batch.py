@@ -150,3 +150,25 @@ def test_per_event_observables():
         want = np.sqrt((syy - sxx) ** 2 + 4 * sxy ** 2) / (sxx + syy)
         assert abs(e2[ev] - want) <= 1e-10 * want
     assert np.all(np.abs(ep0) < 1e-12)  # at rest with pi = 0: T^xx = T^yy = P
+
+
+def test_barrier_timeout_is_reported_and_the_context_survives():
+    """The persistent kernel's grid barrier gives up after a bounded wait: a
+    launch where one block never arrives returns VH_E_TIMEOUT (no fault, no
+    hang), and the same context then runs a batch normally"""
+    import ctypes
+    L = A.lib()
+    sec = ctypes.c_double(-1.0)
+    assert L.vh_batch_barrier_selftest(0, ctypes.byref(sec)) == A.OK
+    assert 0 <= sec.value < 0.1
+    assert L.vh_batch_barrier_selftest(1, ctypes.byref(sec)) == A.E_TIMEOUT
+    assert b"timed out" in L.vh_batch_last_error(None)
+    assert 0 < sec.value < 10, sec.value
+    print("barrier wait gave up after %.3f s" % sec.value)
+    assert L.vh_batch_barrier_selftest(2, None) == A.E_ARG
+    cfg = C.glauber_config(nx=8, ny=8, boost_invariant=True)
+    with Batch(cfg, [24, 30], tau0=cfg.tau0, dtau=cfg.dtau, tau_max=100.0, t_freeze_gev=0.0) as B:
+        B.init_glauber(seeds=[0, 1], bimp=[3.0, 6.0])
+        B.run(4)
+        tau, nst, st = B.events()
+        assert np.all(st == EVENT_RUNNING) and np.all(nst == 4)

@@ -49,6 +49,22 @@ def test_glauber_snapshot_matches_the_python_path(tmp_path):
     assert open(mine, "rb").read() == open(os.path.join(out, "tau0.700fm.bin"), "rb").read()
 
 
+def test_driver_restart_continues_the_run(tmp_path):
+    """--checkpoint after 8 steps, then --restart from it up to step 16: the
+    final restart file and the last snapshot equal those of one 16-step run"""
+    t = str(tmp_path)
+    common = ["--scenario", "glauber", "--nx", "36", "--ny", "36", "--b", "5", "--seed", "1", "--print-every", "0.16"]
+    whole, part = os.path.join(t, "whole"), os.path.join(t, "part")
+    os.makedirs(whole), os.makedirs(part)
+    run_driver(common + ["--steps", "16", "--checkpoint", os.path.join(t, "whole.ck")], whole)
+    run_driver(common + ["--steps", "8", "--checkpoint", os.path.join(t, "half.ck")], part)
+    run_driver(common + ["--steps", "16", "--restart", os.path.join(t, "half.ck"), "--checkpoint",
+                         os.path.join(t, "resumed.ck")], part)
+    assert open(os.path.join(t, "whole.ck"), "rb").read() == open(os.path.join(t, "resumed.ck"), "rb").read()
+    snap = "tau0.920fm.bin"
+    assert open(os.path.join(whole, "res", snap), "rb").read() == open(os.path.join(part, "res", snap), "rb").read()
+
+
 def test_get_primitive():
     cfg = C.gubser_config(nx=21, ny=21)
     with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:

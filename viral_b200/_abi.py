@@ -103,6 +103,9 @@ SIGNATURES = [
     ("vh_batch_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("vh_batch_get_tuning", ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 5),
     ("vh_batch_observables", ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    ("vh_batch_barrier_selftest", ctypes.c_int, [ctypes.c_int, _dp]),
+    ("vh_save_checkpoint", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    ("vh_load_checkpoint", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _dp]),
     ("vh_batch_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("vh_read_ideal_profile", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
                                              ctypes.c_int, _dp, _dp, _dp, _dp]),

@@ -464,6 +464,8 @@ extern "C" const char* vh_last_error(const vh_handle* h) {
   return h ? h->err.c_str() : g_create_err.c_str();
 }
 
+int vh_internal_error(vh_handle* h, int code, const char* msg) { return fail(h, code, msg); }
+
 int vh_internal_config(const vh_handle* h, vh_config* out, std::vector<double>* eos4) {
   if (!h || !out) return VH_E_ARG;
   *out = h->cfg;

@@ -72,7 +72,7 @@ __device__ inline DevCfg event_cfg(const DevCfg& C0, int nx, int ny) {
 // Grid-wide barrier among the co-resident blocks of a cooperative launch.
 // The wait is bounded: after ~2 s the block sets the timeout flag and
 // returns false, and every block leaves the kernel at its next check.
-__device__ inline bool grid_barrier(unsigned int* bar) {
+__device__ inline bool grid_barrier(unsigned int* bar, long long max_spins = 1ll << 24) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* vgen = bar + 1;
@@ -85,7 +85,7 @@ __device__ inline bool grid_barrier(unsigned int* bar) {
     } else {
       long long spins = 0;
       while (*vgen == g) {
-        if (++spins > (1ll << 24)) { atomicOr(bar + 2, 1u); break; }
+        if (++spins > max_spins) { atomicOr(bar + 2, 1u); break; }
         __nanosleep(128);
       }
     }
@@ -188,6 +188,14 @@ __global__ void __launch_bounds__(NC * 32, MINB) k_batch(Args<R> A, int nsteps) 
       *T.running = tot;
     }
   }
+}
+
+// Probe of the bounded barrier: two blocks, of which `absent` never arrive;
+// block 0 waits at grid_barrier and, with a block missing, gives up after
+// 2^20 polls (a fraction of a second) and sets the timeout flag.
+__global__ void k_barrier_probe(unsigned int* bar, int absent) {
+  if ((int)blockIdx.x >= (int)gridDim.x - absent) return;
+  grid_barrier(bar, 1ll << 20);
 }
 
 // copy one event's canonical doubles (18 x n) into its pool view
@@ -702,6 +710,39 @@ extern "C" int vh_batch_autotune(vh_batch* b, const char* cache_path, int probe_
   if (cache_path && best < 1e300) {
     std::ofstream out(cache_path, std::ios::app);
     out << key.str() << "=" << best_v << "," << best_s << "\n";
+  }
+  return VH_OK;
+}
+
+extern "C" int vh_batch_barrier_selftest(int absent_blocks, double* seconds) {
+  if (absent_blocks < 0 || absent_blocks > 1) return VH_E_ARG;
+  unsigned int* bar = nullptr;
+  if (cudaMalloc(&bar, 3 * sizeof(unsigned int)) != cudaSuccess) return VH_E_NOMEM;
+  unsigned int h[3] = {0, 0, 0};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaError_t err = cudaMemset(bar, 0, 3 * sizeof(unsigned int));
+  if (err == cudaSuccess) {
+    cudaEventRecord(e0);
+    k_barrier_probe<<<2, 32>>>(bar, absent_blocks);
+    cudaEventRecord(e1);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMemcpy(h, bar, sizeof(h), cudaMemcpyDeviceToHost);
+  float ms = 0;
+  if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(bar);
+  if (err != cudaSuccess) {
+    g_batch_err = std::string("vh_batch_barrier_selftest: ") + cudaGetErrorString(err);
+    return VH_E_CUDA;
+  }
+  if (seconds) *seconds = ms / 1e3;
+  if (h[2]) {
+    g_batch_err = "grid barrier timed out";
+    return VH_E_TIMEOUT;
   }
   return VH_OK;
 }

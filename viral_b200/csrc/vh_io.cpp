@@ -1,5 +1,6 @@
 // Snapshot writer in the reference's binary layout (NEWEST5/write.h).
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -164,5 +165,80 @@ extern "C" int vh_read_ideal_profile(const char* eps_path, const char* vx_path, 
     uy[c] = g * vy[c];
   }
   if (min_out) *min_out = mn;
+  return VH_OK;
+}
+
+// Restart files: an 8-byte tag, the grid (coords, precision, nx, ny, nz,
+// boost invariance as int32), dx, dy, dz, dtau and tau as doubles, then the
+// 18 canonical fields over the ghost-inclusive grid.  The reference keeps no
+// restart state; these hold everything a step reads (prevu included), so a
+// run resumed from one continues bit for bit.
+namespace {
+const char kCkptTag[8] = {'V', 'H', 'C', 'K', 'P', 'T', '0', '1'};
+struct CkptHead {
+  char tag[8];
+  int32_t coords, precision, nx, ny, nz, boost_invariant;
+  double dx, dy, dz, dtau, tau;
+};
+}  // namespace
+
+extern "C" int vh_save_checkpoint(vh_handle* h, const char* path) {
+  if (!h || !path) return VH_E_ARG;
+  vh_config cfg;
+  int r = vh_internal_config(h, &cfg, nullptr);
+  if (r) return r;
+  int gx, gy, gz;
+  vh_dims(h, &gx, &gy, &gz);
+  const size_t n = (size_t)gx * gy * gz;
+  std::vector<double> f(18 * n);
+  if ((r = vh_get_state(h, f.data()))) return r;
+  CkptHead hd{};
+  std::memcpy(hd.tag, kCkptTag, 8);
+  hd.coords = cfg.coords;
+  hd.precision = cfg.precision;
+  hd.nx = cfg.nx;
+  hd.ny = cfg.ny;
+  hd.nz = cfg.nz;
+  hd.boost_invariant = cfg.boost_invariant;
+  hd.dx = cfg.dx;
+  hd.dy = cfg.dy;
+  hd.dz = cfg.dz;
+  hd.dtau = cfg.dtau;
+  vh_get_time(h, &hd.tau);
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return vh_internal_error(h, VH_E_ARG, "vh_save_checkpoint: cannot open the file for writing");
+  const bool ok = std::fwrite(&hd, sizeof(hd), 1, fp) == 1 && std::fwrite(f.data(), sizeof(double), f.size(), fp) == f.size();
+  const bool closed = std::fclose(fp) == 0;
+  return ok && closed ? VH_OK : vh_internal_error(h, VH_E_ARG, "vh_save_checkpoint: short write");
+}
+
+extern "C" int vh_load_checkpoint(vh_handle* h, const char* path, double* tau_out) {
+  if (!h || !path) return VH_E_ARG;
+  vh_config cfg;
+  int r = vh_internal_config(h, &cfg, nullptr);
+  if (r) return r;
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) return vh_internal_error(h, VH_E_ARG, "vh_load_checkpoint: cannot open the file");
+  CkptHead hd{};
+  if (std::fread(&hd, sizeof(hd), 1, fp) != 1 || std::memcmp(hd.tag, kCkptTag, 8) != 0) {
+    std::fclose(fp);
+    return vh_internal_error(h, VH_E_ARG, "vh_load_checkpoint: not a restart file");
+  }
+  const bool same_grid = hd.coords == cfg.coords && hd.nx == cfg.nx && hd.ny == cfg.ny && hd.nz == cfg.nz &&
+                         hd.boost_invariant == cfg.boost_invariant && hd.dx == cfg.dx && hd.dy == cfg.dy &&
+                         hd.dz == cfg.dz;
+  if (!same_grid) {
+    std::fclose(fp);
+    return vh_internal_error(h, VH_E_ARG, "vh_load_checkpoint: the file's grid differs from the handle's");
+  }
+  int gx, gy, gz;
+  vh_dims(h, &gx, &gy, &gz);
+  const size_t n = (size_t)gx * gy * gz;
+  std::vector<double> f(18 * n);
+  const bool ok = std::fread(f.data(), sizeof(double), f.size(), fp) == f.size();
+  std::fclose(fp);
+  if (!ok) return vh_internal_error(h, VH_E_ARG, "vh_load_checkpoint: the file is truncated");
+  if ((r = vh_set_state(h, f.data(), hd.tau))) return r;
+  if (tau_out) *tau_out = hd.tau;
   return VH_OK;
 }

@@ -50,13 +50,16 @@ struct Options {
   unsigned long long seed = 0;
   double floor_gev = 0.2;    // GeV/fm^3, the library workloads' Glauber floor
   bool quiet = false;
+  std::string restart;      // resume from this restart file
+  std::string checkpoint;   // write a restart file at the end
 };
 
 void usage() {
   std::printf(
       "usage: vh_run [--scenario gubser|glauber|glauber3d|shocktube] [--nx N --ny N --nz N]\n"
       "              [--precision fp64|mixed] [--steps N] [--tau-end T] [--print-every T]\n"
-      "              [--out DIR] [--every FREQ] [--b B] [--seed S] [--floor E_GeV_fm3] [--quiet]\n");
+      "              [--out DIR] [--every FREQ] [--b B] [--seed S] [--floor E_GeV_fm3] [--quiet]\n"
+      "              [--restart FILE] [--checkpoint FILE]\n");
 }
 
 bool parse(int argc, char** argv, Options& o) {
@@ -88,6 +91,8 @@ bool parse(int argc, char** argv, Options& o) {
     else if (a == "--seed") o.seed = std::strtoull(next("--seed"), nullptr, 10);
     else if (a == "--floor") o.floor_gev = std::atof(next("--floor"));
     else if (a == "--quiet") o.quiet = true;
+    else if (a == "--restart") o.restart = next("--restart");
+    else if (a == "--checkpoint") o.checkpoint = next("--checkpoint");
     else { std::fprintf(stderr, "vh_run: unknown option %s\n", a.c_str()); usage(); return false; }
   }
   if (o.scenario != "gubser" && o.scenario != "glauber" && o.scenario != "glauber3d" && o.scenario != "shocktube") {
@@ -171,6 +176,12 @@ int main(int argc, char** argv) {
     if (!r) r = vh_init_profile(h, c.tau0, e.data(), ux.data(), uy.data(), nullptr, nullptr, VH_PI_ZERO, nullptr);
   }
   if (r) { const int code = fail("initial state", h, r); vh_destroy(h); return code; }
+  double tau = c.tau0;
+  if (!o.restart.empty() && (r = vh_load_checkpoint(h, o.restart.c_str(), &tau))) {
+    const int code = fail("vh_load_checkpoint", h, r);
+    vh_destroy(h);
+    return code;
+  }
 
   const int layout = c.boost_invariant ? VH_WRITE_XY : VH_WRITE_FULL;
   auto write = [&](double tau) -> int {
@@ -182,10 +193,11 @@ int main(int argc, char** argv) {
   if (!o.out.empty()) mkdir(o.out.c_str(), 0755);
 
   const double ts = c.dtau;
-  double tau = c.tau0, tau_print = c.tau0;
-  if ((r = write(tau))) { const int code = fail("vh_write", h, r); vh_destroy(h); return code; }
+  // a resumed run keeps the step count and print cadence of the original one
+  int l = 1 + (int)std::lround((tau - c.tau0) / ts);
+  double tau_print = c.tau0 + std::floor((tau - c.tau0) / o.print_every + 1e-6) * o.print_every;
+  if (o.restart.empty() && (r = write(tau))) { const int code = fail("vh_write", h, r); vh_destroy(h); return code; }
   const auto start = std::chrono::steady_clock::now();
-  int l = 1;
   int status = 0;
   while (true) {
     if ((r = vh_step(h, 1))) { status = fail("vh_step", h, r); break; }
@@ -209,6 +221,8 @@ int main(int argc, char** argv) {
     if (tau > o.tau_end) break;                // main.cpp:211
     if (o.max_steps > 0 && l > o.max_steps) break;
   }
+  if (!status && !o.checkpoint.empty() && (r = vh_save_checkpoint(h, o.checkpoint.c_str())))
+    status = fail("vh_save_checkpoint", h, r);
   double sums[4];
   if (!status && vh_conservation_sums(h, sums) == VH_OK && !o.quiet)
     std::printf("tau %.4f fm/c after %d steps; sum tau T^{tau mu} dV = %.10e %.10e %.10e %.10e\n", tau, l - 1, sums[0],

@@ -166,6 +166,15 @@ class Hydro:
     def write(self, path: str, layout: int = A.WRITE_XY, every: int = 1):
         self._chk(A.lib().vh_write(self.h, path.encode(), layout, every))
 
+    def save_checkpoint(self, path: str):
+        self._chk(A.lib().vh_save_checkpoint(self.h, path.encode()))
+
+    def load_checkpoint(self, path: str) -> float:
+        """restores the state and time saved by save_checkpoint; returns tau"""
+        t = ctypes.c_double()
+        self._chk(A.lib().vh_load_checkpoint(self.h, path.encode(), ctypes.byref(t)))
+        return t.value
+
     # ---- observable and its adjoint
     def eps_p(self) -> float:
         v = ctypes.c_double()
