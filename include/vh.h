@@ -62,7 +62,7 @@ enum { VH_TAUPI_15_ETA_OVER_P = 0, VH_TAUPI_5_ETA_OVER_EPP = 1 };
 enum { VH_PI_GIVEN = 0, VH_PI_ZERO = 1, VH_PI_NS = 2 };
 /* snapshot layouts: NEWEST5/write.h's 12 doubles per cell for one xy plane
  * or the full grid, and NEWEST10/write.h's 17 (full pi^{mu nu}) likewise */
-enum { VH_WRITE_XY = 0, VH_WRITE_FULL = 1, VH_WRITE_XY17 = 2, VH_WRITE_FULL17 = 3 };
+enum { VH_WRITE_XY = 0, VH_WRITE_FULL = 1, VH_WRITE_XY17 = 2, VH_WRITE_FULL17 = 3, VH_WRITE_NS_XY = 4 };
 
 typedef struct {
   int coords;           /* VH_COORD_* (NEWEST5 Milne, TXYZ5 Cartesian) */
@@ -172,6 +172,20 @@ int vh_write(vh_handle* h, const char* path, int layout, int every);
  * cell (e, T, P, v^x, v^y, v^eta, the ten pi^{mu nu} in the order tt, tx, ty,
  * t-eta, xx, xy, x-eta, yy, y-eta, eta-eta, Pi), NEWEST10/write.h:51-115 and
  * its WriteResults. */
+
+/* VH_WRITE_NS_XY: NEWEST10's Navier-Stokes snapshot (WriteNSXY,
+ * NEWEST10/write.h:123-170, written as res/NStau%2.3ffm.bin): 11 doubles
+ * per cell, the ten components of vh_get_ns_pi and a zero bulk part, in the
+ * VH_WRITE_XY order (x outer, y inner, central eta slice, every FREQ-th). */
+
+/* Navier-Stokes shear pi^{mu nu}_NS = 2 eta sigma^{mu nu} at the current
+ * state, ten fields of the ghost-inclusive grid in the order tt, tx, ty,
+ * t-eta, xx, xy, x-eta, yy, y-eta, eta-eta (NEWEST10/Source.h:643-753,
+ * CalcNS), with the step's velocity derivatives: d_tau u = (u - prevu)/dtau
+ * and WENO derivatives in space (NEWEST10/Source.h:3-95).  Meaningful on
+ * the interior cells.  Evaluated in FP64 (from the FP32 state in the mixed
+ * mode). */
+int vh_get_ns_pi(vh_handle* h, double* pi10);
 
 /* Restart files.  vh_save_checkpoint writes the grid, tau and the 18
  * canonical fields of every cell (ghosts and the previous velocity

@@ -884,6 +884,33 @@ void vho_ns_init(vho_grid* g, double tau, double ts) {
   vho_fill_tmunu(g, tau);
 }
 
+/* Navier-Stokes shear 2 eta sigma^{mu nu}, all ten components in the order
+ * tt, tx, ty, t-eta, xx, xy, x-eta, yy, y-eta, eta-eta, for one cell from
+ * (e, u, du, tau).  NEWEST10/Source.h:643-753 (CalcNS) writes the same
+ * tensor as expanded polynomials in u and du; here it is the projector form
+ * of is_kinematics. */
+void vho_ns_pi10_cell(const vho_grid* g, double tau, double e, const double* u, const double* du, double* out10) {
+  static const int MU[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3}, NU[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+  double sig[4][4], th, acc[4], eta, tp;
+  transport(&g->c, e, eos_P(&g->c, e), &eta, &tp);
+  is_kinematics(g->c.cartesian, tau, u, du, sig, &th, acc);
+  for (int q = 0; q < 10; q++) out10[q] = 2.0 * eta * sig[MU[q]][NU[q]];
+}
+
+/* The same on every cell with the velocity derivatives the step would use
+ * at this moment (d_tau u from prevu over ts): out[10*G]. */
+void vho_ns_pi10(vho_grid* g, double tau, double ts, double* out) {
+  const size_t n = g->n;
+  calc_du(g, ts);
+  for (size_t c = 0; c < n; c++) {
+    double e, u[4], p[5], du[16], o[10];
+    load_cell(g, c, &e, u, p);
+    for (int a = 0; a < 16; a++) du[a] = g->du[(size_t)a * n + c];
+    vho_ns_pi10_cell(g, tau, e, u, du, o);
+    for (int q = 0; q < 10; q++) out[(size_t)q * n + c] = o[q];
+  }
+}
+
 double vho_max_temp_gev(const vho_grid* g) {
   double tmax = 0;
   for (int k = g->kl; k < g->kr; k++)

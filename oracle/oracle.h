@@ -74,6 +74,13 @@ void vho_stage_terms(vho_grid* g, double tau, double ts, double* src, double* re
 /* Navier-Stokes pi and T^{tau mu} on every cell (NEWEST5/Source.h:535-630) */
 void vho_ns_init(vho_grid* g, double tau, double ts);
 
+/* Navier-Stokes shear 2 eta sigma^{mu nu}, ten components (tt, tx, ty,
+ * t-eta, xx, xy, x-eta, yy, y-eta, eta-eta) as NEWEST10/Source.h:643-753:
+ * for one cell from du16 (du[l*4+m] = d_m u^l), or on every cell with the
+ * step's velocity derivatives (out[10*G]) */
+void vho_ns_pi10_cell(const vho_grid* g, double tau, double e, const double* u, const double* du16, double* out10);
+void vho_ns_pi10(vho_grid* g, double tau, double ts, double* out);
+
 /* zero-gradient (or Gubser-mirror) ghost copy (NEWEST5/boundary.h) */
 void vho_boundary(vho_grid* g);
 

@@ -106,7 +106,7 @@ class Oracle:
             for name in ("vho_destroy", "vho_dims", "vho_set_state", "vho_get_state", "vho_step",
                          "vho_stage_terms", "vho_ns_init", "vho_boundary", "vho_fill_tmunu",
                          "vho_max_temp_gev", "vho_last_iterations", "vho_eos", "vho_con2prim",
-                         "vho_is_source", "vho_residual"):
+                         "vho_is_source", "vho_residual", "vho_ns_pi10", "vho_ns_pi10_cell"):
                 getattr(L, name).argtypes = None
             L.vho_destroy.argtypes = [ctypes.c_void_p]
             L.vho_set_state.argtypes = [ctypes.c_void_p, _dp]
@@ -126,6 +126,8 @@ class Oracle:
             L.vho_con2prim.restype = ctypes.c_int
             L.vho_is_source.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp, _dp, _dp, ctypes.c_double, _dp]
             L.vho_residual.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+            L.vho_ns_pi10.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp]
+            L.vho_ns_pi10_cell.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
             cls._lib = L
         return cls._lib
 
@@ -160,6 +162,18 @@ class Oracle:
 
     def ns_init(self, tau, ts):
         self.lib().vho_ns_init(self.h, tau, ts)
+
+    def ns_pi10(self, tau, ts):
+        """2 eta sigma^{mu nu} (10, n) with the step's velocity derivatives"""
+        out = np.zeros((10, self.n))
+        self.lib().vho_ns_pi10(self.h, tau, ts, _ptr(out))
+        return out
+
+    def ns_pi10_cell(self, tau, e, u, du16):
+        out = np.zeros(10)
+        self.lib().vho_ns_pi10_cell(self.h, tau, e, _ptr(np.ascontiguousarray(u, dtype=np.float64)),
+                                    _ptr(np.ascontiguousarray(du16, dtype=np.float64)), _ptr(out))
+        return out
 
     def boundary(self):
         self.lib().vho_boundary(self.h)
@@ -247,6 +261,30 @@ class RefBuild:
         self.L.ref_residual(_ptr(np.ascontiguousarray(x, dtype=np.float64)),
                             _ptr(np.ascontiguousarray(p, dtype=np.float64)), _ptr(y), _ptr(J))
         return y, J.reshape(4, 4)
+
+
+class RefNS10:
+    """NEWEST10's CalcNS in its default compile-time block, boost invariant
+    (oracle/ref_ns10.cpp)."""
+
+    def __init__(self):
+        L = _load(os.path.join(HERE, "_ref", "libref_ns10_lbi.so"))
+        L.ref10_calc_ns.argtypes = [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
+        d = (ctypes.c_int * 9)()
+        c = (ctypes.c_double * 3)()
+        L.ref10_init(d, c)
+        self.L = L
+        self.gx, self.gy, self.gz, self.il, self.ir, self.jl, self.jr, self.kl, self.kr = list(d)
+        self.dx, self.dy, self.factor = list(c)
+        self.n = self.gx * self.gy * self.gz
+
+    def calc_ns(self, f, du3, tau, ts):
+        """returns nspi + nsPI (11, n) and the du it used (16, n)"""
+        f = np.ascontiguousarray(f, dtype=np.float64).reshape(NF, self.n)
+        du3 = np.ascontiguousarray(du3, dtype=np.float64).reshape(4, self.n)
+        ns = np.zeros((11, self.n)); du = np.zeros((16, self.n))
+        self.L.ref10_calc_ns(_ptr(f), _ptr(du3), tau, ts, _ptr(ns), _ptr(du))
+        return ns, du
 
 
 # ---------------------------------------------------------------- inputs

@@ -15,7 +15,8 @@ T^{tau mu} from the oracle's closure), and the reference computes:
 Outputs are stored at a seeded sample of interior cells (plus per-field
 sums over the whole grid), so that the fixtures stay small.  A fifth
 fixture, cart_3d_shock, is the reference's own Cartesian scenario (the
-shock tube of its default TXYZ5 block) after 20 steps.  The CPU tests
+shock tube of its default TXYZ5 block) after 20 steps; a sixth, ns10_lbi,
+is NEWEST10's ten-component Navier-Stokes shear tensor (CalcNS).  The CPU tests
 rebuild the same inputs and check the oracle against these numbers.
 """
 from __future__ import annotations
@@ -30,7 +31,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from pyoracle import Oracle, OracleConfig, RefBuild, smooth_state  # noqa: E402
+from pyoracle import Oracle, OracleConfig, RefBuild, RefNS10, grid_coords, smooth_state  # noqa: E402
 
 # reference scenario blocks (oracle/Makefile) and the EOS / transport they compile
 SCENARIOS = {
@@ -140,10 +141,33 @@ def make_shock() -> dict:
             "state": s[:14, cells], "state_sum": s.sum(axis=1)}
 
 
+NS10_TAU = 1.3
+NS10_SEED = 11
+
+
+def make_ns10() -> dict:
+    """NEWEST10's Navier-Stokes shear tensor (CalcNS, ten components) in its
+    default compile-time block, boost invariant.  The state is the seeded
+    smooth state of the other fixtures (u^eta nonzero); du[l][3], which that
+    build does not compute, is seeded noise, so that every term counts."""
+    R = RefNS10()
+    x, y, z = grid_coords(R.gx, R.gy, R.gz, R.dx, R.dy, 0.1, True)
+    f = smooth_state(x, y, z, NS10_TAU, TS, seed=SEED)
+    du3 = 0.1 * np.random.default_rng(NS10_SEED).standard_normal((4, R.n))
+    ns, du = R.calc_ns(f, du3, NS10_TAU, TS)
+    idx = np.arange(R.n)
+    i, j = idx % R.gx, idx // R.gx
+    inner = np.where((i >= R.il) & (i < R.ir) & (j >= R.jl) & (j < R.jr))[0]
+    cells = np.sort(np.random.default_rng(123).choice(inner, size=NSAMPLE, replace=False))
+    return {"cells": cells, "tau": NS10_TAU, "ts": TS, "seed": SEED,
+            "dims": np.array([R.gx, R.gy, R.gz, 1]), "consts": np.array([R.dx, R.dy, R.factor]),
+            "ns": ns[:, cells], "du": du[:, cells], "ns_sum": ns[:, inner].sum(axis=1)}
+
+
 def main():
-    which = sys.argv[1:] or list(SCENARIOS) + ["cart_3d_shock"]
+    which = sys.argv[1:] or list(SCENARIOS) + ["cart_3d_shock", "ns10_lbi"]
     for v in which:
-        d = make_shock() if v == "cart_3d_shock" else make(v)
+        d = make_shock() if v == "cart_3d_shock" else make_ns10() if v == "ns10_lbi" else make(v)
         path = os.path.join(HERE, f"ref_{v}.npz")
         np.savez_compressed(path, **d)
         print(path, os.path.getsize(path))

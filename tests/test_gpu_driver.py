@@ -65,6 +65,24 @@ def test_driver_restart_continues_the_run(tmp_path):
     assert open(os.path.join(whole, "res", snap), "rb").read() == open(os.path.join(part, "res", snap), "rb").read()
 
 
+def test_driver_navier_stokes_files(tmp_path):
+    """--ns: beside each snapshot the Navier-Stokes file of NEWEST10's
+    initialisation (res/NStau%2.3ffm.bin), the bytes vh_write gives"""
+    out = run_driver(["--scenario", "gubser", "--nx", "33", "--ny", "33", "--steps", "3", "--print-every", "0.03",
+                      "--ns"], str(tmp_path))
+    names = sorted(os.listdir(out))
+    assert "NStau1.000fm.bin" in names and "NStau1.030fm.bin" in names, names
+    cfg = C.gubser_config(nx=33, ny=33)
+    with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:
+        first = os.path.join(str(tmp_path), "ns0.bin")
+        H.write(first, A.WRITE_NS_XY, 1)
+        H.step(3)
+        last = os.path.join(str(tmp_path), "ns3.bin")
+        H.write(last, A.WRITE_NS_XY, 1)
+    assert open(first, "rb").read() == open(os.path.join(out, "NStau1.000fm.bin"), "rb").read()
+    assert open(last, "rb").read() == open(os.path.join(out, "NStau1.030fm.bin"), "rb").read()
+
+
 def test_get_primitive():
     cfg = C.gubser_config(nx=21, ny=21)
     with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:

@@ -121,3 +121,38 @@ def test_cartesian_shock_tube():
         if grp:
             assert scaled_err(s[grp][:, c], g["state"][grp]) <= TOL, grp
     assert np.allclose(s.sum(axis=1)[:14], g["state_sum"][:14], rtol=1e-12, atol=1e-9)
+
+
+def test_navier_stokes_shear_ten_components():
+    """NEWEST10's CalcNS (ten components of 2 eta sigma^{mu nu} as expanded
+    polynomials): the oracle's projector form at the reference's own
+    velocity derivatives, with u^eta and d_eta u^mu nonzero, and the
+    oracle's velocity derivatives against the reference's"""
+    g = np.load(os.path.join(GOLD, "ref_ns10_lbi.npz"))
+    gx, gy, gz, _ = (int(v) for v in g["dims"])
+    dx, dy, factor = (float(v) for v in g["consts"])
+    tau, ts = float(g["tau"]), float(g["ts"])
+    cfg = OracleConfig(nx=gx - 6, ny=gy - 6, nz=1, boost_invariant=True, cartesian=False, dx=dx, dy=dy, dz=0.1,
+                       eos_kind=0, eos_a=factor, etas0=1 / (4 * math.pi), hbarc=0.1973, taupi_kind=0)
+    x, y, z = grid_coords(gx, gy, gz, dx, dy, 0.1, True)
+    f = smooth_state(x, y, z, tau, ts, seed=int(g["seed"]))
+    assert np.abs(f[4]).max() > 0.01  # u^eta is exercised
+    O = Oracle(cfg)
+    O.set_state(f)
+    cells, ns, du = g["cells"], g["ns"], g["du"]
+    assert np.all(ns[10] == 0)  # no bulk viscosity in the build
+    mine = np.array([O.ns_pi10_cell(tau, f[0, c], f[1:5, c], du[:, a]) for a, c in enumerate(cells)]).T
+    for q in range(10):
+        assert scaled_err(mine[q], ns[q]) <= TOL, q
+    # the step's velocity derivatives (d_tau from prevu, WENO in x and y)
+    grid = O.ns_pi10(tau, ts)
+    _, _, odu = O.stage_terms(tau, ts)
+    for q in range(16):
+        if q % 4 != 3:
+            assert scaled_err(odu[q, cells], du[q]) <= TOL, q
+    # with d_eta u = 0 (what a boost-invariant grid has) the grid path equals
+    # the pointwise one
+    du0 = du.copy()
+    du0[3::4] = 0
+    again = np.array([O.ns_pi10_cell(tau, f[0, c], f[1:5, c], du0[:, a]) for a, c in enumerate(cells)]).T
+    assert np.array_equal(grid[:, cells], again)

@@ -27,7 +27,7 @@ RECON_WENO5, RECON_MINMOD = 0, 1
 EOS_CONFORMAL, EOS_TABLE = 0, 1
 TAUPI_15_ETA_OVER_P, TAUPI_5_ETA_OVER_EPP = 0, 1
 PI_GIVEN, PI_ZERO, PI_NS = 0, 1, 2
-WRITE_XY, WRITE_FULL, WRITE_XY17, WRITE_FULL17 = 0, 1, 2, 3
+WRITE_XY, WRITE_FULL, WRITE_XY17, WRITE_FULL17, WRITE_NS_XY = 0, 1, 2, 3, 4
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -104,6 +104,7 @@ SIGNATURES = [
     ("vh_batch_get_tuning", ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 5),
     ("vh_batch_observables", ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
     ("vh_batch_barrier_selftest", ctypes.c_int, [ctypes.c_int, _dp]),
+    ("vh_get_ns_pi", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("vh_save_checkpoint", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("vh_load_checkpoint", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _dp]),
     ("vh_batch_last_error", ctypes.c_char_p, [ctypes.c_void_p]),

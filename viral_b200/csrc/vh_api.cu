@@ -321,6 +321,28 @@ extern "C" int vh_get_primitive(vh_handle* h, double* e, double* P, double* T, d
   return VH_OK;
 }
 
+template <class R>
+static int ns_pi10(vh_handle* h, const DevPtrs<R>& P, double* out) {
+  const DevCfg& C = h->C;
+  R* du16 = P.base1;  // 16 of the step's 34 scratch arrays, free between steps
+  k_du_full<R><<<grid1(C.n, 128), 128, 0, h->stream>>>(C, P, du16, h->cfg.dtau);
+  k_ns_pi10<R><<<grid1(C.n, 128), 128, 0, h->stream>>>(C, P, du16, h->tau, out);
+  VH_CUDA(h, cudaGetLastError());
+  return VH_OK;
+}
+
+extern "C" int vh_get_ns_pi(vh_handle* h, double* pi10) {
+  if (!h || !pi10) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  const long long n = h->C.n;
+  double* buf = h->stage;  // 18 x n doubles; 10 are used
+  int r = h->mixed ? ns_pi10<float>(h, h->pf, buf) : ns_pi10<double>(h, h->pd, buf);
+  if (r) return r;
+  VH_CUDA(h, cudaMemcpyAsync(pi10, buf, 10 * sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VH_OK;
+}
+
 extern "C" int vh_landau_match(const double* tmunu10, long long n, double tau, int cartesian, double* e, double* u4,
                                long long* nfail) {
   if (!tmunu10 || !e || !u4 || n < 1 || (!cartesian && !(tau > 0))) return VH_E_ARG;

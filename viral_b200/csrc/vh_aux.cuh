@@ -232,6 +232,31 @@ __global__ void k_ns_pi(DevCfg C, DevPtrs<R> P, const R* du16, double tau) {
   P.A(8)[c] = (R)2 * eta * sig[2][3];
 }
 
+// Navier-Stokes shear 2 eta sigma^{mu nu}, all ten components (tt, tx, ty,
+// t-eta, xx, xy, x-eta, yy, y-eta, eta-eta) on every cell from du16, in
+// FP64 whatever the state's type: out10[q*n + c].  NEWEST10/Source.h:643-753
+// (CalcNS) expands the same tensor into polynomials of u and du.
+template <class R>
+__global__ void k_ns_pi10(DevCfg C, DevPtrs<R> P, const R* du16, double tau, double* out10) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C.n) return;
+  double u[4], du[4][4];
+  const double e = (double)P.e()[c];
+#pragma unroll
+  for (int l = 0; l < 4; l++) u[l] = (double)P.u(l)[c];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) du[a][b] = (double)du16[(a * 4 + b) * C.n + c];
+  double eta, tp;
+  transport<double>(C, e, eos_P<double>(C, e), &eta, &tp);
+  double sig[4][4], th, acc[4];
+  is_kinematics<double, true>(C.cart, tau, u, du, sig, th, acc);
+  const int MU[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3}, NU[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+#pragma unroll
+  for (int q = 0; q < 10; q++) out10[q * C.n + c] = 2.0 * eta * sig[MU[q]][NU[q]];
+}
+
 // Sources at the current state for the debug dump (interior only).
 template <class R>
 __global__ void k_debug_src(DevCfg C, DevPtrs<R> P, const R* du16, R* src9, double tau) {

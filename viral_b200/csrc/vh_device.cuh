@@ -361,8 +361,9 @@ VH_HD inline R mm_right(R th, R qm1, R qc, R qp1) {
 //       + pi d_i v^i
 // with sigma the fully projected shear tensor, theta = nabla.u and
 // a_b = u^a nabla_a u_b (NEWEST5/Source.h:317-370; Cartesian: no
-// Christoffels, TXYZ5/Source.h:291-335).  du[l][m] = d_m u^l.
-template <class R>
+// Christoffels, TXYZ5/Source.h:291-335).  du[l][m] = d_m u^l.  The step
+// needs the rows x and y of sigma (columns x, y, eta); FULL fills all of it.
+template <class R, bool FULL = false>
 VH_HD inline void is_kinematics(int cart, R tau, const R* u, const R du[4][4], R sig[4][4], R& theta, R acc[4]) {
   const R t2 = cart ? (R)1 : tau * tau;
   const R g[4] = {(R)1, (R)-1, (R)-1, -t2};
@@ -400,10 +401,11 @@ VH_HD inline void is_kinematics(int cart, R tau, const R* u, const R du[4][4], R
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 4; b++) S[a][b] = (R)0.5 * (Dl[a][b] + Dl[b][a]);
-  // only sigma^{xx}, sigma^{yy}, sigma^{xy}, sigma^{x eta}, sigma^{y eta}
-  // (rows x, y and columns x, y, eta) are used
+  // the step uses only sigma^{xx}, sigma^{yy}, sigma^{xy}, sigma^{x eta},
+  // sigma^{y eta} (rows x, y and columns x, y, eta)
+  constexpr int m0 = FULL ? 0 : 1, m1 = FULL ? 4 : 3, v0 = FULL ? 0 : 1;
 #pragma unroll
-  for (int m = 1; m < 3; m++)
+  for (int m = m0; m < m1; m++)
 #pragma unroll
     for (int b = 0; b < 4; b++) {
       R s = 0;
@@ -412,9 +414,9 @@ VH_HD inline void is_kinematics(int cart, R tau, const R* u, const R du[4][4], R
       M[m][b] = s;
     }
 #pragma unroll
-  for (int m = 1; m < 3; m++)
+  for (int m = m0; m < m1; m++)
 #pragma unroll
-    for (int v = 1; v < 4; v++) {
+    for (int v = v0; v < 4; v++) {
       R s = 0;
 #pragma unroll
       for (int b = 0; b < 4; b++) s += M[m][b] * Dt[v][b];

@@ -41,10 +41,12 @@ struct HostEos {
 }  // namespace
 
 extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
-  if (!h || !path || every < 1 || layout < VH_WRITE_XY || layout > VH_WRITE_FULL17) return VH_E_ARG;
+  if (!h || !path || every < 1 || layout < VH_WRITE_XY || layout > VH_WRITE_NS_XY) return VH_E_ARG;
   const bool v17 = layout == VH_WRITE_XY17 || layout == VH_WRITE_FULL17;
-  const int NV = v17 ? 17 : 12;
+  const bool nsw = layout == VH_WRITE_NS_XY;
+  const int NV = nsw ? 11 : (v17 ? 17 : 12);
   if (v17) layout = layout == VH_WRITE_XY17 ? VH_WRITE_XY : VH_WRITE_FULL;
+  if (nsw) layout = VH_WRITE_XY;
   vh_config cfg;
   std::vector<double> tab;
   int r = vh_internal_config(h, &cfg, &tab);
@@ -60,6 +62,13 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
     pT.resize(n); pP.resize(n); pi10.resize(10 * (size_t)n);
     if ((r = vh_get_primitive(h, nullptr, pP.data(), pT.data(), nullptr, pi10.data()))) return r;
   }
+  // NEWEST10/write.h:123-170 (WriteNSXY): the ten Navier-Stokes pi^{mu nu}
+  // and the (zero) bulk part per cell
+  std::vector<double> nspi;
+  if (nsw) {
+    nspi.resize(10 * (size_t)n);
+    if ((r = vh_get_ns_pi(h, nspi.data()))) return r;
+  }
   HostEos eos;
   eos.kind = cfg.eos_kind;
   eos.a = cfg.eos_a;
@@ -74,6 +83,11 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
   const int nzi = bi ? 1 : cfg.nz, kl = bi ? 0 : 3;
   auto rec = [&](int i, int j, int k, double* o) {
     const long long c = ((long long)k * gy + j) * gx + i;
+    if (nsw) {
+      for (int l = 0; l < 10; l++) o[l] = nspi[(size_t)l * n + c];
+      o[10] = 0.0;  // no bulk viscosity
+      return;
+    }
     const double e = f[c], u0 = f[n + c];
     o[0] = e;
     o[1] = eos.T(e);

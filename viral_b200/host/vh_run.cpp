@@ -20,7 +20,8 @@
 //              conformal EOS with 42.25 degrees of freedom, eta/s 0.01/(4 pi)
 // Every run also stops at tau > 25.3 fm/c (main.cpp:211) or --tau-end.
 // Snapshots use the reference's names and layouts (res/tau%2.3ffm.bin, one xy
-// plane on boost-invariant grids, the full grid otherwise).
+// plane on boost-invariant grids, the full grid otherwise); with --ns each
+// comes with NEWEST10's Navier-Stokes file res/NStau%2.3ffm.bin.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -52,6 +53,7 @@ struct Options {
   bool quiet = false;
   std::string restart;      // resume from this restart file
   std::string checkpoint;   // write a restart file at the end
+  bool ns = false;          // also write res/NStau%2.3ffm.bin beside each snapshot
 };
 
 void usage() {
@@ -59,7 +61,7 @@ void usage() {
       "usage: vh_run [--scenario gubser|glauber|glauber3d|shocktube] [--nx N --ny N --nz N]\n"
       "              [--precision fp64|mixed] [--steps N] [--tau-end T] [--print-every T]\n"
       "              [--out DIR] [--every FREQ] [--b B] [--seed S] [--floor E_GeV_fm3] [--quiet]\n"
-      "              [--restart FILE] [--checkpoint FILE]\n");
+      "              [--restart FILE] [--checkpoint FILE] [--ns]\n");
 }
 
 bool parse(int argc, char** argv, Options& o) {
@@ -93,6 +95,7 @@ bool parse(int argc, char** argv, Options& o) {
     else if (a == "--quiet") o.quiet = true;
     else if (a == "--restart") o.restart = next("--restart");
     else if (a == "--checkpoint") o.checkpoint = next("--checkpoint");
+    else if (a == "--ns") o.ns = true;
     else { std::fprintf(stderr, "vh_run: unknown option %s\n", a.c_str()); usage(); return false; }
   }
   if (o.scenario != "gubser" && o.scenario != "glauber" && o.scenario != "glauber3d" && o.scenario != "shocktube") {
@@ -188,7 +191,11 @@ int main(int argc, char** argv) {
     if (o.out.empty()) return 0;
     char name[512];
     std::snprintf(name, sizeof name, "%s/tau%2.3ffm.bin", o.out.c_str(), tau);
-    return vh_write(h, name, layout, o.write_every);
+    if (int w = vh_write(h, name, layout, o.write_every)) return w;
+    if (!o.ns) return 0;
+    // NEWEST10/init.h:660-661 writes the Navier-Stokes pi of the initial state
+    std::snprintf(name, sizeof name, "%s/NStau%2.3ffm.bin", o.out.c_str(), tau);
+    return vh_write(h, name, VH_WRITE_NS_XY, o.write_every);
   };
   if (!o.out.empty()) mkdir(o.out.c_str(), 0755);
 

@@ -114,6 +114,12 @@ class Hydro:
         self._chk(A.lib().vh_get_primitive(self.h, A.ptr(e), A.ptr(P), A.ptr(T), A.ptr(u), A.ptr(pi)))
         return dict(e=e, P=P, T=T, u=u, pi=pi)
 
+    def get_ns_pi(self) -> np.ndarray:
+        """Navier-Stokes 2 eta sigma^{mu nu} (10, n: tt tx ty te xx xy xe yy ye ee)"""
+        out = np.zeros((10, self.n))
+        self._chk(A.lib().vh_get_ns_pi(self.h, A.ptr(out)))
+        return out
+
     def init_tmunu(self, tau: float, tmunu10: np.ndarray) -> int:
         """state from T^{mu nu} (10, n) by Landau matching; returns the cells
         without a timelike eigenpair (raises when there are any)"""
