@@ -57,7 +57,7 @@ enum { VH_RECON_WENO5 = 0, VH_RECON_MINMOD = 1 };
 enum { VH_EOS_CONFORMAL = 0, VH_EOS_TABLE = 1 };
 /* relaxation time: 1.5 eta / P (NEWEST5/maindef.h:69,126,286) or
  * 5 eta / (e + P) (NEWEST5/maindef.h:339, the Gubser test) */
-enum { VH_TAUPI_15_ETA_OVER_P = 0, VH_TAUPI_5_ETA_OVER_EPP = 1 };
+enum { VH_TAUPI_15_ETA_OVER_P = 0, VH_TAUPI_5_ETA_OVER_EPP = 1, VH_TAUPI_CONST = 2 };
 /* initial pi: given, zero, or Navier-Stokes (NEWEST5/Source.h:535-630) */
 enum { VH_PI_GIVEN = 0, VH_PI_ZERO = 1, VH_PI_NS = 2 };
 /* snapshot layouts: NEWEST5/write.h's 12 doubles per cell for one xy plane
@@ -87,6 +87,8 @@ typedef struct {
   int gubser_mirror;    /* ghost u^x,u^y mirrored across the face (NEWEST5/
                            boundary.h:32-37, Gubser test) */
   double minmod_theta;  /* generalized-minmod theta (NEWEST5/maindef.h:370) */
+  double taupi_const;   /* VH_TAUPI_CONST: tau_pi in fm/c (the Bjorken block,
+                           NEWEST5/maindef.h:228) */
 } vh_config;
 
 typedef struct vh_handle vh_handle;

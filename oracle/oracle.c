@@ -97,7 +97,7 @@ static inline void transport(const vho_config* c, double e, double P, double* et
   double tg = T * c->hbarc - c->etas_tc;
   double etas = c->etas0 + c->etas1 * (tg > 0 ? tg : 0.0);
   *eta = etas * s;
-  *taupi = (c->taupi_kind == 1) ? 5.0 * (*eta) / (e + P) : 1.5 * ((*eta) / P);
+  *taupi = (c->taupi_kind == 1) ? 5.0 * (*eta) / (e + P) : c->taupi_kind == 2 ? c->taupi_const : 1.5 * ((*eta) / P);
 }
 
 void vho_eos(const vho_grid* g, double e, double* out) {

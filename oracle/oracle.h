@@ -44,11 +44,13 @@ typedef struct {
    * s = (e + P)/T; T in GeV inside the bracket */
   double etas0, etas1, etas_tc, hbarc;
   /* relaxation time: 0 -> 1.5 eta / P (NEWEST5/maindef.h:69);
-   *                  1 -> 5 eta / (e + P) (NEWEST5/maindef.h:339) */
+   *                  1 -> 5 eta / (e + P) (NEWEST5/maindef.h:339);
+   *                  2 -> taupi_const (NEWEST5/maindef.h:228, Bjorken) */
   int taupi_kind;
   int gubser_mirror;    /* ghost u^x,u^y mirrored (NEWEST5/boundary.h:32-37) */
   int recon;            /* 0: WENO5 (reference); 1: generalized minmod */
   double minmod_theta;  /* generalized minmod theta (NEWEST5/maindef.h:370) */
+  double taupi_const;   /* taupi_kind 2: constant tau_pi (NEWEST5/maindef.h:228) */
 } vho_config;
 
 typedef struct vho_grid vho_grid;

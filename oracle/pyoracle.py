@@ -36,7 +36,7 @@ class _Cfg(ctypes.Structure):
         ("etas0", ctypes.c_double), ("etas1", ctypes.c_double), ("etas_tc", ctypes.c_double),
         ("hbarc", ctypes.c_double),
         ("taupi_kind", ctypes.c_int), ("gubser_mirror", ctypes.c_int),
-        ("recon", ctypes.c_int), ("minmod_theta", ctypes.c_double),
+        ("recon", ctypes.c_int), ("minmod_theta", ctypes.c_double), ("taupi_const", ctypes.c_double),
     ]
 
 
@@ -57,7 +57,8 @@ class OracleConfig:
     etas1: float = 0.0
     etas_tc: float = 0.154
     hbarc: float = 0.19733
-    taupi_kind: int = 0        # 0: 1.5 eta/P, 1: 5 eta/(e+P)
+    taupi_kind: int = 0        # 0: 1.5 eta/P, 1: 5 eta/(e+P), 2: taupi_const
+    taupi_const: float = 0.0
     gubser_mirror: bool = False
     recon: int = 0             # 0 WENO5, 1 generalized minmod
     minmod_theta: float = 1.1
@@ -83,6 +84,7 @@ class OracleConfig:
         c.taupi_kind = self.taupi_kind
         c.gubser_mirror = int(self.gubser_mirror)
         c.recon, c.minmod_theta = self.recon, self.minmod_theta
+        c.taupi_const = self.taupi_const
         return c
 
 

@@ -16,7 +16,8 @@ Outputs are stored at a seeded sample of interior cells (plus per-field
 sums over the whole grid), so that the fixtures stay small.  A fifth
 fixture, cart_3d_shock, is the reference's own Cartesian scenario (the
 shock tube of its default TXYZ5 block) after 20 steps; a sixth, ns10_lbi,
-is NEWEST10's ten-component Navier-Stokes shear tensor (CalcNS).  The CPU tests
+is NEWEST10's ten-component Navier-Stokes shear tensor (CalcNS); a
+seventh, bjorken, is the reference's Bjorken scenario run to tau = 10.  The CPU tests
 rebuild the same inputs and check the oracle against these numbers.
 """
 from __future__ import annotations
@@ -141,6 +142,41 @@ def make_shock() -> dict:
             "state": s[:14, cells], "state_sum": s.sum(axis=1)}
 
 
+BJORKEN_STEPS = 940
+
+
+def make_bjorken() -> dict:
+    """The reference's Bjorken scenario (NEWEST5/maindef.h:195-235,
+    init.h:283-340): a uniform fluid at rest in Milne coordinates with
+    e = 30 GeV/fm^3 at tau = 0.6 fm/c, run BJORKEN_STEPS steps of 0.01 fm/c to
+    tau = 10 (main.cpp:208-211).  Records, after every step, the centre
+    cell's temperature in fm^-1 (main.cpp:146 prints it times GEVFM/1000),
+    and the final state of the centre cell."""
+    R = RefBuild("bjorken")
+    sc = dict(etas0=0.2, taupi_kind=2, taupi_const=0.01, cartesian=False, mirror=False)
+    cfg = OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=1, boost_invariant=True, cartesian=False, dx=R.dx, dy=R.dy,
+                       dz=R.dz, eos_kind=0, eos_a=R.factor, etas0=sc["etas0"], etas1=0.0, hbarc=R.gevfm,
+                       taupi_kind=2, taupi_const=0.01)
+    f = np.zeros((18, R.n))
+    f[0] = 30.0 / R.gevfm
+    f[1] = 1.0
+    f[14] = 1.0
+    O = Oracle(cfg)
+    O.set_state(f)
+    O.fill_tmunu(0.6)
+    f = O.get_state()
+    R.set_state(f)
+    centre = (R.gy // 2) * R.gx + R.gx // 2
+    tau, temps = 0.6, []
+    for _ in range(BJORKEN_STEPS):
+        R.step(tau, 0.01)
+        tau += 0.01
+        temps.append(R.eos(R.get_state()[0, centre])[2])
+    return {"tau0": 0.6, "ts": 0.01, "steps": BJORKEN_STEPS, "centre": centre,
+            "dims": np.array([R.gx, R.gy, R.gz, 1]), "consts": np.array([R.dx, R.dy, R.dz, R.factor, R.gevfm]),
+            "temp": np.array(temps), "final": R.get_state()[:, centre]}
+
+
 NS10_TAU = 1.3
 NS10_SEED = 11
 
@@ -165,9 +201,10 @@ def make_ns10() -> dict:
 
 
 def main():
-    which = sys.argv[1:] or list(SCENARIOS) + ["cart_3d_shock", "ns10_lbi"]
+    special = {"cart_3d_shock": make_shock, "ns10_lbi": make_ns10, "bjorken": make_bjorken}
+    which = sys.argv[1:] or list(SCENARIOS) + list(special)
     for v in which:
-        d = make_shock() if v == "cart_3d_shock" else make_ns10() if v == "ns10_lbi" else make(v)
+        d = special[v]() if v in special else make(v)
         path = os.path.join(HERE, f"ref_{v}.npz")
         np.savez_compressed(path, **d)
         print(path, os.path.getsize(path))

@@ -54,11 +54,12 @@ def arr(n):
 
 
 def cfgs():
-    """conformal and tabulated EOS; both tau_pi forms; eta/s with a T kink"""
+    """conformal and tabulated EOS; the three tau_pi forms; eta/s with a T kink"""
     a = C.glauber_config(nx=8, ny=8, boost_invariant=True, etas0=0.08, etas1=1.0)
     b = Config(nx=8, ny=8, eos_kind=A.EOS_CONFORMAL, etas0=0.2, etas1=0.5, etas_tc=0.154,
                taupi_kind=A.TAUPI_5_ETA_OVER_EPP)
-    return [("table", a), ("conformal", b)]
+    c = C.bjorken_config(nx=8, ny=8)  # tau_pi a constant 0.01 fm/c
+    return [("table", a), ("conformal", b), ("const_taupi", c)]
 
 
 def fd(f, x, h):
@@ -135,7 +136,7 @@ def src_inputs(rng, e):
     return np.array([e, u0, u1, u2, *p, *du])
 
 
-@pytest.mark.parametrize("which", ["table", "conformal"])
+@pytest.mark.parametrize("which", ["table", "conformal", "const_taupi"])
 def test_src2d_vjp(L, which):
     rng = np.random.default_rng(3 if which == "table" else 4)
     cfg = dict(cfgs())[which]
@@ -165,7 +166,7 @@ def test_src2d_vjp(L, which):
             check_vjp(J, got, ob, 5e-6)
 
 
-@pytest.mark.parametrize("which", ["table", "conformal"])
+@pytest.mark.parametrize("which", ["table", "conformal", "const_taupi"])
 def test_con2prim_ift_vjp(L, which):
     rng = np.random.default_rng(7)
     cfg = dict(cfgs())[which]
@@ -203,7 +204,7 @@ def test_con2prim_ift_vjp(L, which):
             check_vjp(J, np.concatenate([Tb, pb]), xb, 2e-6)
 
 
-@pytest.mark.parametrize("which", ["table", "conformal"])
+@pytest.mark.parametrize("which", ["table", "conformal", "const_taupi"])
 def test_eos_derivative(L, which):
     cfg = dict(cfgs())[which]
     c = cfg.to_c()

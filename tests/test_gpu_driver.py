@@ -83,6 +83,27 @@ def test_driver_navier_stokes_files(tmp_path):
     assert open(last, "rb").read() == open(os.path.join(out, "NStau1.030fm.bin"), "rb").read()
 
 
+def test_driver_bjorken_temperature_file(tmp_path):
+    """--scenario bjorken writes ./temp.txt as the reference's main loop
+    does: per step the tau the step started from and the centre cell's
+    T (fm^-1) x 0.1973 / 1000, until tau > 10 fm/c"""
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_bjorken.npz"))
+    r = subprocess.run([build.build_driver(), "--scenario", "bjorken", "--quiet"], capture_output=True, text=True,
+                       timeout=600, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    rows = np.loadtxt(os.path.join(str(tmp_path), "temp.txt"))
+    tau, nsteps = 0.6, 0
+    while True:  # the reference's loop: tau += ts, break once tau > 10
+        tau += 0.01
+        nsteps += 1
+        if tau > 10:
+            break
+    assert rows.shape == (nsteps, 2)
+    assert np.allclose(rows[:, 0], 0.6 + 0.01 * np.arange(nsteps), atol=1e-9)
+    m = min(nsteps, len(g["temp"]))
+    assert np.allclose(rows[:m, 1], g["temp"][:m] * 0.1973 / 1000, rtol=1e-5, atol=0)
+
+
 def test_get_primitive():
     cfg = C.gubser_config(nx=21, ny=21)
     with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:

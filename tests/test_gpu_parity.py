@@ -219,3 +219,25 @@ def test_cartesian_shock_tube_matches_reference(precision):
         worst = max(worst, err)
     print("shock tube, precision %d: max error %.2e" % (precision, worst))
     assert worst <= tol
+
+
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_bjorken_scenario_matches_reference(precision):
+    """The reference's Bjorken scenario, 940 steps to tau = 10 fm/c: the
+    centre temperature after every step against the compiled reference's
+    (tests/golden/ref_bjorken.npz); FP64 to 1e-12, mixed to 1e-5"""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_bjorken.npz"))
+    cfg = C.bjorken_config(precision=precision)
+    c = int(g["centre"])
+    temps = []
+    with C.make_hydro(cfg, C.bjorken_inputs(cfg)) as H:
+        for _ in range(int(g["steps"])):
+            H.step(1)
+            temps.append(H.get_primitive()["T"][c])
+        final = H.get_state()[:, c]
+    err = float(np.max(np.abs(np.array(temps) - g["temp"]) / g["temp"]))
+    print("Bjorken %s: max rel err of T over 940 steps %.2e" % ("fp64" if precision == A.PREC_FP64 else "mixed", err))
+    assert err <= (1e-12 if precision == A.PREC_FP64 else 1e-5)
+    if precision == A.PREC_FP64:
+        assert np.max(np.abs(final - g["final"])) <= 1e-12 * np.max(np.abs(g["final"]))

@@ -156,3 +156,43 @@ def test_navier_stokes_shear_ten_components():
     du0[3::4] = 0
     again = np.array([O.ns_pi10_cell(tau, f[0, c], f[1:5, c], du0[:, a]) for a, c in enumerate(cells)]).T
     assert np.array_equal(grid[:, cells], again)
+
+
+def bjorken_oracle(g):
+    gx, gy, gz, _ = (int(v) for v in g["dims"])
+    dx, dy, dz, factor, gevfm = (float(v) for v in g["consts"])
+    cfg = OracleConfig(nx=gx - 6, ny=gy - 6, nz=1, boost_invariant=True, dx=dx, dy=dy, dz=dz, eos_kind=0,
+                       eos_a=factor, etas0=0.2, etas1=0.0, hbarc=gevfm, taupi_kind=2, taupi_const=0.01)
+    f = np.zeros((18, gx * gy))
+    f[0] = 30.0 / gevfm
+    f[1] = 1.0
+    f[14] = 1.0
+    O = Oracle(cfg)
+    O.set_state(f)
+    O.fill_tmunu(float(g["tau0"]))
+    return O
+
+
+def test_bjorken_scenario():
+    """The reference's Bjorken scenario (uniform fluid at rest in Milne
+    coordinates, eta/s = 0.2, tau_pi = 0.01 fm/c) to tau = 10 fm/c: the
+    oracle's centre temperature after every step is the reference's, and it
+    follows first-order viscous Bjorken flow,
+    T = T0 (tau0/tau)^(1/3) [1 + 2 (eta/s) (1 - (tau0/tau)^(2/3)) / (3 tau0 T0)],
+    to 0.2 % (the viscous heating itself is 10 % at tau = 10)"""
+    g = np.load(os.path.join(GOLD, "ref_bjorken.npz"))
+    O = bjorken_oracle(g)
+    c, ts = int(g["centre"]), float(g["ts"])
+    tau, temps = float(g["tau0"]), []
+    for _ in range(int(g["steps"])):
+        assert O.step(tau, ts) == 0
+        tau += ts
+        temps.append(O.eos(O.get_state()[0, c])[2])
+    temps = np.array(temps)
+    assert np.max(np.abs(temps - g["temp"]) / g["temp"]) <= TOL
+    assert scaled_err(O.get_state()[:, c], g["final"]) <= TOL
+    t0, T0 = float(g["tau0"]), (30.0 / float(g["consts"][4]) / float(g["consts"][3])) ** 0.25
+    taus = t0 + ts * np.arange(1, len(temps) + 1)
+    first_order = T0 * (t0 / taus) ** (1 / 3) * (1 + 2 * 0.2 * (1 - (t0 / taus) ** (2 / 3)) / (3 * t0 * T0))
+    assert np.max(np.abs(temps / first_order - 1)) <= 2e-3
+    assert temps[-1] / (T0 * (t0 / taus[-1]) ** (1 / 3)) - 1 > 0.09

@@ -25,7 +25,7 @@ COORD_MILNE, COORD_CARTESIAN = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 RECON_WENO5, RECON_MINMOD = 0, 1
 EOS_CONFORMAL, EOS_TABLE = 0, 1
-TAUPI_15_ETA_OVER_P, TAUPI_5_ETA_OVER_EPP = 0, 1
+TAUPI_15_ETA_OVER_P, TAUPI_5_ETA_OVER_EPP, TAUPI_CONST = 0, 1, 2
 PI_GIVEN, PI_ZERO, PI_NS = 0, 1, 2
 WRITE_XY, WRITE_FULL, WRITE_XY17, WRITE_FULL17, WRITE_NS_XY = 0, 1, 2, 3, 4
 
@@ -43,6 +43,7 @@ class VhConfig(ctypes.Structure):
         ("etas0", ctypes.c_double), ("etas1", ctypes.c_double), ("etas_tc", ctypes.c_double),
         ("hbarc", ctypes.c_double),
         ("taupi_kind", ctypes.c_int), ("gubser_mirror", ctypes.c_int), ("minmod_theta", ctypes.c_double),
+        ("taupi_const", ctypes.c_double),
     ]
 
 

@@ -28,6 +28,30 @@ def eos_table() -> np.ndarray:
     return _EOS_CACHE["t"]
 
 
+BJORKEN_GEVFM = 0.1973                     # the reference's GEVFM (NEWEST5/main.cpp:46)
+BJORKEN_A = 3 * 42.25 * math.pi ** 2 / 90  # FACTOR, DOF = 42.25 (NEWEST5/maindef.h)
+BJORKEN_E0 = 30.0 / BJORKEN_GEVFM           # 30 GeV/fm^3 (NEWEST5/init.h:292)
+
+
+def bjorken_config(nx=10, ny=10, precision=A.PREC_FP64) -> Config:
+    """The reference's Bjorken scenario block (NEWEST5/maindef.h:195-235):
+    a uniform boost-invariant fluid, 10x10 cells of 0.1 fm, tau0 = 0.6 fm/c,
+    dtau = 0.01, conformal e = a T^4 with 42.25 degrees of freedom,
+    eta = 0.2 s, tau_pi = 0.01 fm/c."""
+    return Config(nx=nx, ny=ny, nz=1, boost_invariant=True, precision=precision, dx=0.1, dy=0.1, tau0=0.6,
+                  dtau=0.01, eos_kind=A.EOS_CONFORMAL, eos_a=BJORKEN_A, etas0=0.2, etas1=0.0,
+                  hbarc=BJORKEN_GEVFM, taupi_kind=A.TAUPI_CONST, taupi_const=0.01)
+
+
+def bjorken_inputs(cfg: Config):
+    """NEWEST5/init.h:283-340: e = 30 GeV/fm^3 on every cell, at rest in
+    Milne coordinates (Bjorken flow), prevu = u, pi = 0."""
+    gx, gy, gz = cfg.gdims()
+    n = gx * gy * gz
+    z = np.zeros(n)
+    return dict(tau=cfg.tau0, e=np.full(n, BJORKEN_E0), ux=z, uy=z.copy(), ueta=None, prevu=None, pi_mode=A.PI_ZERO)
+
+
 def gubser_config(nx=129, ny=129, dx=0.1, precision=A.PREC_FP64, recon=A.RECON_WENO5) -> Config:
     return Config(nx=nx, ny=ny, nz=1, boost_invariant=True, precision=precision, recon=recon, dx=dx, dy=dx,
                   tau0=1.0, dtau=0.01, eos_kind=A.EOS_CONFORMAL, eos_a=A_QGP, etas0=0.2, etas1=0.0,

@@ -214,7 +214,7 @@ VH_HD inline void src2d_vjp(const DevCfg& C, R tau, R e, const R* u3v, const R* 
   const bool kink = tg > (R)0;
   const R etas = (R)C.etas0 + (R)C.etas1 * (kink ? tg : (R)0);
   const R eta = etas * s;
-  const R tp = C.taupi_kind == 1 ? (R)5 * eta * iep : (R)1.5 * (eta * iP);
+  const R tp = C.taupi_kind == 1 ? (R)5 * eta * iep : C.taupi_kind == 2 ? (R)C.taupi_c : (R)1.5 * (eta * iP);
   const R itp = (R)1 / tp;
   const R u0 = u[0], u1 = u[1], u2 = u[2];
   const R iu0 = (R)1 / u0, iD = iu0 * iu0, it2 = (R)1 / t2;
@@ -359,7 +359,7 @@ VH_HD inline void src2d_vjp(const DevCfg& C, R tau, R e, const R* u3v, const R* 
     etab += tpb * (R)5 * iep;
     const R eppb = -tpb * (R)5 * eta * (iep * iep);
     eb_ += eppb; Pb += eppb;
-  } else {
+  } else if (C.taupi_kind == 0) {
     etab += tpb * (R)1.5 * iP;
     Pb -= tpb * (R)1.5 * eta * (iP * iP);
   }

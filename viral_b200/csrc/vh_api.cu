@@ -33,7 +33,9 @@ static int validate(const vh_config* c, std::string& why) {
     for (int i = 1; i < c->eos_n; i++)
       if (!(c->eos_e[i] > c->eos_e[i - 1])) { why = "eos table e must increase"; return VH_E_ARG; }
   } else { why = "eos_kind"; return VH_E_ARG; }
-  if (c->taupi_kind != VH_TAUPI_15_ETA_OVER_P && c->taupi_kind != VH_TAUPI_5_ETA_OVER_EPP) { why = "taupi_kind"; return VH_E_ARG; }
+  if (c->taupi_kind != VH_TAUPI_15_ETA_OVER_P && c->taupi_kind != VH_TAUPI_5_ETA_OVER_EPP &&
+      c->taupi_kind != VH_TAUPI_CONST) { why = "taupi_kind"; return VH_E_ARG; }
+  if (c->taupi_kind == VH_TAUPI_CONST && !(c->taupi_const > 0)) { why = "taupi_const"; return VH_E_ARG; }
   return VH_OK;
 }
 
@@ -62,6 +64,7 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
   C.eos_kind = cfg->eos_kind; C.eos_a = cfg->eos_a; C.eos_n = 0;
   C.etas0 = cfg->etas0; C.etas1 = cfg->etas1; C.etas_tc = cfg->etas_tc; C.hbarc = cfg->hbarc;
   C.taupi_kind = cfg->taupi_kind;
+  C.taupi_c = cfg->taupi_const;
   C.mm_theta = cfg->minmod_theta;
   h->tau = cfg->tau0;
 

@@ -30,6 +30,7 @@ struct DevCfg {
   const float* eos_f;           // the same in float
   double etas0, etas1, etas_tc, hbarc;
   int taupi_kind;
+  double taupi_c;               // tau_pi of VH_TAUPI_CONST
   double mm_theta;
 };
 
@@ -181,7 +182,7 @@ VH_HD inline void transport_T(const DevCfg& C, R e, R P, R T, R* eta, R* taupi) 
   R tg = T * (R)C.hbarc - (R)C.etas_tc;
   R etas = (R)C.etas0 + (R)C.etas1 * (tg > (R)0 ? tg : (R)0);
   *eta = etas * s;
-  *taupi = (C.taupi_kind == 1) ? (R)5 * (*eta) / (e + P) : (R)1.5 * ((*eta) / P);
+  *taupi = (C.taupi_kind == 1) ? (R)5 * (*eta) / (e + P) : C.taupi_kind == 2 ? (R)C.taupi_c : (R)1.5 * ((*eta) / P);
 }
 template <class R>
 VH_HD inline void transport(const DevCfg& C, R e, R P, R* eta, R* taupi) {
@@ -190,7 +191,7 @@ VH_HD inline void transport(const DevCfg& C, R e, R P, R* eta, R* taupi) {
   R tg = T * (R)C.hbarc - (R)C.etas_tc;
   R etas = (R)C.etas0 + (R)C.etas1 * (tg > (R)0 ? tg : (R)0);
   *eta = etas * s;
-  *taupi = (C.taupi_kind == 1) ? (R)5 * (*eta) / (e + P) : (R)1.5 * ((*eta) / P);
+  *taupi = (C.taupi_kind == 1) ? (R)5 * (*eta) / (e + P) : C.taupi_kind == 2 ? (R)C.taupi_c : (R)1.5 * ((*eta) / P);
 }
 
 // --------------------------------------------------- pi closure (A1..A5)

@@ -18,6 +18,13 @@
 //              init.h:151-210): 10x10x101 cells of 0.1 fm, t0 = 0, dt 0.01,
 //              e = 16 fm^-4 for z < 0 and 1 fm^-4 for z >= 0 at rest,
 //              conformal EOS with 42.25 degrees of freedom, eta/s 0.01/(4 pi)
+//   bjorken    the Bjorken block of NEWEST5 (maindef.h:195-235, init.h:283-340):
+//              10x10 boost-invariant cells of 0.1 fm, e = 30 GeV/fm^3 at rest,
+//              tau0 0.6, dtau 0.01, conformal EOS with 42.25 degrees of
+//              freedom, eta = 0.2 s, tau_pi = 0.01 fm/c; after each step the
+//              centre cell's T (fm^-1) times GEVFM/1000 goes to ./temp.txt
+//              beside the tau the step started from (main.cpp:145-147);
+//              stops after tau > 10 fm/c (main.cpp:199-210)
 // Every run also stops at tau > 25.3 fm/c (main.cpp:211) or --tau-end.
 // Snapshots use the reference's names and layouts (res/tau%2.3ffm.bin, one xy
 // plane on boost-invariant grids, the full grid otherwise); with --ns each
@@ -58,7 +65,7 @@ struct Options {
 
 void usage() {
   std::printf(
-      "usage: vh_run [--scenario gubser|glauber|glauber3d|shocktube] [--nx N --ny N --nz N]\n"
+      "usage: vh_run [--scenario gubser|glauber|glauber3d|shocktube|bjorken] [--nx N --ny N --nz N]\n"
       "              [--precision fp64|mixed] [--steps N] [--tau-end T] [--print-every T]\n"
       "              [--out DIR] [--every FREQ] [--b B] [--seed S] [--floor E_GeV_fm3] [--quiet]\n"
       "              [--restart FILE] [--checkpoint FILE] [--ns]\n");
@@ -117,6 +124,7 @@ int main(int argc, char** argv) {
   if (!parse(argc, argv, o)) return 2;
   const bool gubser = o.scenario == "gubser", three_d = o.scenario == "glauber3d";
   const bool shock = o.scenario == "shocktube";
+  const bool bjorken = o.scenario == "bjorken";
 
   vh_config c;
   std::memset(&c, 0, sizeof c);
@@ -133,6 +141,12 @@ int main(int argc, char** argv) {
     c.eos_kind = VH_EOS_CONFORMAL; c.eos_a = 3 * 42.25 * M_PI * M_PI / 90;
     c.hbarc = 0.1973;
     c.etas0 = 0.01 / (4 * M_PI); c.etas_tc = 0.154; c.taupi_kind = VH_TAUPI_15_ETA_OVER_P;
+  } else if (bjorken) {
+    c.nx = o.nx ? o.nx : 10; c.ny = o.ny ? o.ny : 10; c.nz = 1; c.boost_invariant = 1;
+    c.dx = c.dy = 0.1; c.dz = 1.0; c.tau0 = 0.6; c.dtau = 0.01;
+    c.eos_kind = VH_EOS_CONFORMAL; c.eos_a = 3 * 42.25 * M_PI * M_PI / 90;
+    c.hbarc = 0.1973;
+    c.etas0 = 0.2; c.etas_tc = 0.154; c.taupi_kind = VH_TAUPI_CONST; c.taupi_const = 0.01;
   } else if (gubser) {
     c.nx = o.nx ? o.nx : 129; c.ny = o.ny ? o.ny : 129; c.nz = 1; c.boost_invariant = 1;
     c.dx = c.dy = 0.1; c.dz = 1.0; c.tau0 = 1.0; c.dtau = 0.01;
@@ -166,6 +180,9 @@ int main(int argc, char** argv) {
         const double z = -((c.nz / 2) * c.dz) + (k - VH_NGHOST) * c.dz;
         e[(size_t)k * gx * gy + q] = z < 0 ? 16.0 : 1.0;
       }
+    r = vh_init_profile(h, c.tau0, e.data(), ux.data(), uy.data(), nullptr, nullptr, VH_PI_ZERO, nullptr);
+  } else if (bjorken) {
+    for (size_t q = 0; q < n; q++) e[q] = 30.0 / c.hbarc;
     r = vh_init_profile(h, c.tau0, e.data(), ux.data(), uy.data(), nullptr, nullptr, VH_PI_ZERO, nullptr);
   } else if (gubser) {
     r = vh_profile_gubser(c.nx, c.ny, c.dx, c.dy, 1.0, c.tau0, c.dtau, 0.6, c.eos_a, kHbarc, e.data(), ux.data(),
@@ -206,8 +223,20 @@ int main(int argc, char** argv) {
   if (o.restart.empty() && (r = write(tau))) { const int code = fail("vh_write", h, r); vh_destroy(h); return code; }
   const auto start = std::chrono::steady_clock::now();
   int status = 0;
+  FILE* temp_txt = bjorken ? std::fopen("temp.txt", "w") : nullptr;
+  if (bjorken && !temp_txt) { const int code = fail("temp.txt", h, VH_E_ARG); vh_destroy(h); return code; }
+  std::vector<double> tcell(bjorken ? n : 0);
+  const size_t centre = (size_t)(gy / 2) * gx + gx / 2;  // HydroGrid[XCM/2][YCM/2][0]
   while (true) {
     if ((r = vh_step(h, 1))) { status = fail("vh_step", h, r); break; }
+    if (bjorken) {
+      // main.cpp:146: tau before the increment, fmtoMev(FT(e)) / 1000
+      if ((r = vh_get_primitive(h, nullptr, nullptr, tcell.data(), nullptr, nullptr))) {
+        status = fail("vh_get_primitive", h, r);
+        break;
+      }
+      std::fprintf(temp_txt, "%g  %g\n", tau, tcell[centre] * c.hbarc / 1000);
+    }
     tau += ts;
     double tmax_gev = 0;
     if ((r = vh_max_temperature(h, &tmax_gev))) { status = fail("vh_max_temperature", h, r); break; }
@@ -224,10 +253,12 @@ int main(int argc, char** argv) {
     if (std::fabs(tau - (c.tau0 + ts)) < 1e-6 && (r = write(tau))) { status = fail("vh_write", h, r); break; }
     l++;
     if (gubser && tau > 9) break;             // main.cpp:196-199
-    if (!gubser && !shock && tmax_mev < 120) break;  // main.cpp:201-204
+    if (!gubser && !shock && !bjorken && tmax_mev < 120) break;  // main.cpp:201-204
+    if (bjorken && tau > 10) break;           // main.cpp:208-210
     if (tau > o.tau_end) break;                // main.cpp:211
     if (o.max_steps > 0 && l > o.max_steps) break;
   }
+  if (temp_txt) std::fclose(temp_txt);
   if (!status && !o.checkpoint.empty() && (r = vh_save_checkpoint(h, o.checkpoint.c_str())))
     status = fail("vh_save_checkpoint", h, r);
   double sums[4];

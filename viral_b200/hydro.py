@@ -43,6 +43,7 @@ class Config:
     taupi_kind: int = A.TAUPI_15_ETA_OVER_P
     gubser_mirror: bool = False
     minmod_theta: float = 1.1
+    taupi_const: float = 0.0  # tau_pi (fm/c) with TAUPI_CONST
     _keep: list = field(default_factory=list, repr=False)
 
     def gdims(self):
@@ -65,6 +66,7 @@ class Config:
         c.taupi_kind = self.taupi_kind
         c.gubser_mirror = int(self.gubser_mirror)
         c.minmod_theta = self.minmod_theta
+        c.taupi_const = self.taupi_const
         return c
 
 
