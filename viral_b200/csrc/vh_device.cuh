@@ -575,8 +575,12 @@ VH_HD inline bool solve4(double A[4][4], double b[4]) {
 // (about 1.5 more iterations per cell, and warps wait for their slowest
 // cell).  The Jacobian is formed together with the residual at every trial
 // point, so an accepted full step (the common case) costs one evaluation.
+// With qtol > 0 the loop also stops after an undamped step with every
+// |dx_i| <= qtol |x_i| (or dx_i = 0): in the quadratic regime the error left
+// after such a step is of order |dx|^2, so qtol = 1e-8 leaves ~1e-16 and
+// saves the confirming iteration whose step would fall below rtol.
 VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, double tau, double* x,
-                               double rtol = 1e-16) {
+                               double rtol = 1e-16, double qtol = 0.0) {
   const double t2 = C.cart ? 1.0 : tau * tau;
   double y[4], J[4][4];
   c2p_fj(C, Tt, p, t2, x, y, J, true);
@@ -601,13 +605,15 @@ VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, do
       t *= (sqrt(1.0 + 6.0 * r) - 1.0) / (3.0 * r);
     }
     if (!ok) return -1;
-    bool conv = true;
+    bool conv = true, quad = t == 1.0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       double dx = xt[i] - x[i];
       x[i] = xt[i];
       if (!(fabs(dx) < rtol * fabs(x[i]) || dx == 0.0)) conv = false;
+      if (!(fabs(dx) <= qtol * fabs(x[i]) || dx == 0.0)) quad = false;
     }
+    if (quad) conv = true;
     phi = phi1;
     if (conv) break;
   }

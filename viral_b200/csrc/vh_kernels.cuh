@@ -479,7 +479,7 @@ __device__ __forceinline__ unsigned root_cell(const DevCfg& C, const DevPtrs<R>&
     for (int l = 0; l < 4; l++) Tt[l] = (double)q9[l];
 #pragma unroll
     for (int l = 0; l < 5; l++) pd[l] = (double)q9[4 + l];
-    const int it = con2prim(C, Tt, pd, tau1, x, sizeof(R) == 4 ? 1e-10 : 1e-13);
+    const int it = con2prim(C, Tt, pd, tau1, x, sizeof(R) == 4 ? 1e-10 : 1e-13, sizeof(R) == 4 ? 1e-6 : 1e-8);
     if (it < 0) {
       atomicOr(P.status, ST_ROOT);
     } else {

@@ -105,7 +105,8 @@ bool parse(int argc, char** argv, Options& o) {
     else if (a == "--ns") o.ns = true;
     else { std::fprintf(stderr, "vh_run: unknown option %s\n", a.c_str()); usage(); return false; }
   }
-  if (o.scenario != "gubser" && o.scenario != "glauber" && o.scenario != "glauber3d" && o.scenario != "shocktube") {
+  if (o.scenario != "gubser" && o.scenario != "glauber" && o.scenario != "glauber3d" && o.scenario != "shocktube" &&
+      o.scenario != "bjorken") {
     std::fprintf(stderr, "vh_run: unknown scenario %s\n", o.scenario.c_str());
     return false;
   }
