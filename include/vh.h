@@ -175,6 +175,13 @@ int vh_write(vh_handle* h, const char* path, int layout, int every);
  * t-eta, xx, xy, x-eta, yy, y-eta, eta-eta, Pi), NEWEST10/write.h:51-115 and
  * its WriteResults. */
 
+/* The reference's evolved variables Var[10] on every cell (CopyPrimary-
+ * VariablesToVar, NEWEST5/hydroKT.h:345-361): tau T^{tau mu} (T^{t mu} in
+ * Cartesian coordinates, TXYZ5/hydroKT.h:270-286), pi^{xx}, pi^{yy},
+ * pi^{xy}, pi^{x eta}, pi^{y eta}, and the bulk pressure (zero): 10 fields
+ * of the ghost-inclusive grid. */
+int vh_get_conserved(vh_handle* h, double* var10);
+
 /* VH_WRITE_NS_XY: NEWEST10's Navier-Stokes snapshot (WriteNSXY,
  * NEWEST10/write.h:123-170, written as res/NStau%2.3ffm.bin): 11 doubles
  * per cell, the ten components of vh_get_ns_pi and a zero bulk part, in the

@@ -241,3 +241,18 @@ def test_bjorken_scenario_matches_reference(precision):
     assert err <= (1e-12 if precision == A.PREC_FP64 else 1e-5)
     if precision == A.PREC_FP64:
         assert np.max(np.abs(final - g["final"])) <= 1e-12 * np.max(np.abs(g["final"]))
+
+
+@pytest.mark.parametrize("cfgkw", [dict(), dict(coords=A.COORD_CARTESIAN, tau0=1.0)])
+def test_get_conserved(cfgkw):
+    """the reference's Var: tau T^{tau mu} (T^{t mu} in Cartesian), pi, 0"""
+    cfg = milne3d(**cfgkw)
+    f = smooth_inputs(cfg, cfg.tau0, seed=2)
+    with Hydro(cfg) as H:
+        H.set_state(f, cfg.tau0)
+        H.step(2)
+        s, tau, var = H.get_state(), H.tau, H.get_conserved()
+    t = 1.0 if cfg.coords == A.COORD_CARTESIAN else tau
+    assert np.array_equal(var[:4], t * s[10:14])
+    assert np.array_equal(var[4:9], s[5:10])
+    assert np.all(var[9] == 0)

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -331,6 +332,22 @@ static int ns_pi10(vh_handle* h, const DevPtrs<R>& P, double* out) {
   k_du_full<R><<<grid1(C.n, 128), 128, 0, h->stream>>>(C, P, du16, h->cfg.dtau);
   k_ns_pi10<R><<<grid1(C.n, 128), 128, 0, h->stream>>>(C, P, du16, h->tau, out);
   VH_CUDA(h, cudaGetLastError());
+  return VH_OK;
+}
+
+extern "C" int vh_get_conserved(vh_handle* h, double* var10) {
+  if (!h || !var10) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  const size_t n = (size_t)h->C.n;
+  std::vector<double> f(18 * n);
+  int r = vh_get_state(h, f.data());
+  if (r) return r;
+  // NEWEST5/hydroKT.h:345-361 (TXYZ5/hydroKT.h:270-286 without the tau)
+  const double t = h->C.cart ? 1.0 : h->tau;
+  for (int l = 0; l < 4; l++)
+    for (size_t c = 0; c < n; c++) var10[l * n + c] = t * f[(10 + l) * n + c];
+  for (int l = 0; l < 5; l++) std::copy(f.begin() + (5 + l) * n, f.begin() + (6 + l) * n, var10 + (4 + l) * n);
+  std::fill(var10 + 9 * n, var10 + 10 * n, 0.0);  // bulk pressure: not evolved
   return VH_OK;
 }
 

@@ -496,8 +496,25 @@ __device__ __forceinline__ unsigned root_cell(const DevCfg& C, const DevPtrs<R>&
       for (int l = 0; l < 4; l++) P.u(l)[c] = u[l];
     }
     // ghost copy of boundary cells: faces only, corners untouched
-    // (NEWEST5/boundary.h:1-276); Gubser test mirrors u^x,u^y
+    // (NEWEST5/boundary.h:1-276); Gubser test mirrors u^x,u^y.  A boundary
+    // cell reads back the conserved set and prevu it stored above, so that
+    // they need not stay in registers through the root-find.
     const bool mir = C.mirror;
+    const bool edge = i == C.il || i == C.ir - 1 || j == C.jl || j == C.jr - 1 || (!C.bi && (k == C.kl || k == C.kr - 1));
+    const bool near = mir && (i - C.il < NG || C.ir - 1 - i < NG || j - C.jl < NG || C.jr - 1 - j < NG);
+    if (!edge && !near) {
+      if (STAGE == 2 && t_gev) *t_gev = C.hbarc * (double)eos_T<R>(C, e);
+      return my_it;
+    }
+    R qb[9], pb[4];
+    if (edge) {
+#pragma unroll
+      for (int l = 0; l < 9; l++) qb[l] = P.S(out_b, l)[c];
+#pragma unroll
+      for (int l = 0; l < 4; l++) pb[l] = P.pu(l)[c];
+    }
+    q9 = qb;
+    pu = pb;
     if (i == C.il)
       for (int m = 0; m < NG; m++) ghost_put<R>(P, out_b, cix(C, m, j, k), e, u, pu, q9, mir);
     if (i == C.ir - 1)
@@ -536,10 +553,11 @@ __device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R
   return root_cell<R, STAGE>(C, P, tau_n, ts, x, e, u, pu, q9, t_gev);
 }
 
-// one thread per interior cell; 6 blocks per SM (80 registers: the spills
-// cost less than the latency the extra warps hide, measured)
+// one thread per interior cell; 5 blocks per SM (96 registers), measured
+// against 4 to 8 on the 161x161x41 event: fewer registers spill more than the
+// extra warps hide, more registers leave the FP64 Newton chain too few warps
 template <class R, int STAGE>
-__global__ void __launch_bounds__(128, 6) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
+__global__ void __launch_bounds__(128, 5) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
   if (*P.status) return;
   const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -116,6 +116,12 @@ class Hydro:
         self._chk(A.lib().vh_get_primitive(self.h, A.ptr(e), A.ptr(P), A.ptr(T), A.ptr(u), A.ptr(pi)))
         return dict(e=e, P=P, T=T, u=u, pi=pi)
 
+    def get_conserved(self) -> np.ndarray:
+        """the reference's Var (10, n): tau T^{tau mu}, pi (5), bulk (0)"""
+        out = np.zeros((10, self.n))
+        self._chk(A.lib().vh_get_conserved(self.h, A.ptr(out)))
+        return out
+
     def get_ns_pi(self) -> np.ndarray:
         """Navier-Stokes 2 eta sigma^{mu nu} (10, n: tt tx ty te xx xy xe yy ye ee)"""
         out = np.zeros((10, self.n))
