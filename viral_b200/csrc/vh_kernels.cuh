@@ -553,9 +553,9 @@ __device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R
   return root_cell<R, STAGE>(C, P, tau_n, ts, x, e, u, pu, q9, t_gev);
 }
 
-// one thread per interior cell; 5 blocks per SM (96 registers), measured
-// against 4 to 8 on the 161x161x41 event: fewer registers spill more than the
-// extra warps hide, more registers leave the FP64 Newton chain too few warps
+// one thread per interior cell; 5 blocks per SM (96 registers): the fastest
+// of 5 to 8 on the 161x161x41 event (4, at 128 registers, was slower in an
+// earlier version); fewer registers spill more than the extra warps hide
 template <class R, int STAGE>
 __global__ void __launch_bounds__(128, 5) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
   if (*P.status) return;
