@@ -236,11 +236,13 @@ def algorithmic_bytes(cfg, kernel: str) -> float:
 
 
 # DRAM bytes (read + write) per interior cell and launch, from one ncu capture
-# of the 121x121x31 case of the bench event (profiles/step_kernels_*.md),
-# scaled to a full launch by the cells processed
+# of the 121x121x31 case of the bench event (profiles/step_kernels_*.md and,
+# for the FP64 stage-1 update, profiles/update_kernel_*.md; the stage-2
+# figures predate the current update kernel), scaled to a full launch by the
+# cells processed
 MEASURED_TRAFFIC_PER_CELL = {
     ("fp64", "k_dir_x"): 150.0, ("fp64", "k_dir_y"): 239.0, ("fp64", "k_dir_eta"): 261.0,
-    ("fp64", "k_update_stage1"): 663.0, ("fp64", "k_update_stage2"): 651.0,
+    ("fp64", "k_update_stage1"): 538.0, ("fp64", "k_update_stage2"): 651.0,
     ("mixed", "k_dir_x"): 63.0, ("mixed", "k_dir_y"): 104.0, ("mixed", "k_dir_eta"): 114.0,
     ("mixed", "k_update_stage1"): 200.0, ("mixed", "k_update_stage2"): 223.0,
 }
