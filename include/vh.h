@@ -130,12 +130,34 @@ int vh_landau_match(const double* tmunu10, long long n, double tau, int cartesia
                     long long* nfail);
 /* Initial state from T^{mu nu} on the handle's ghost-inclusive grid (10 x n
  * host doubles as above), as the reference's Glasma initialisation builds it
- * (NEWEST5/ginit.h:658-1052): Landau matching, P(e) from the EOS, the five
- * evolved components of pi^{mu nu} = T^{mu nu} - (e+P) u^mu u^nu + P g^{mu nu}
- * (the trace part, a bulk pressure, is not evolved and is dropped),
- * prevu = u, T^{tau mu} from (e, u, pi).  VH_E_ROOTFIND, with *nfail > 0,
- * when some cell has no timelike eigenpair. */
+ * (NEWEST5/ginit.h:658-1052): Landau matching, P(e) from the EOS, and the
+ * five evolved components of pi^{mu nu} = T^{mu nu} - T_id^{mu nu}
+ * - PI (g^{mu nu} - u^mu u^nu), T_id = (e+P) u u - P g, PI = -(e - 3P)/3
+ * (the trace of T_id: for the traceless field tensor pi comes out
+ * traceless; PI is not evolved), prevu = u, T^{tau mu} from (e, u, pi).
+ * VH_E_ROOTFIND, with *nfail > 0, when some cell has no timelike eigenpair. */
 int vh_init_tmunu(vh_handle* h, double tau, const double* tmunu10, long long* nfail);
+/* prevu from T^{mu nu} at tau_prev = tau0 - dtau by Landau matching, after
+ * vh_init_tmunu (the reference calls ginit at tau0 - ts first and keeps
+ * only the velocity, NEWEST5/init.h:658-662, ginit.h:945-953). */
+int vh_init_prevu_tmunu(vh_handle* h, double tau_prev, const double* tmunu10, long long* nfail);
+/* The reference's optical-Glauber CGC tensor (NEWEST5/ginit.h:658-913) at
+ * tau on the ghost-inclusive grid of nx x ny (x nz) cells: T^{mu nu} in the
+ * order of vh_landau_match.  Thickness functions mu1, mu2 of two
+ * Woods-Saxon nuclei (mass number, diffuseness ws_a; R = 1.12 A^(1/3) -
+ * 0.86 A^(-1/3)) centred at x = +x_pos and -x_pos, integrated along the
+ * beam axis and scaled by 2 thickness_scale; e = N mu1 mu2 with N setting
+ * the grid maximum to e_peak (fm^-4; the reference uses 0.58 e_max(tau),
+ * e_max from T = 0.4 GeV at 0.6 fm/c scaled by (tau/0.6)^(-4/3));
+ * alpha = -grad e, beta = N (mu1 grad mu2 - mu2 grad mu1) by WENO
+ * derivatives (of log mu for the thicknesses); T^{mu nu} to order tau^2
+ * with the coefficient delta (the reference's 100) of its e-proportional
+ * terms; an eta profile flat for |eta| < eta_flat/2 with unit-width
+ * Gaussian tails.  The reference's values: x_pos 3, A 197, ws_a 0.546,
+ * thickness_scale 12.2546, eta_flat 4, delta 100.  Host arrays. */
+int vh_profile_cgc(int nx, int ny, int nz, int boost_invariant, double dx, double dy, double dz, double tau,
+                   double x_pos, double mass_number, double ws_a, double thickness_scale, double e_peak,
+                   double eta_flat, double delta, double* tmunu10);
 
 /* Initialise from a profile (the reference's init(tau, ts) with a scenario,
  * NEWEST5/init.h:556-704): e, u^x, u^y, u^eta on the ghost-inclusive grid

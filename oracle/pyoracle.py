@@ -289,6 +289,62 @@ class RefNS10:
         return ns, du
 
 
+_EIG_FN = ctypes.CFUNCTYPE(ctypes.c_int, _dp, _dp, _dp, _dp, _dp)
+
+
+def _eig_callback(a, wr, wi, vr, vi):
+    """eigenpairs of a real 4x4 matrix (LAPACK dgeev through NumPy) for the
+    GSL stand-in of the reference harness"""
+    A = np.ctypeslib.as_array(a, shape=(16,)).reshape(4, 4).copy()
+    w, v = np.linalg.eig(A)
+    w = np.asarray(w, dtype=complex)
+    v = np.asarray(v, dtype=complex)
+    for i in range(4):
+        wr[i] = w[i].real
+        wi[i] = w[i].imag
+        for j in range(4):
+            vr[j * 4 + i] = v[j, i].real
+            vi[j * 4 + i] = v[j, i].imag
+    return 0
+
+
+class RefGinit:
+    """NEWEST5's Glasma initialisation (ginit.h) in its GINIT block, one
+    rank's window of the reference's 10 x 10 layout (oracle/ref_ginit.cpp)."""
+
+    def __init__(self, xcord=4, ycord=4):
+        L = _load(os.path.join(HERE, "_ref", "libref_ginit.so"))
+        L.ref_ginit_run.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.ref_ginit_eos.argtypes = [ctypes.c_double, _dp]
+        L.ref_ginit_e_at_0p4gev.restype = ctypes.c_double
+        self._cb = _EIG_FN(_eig_callback)
+        L.ref_ginit_set_eig(self._cb)
+        d = (ctypes.c_int * 10)()
+        c = (ctypes.c_double * 8)()
+        L.ref_ginit_init(xcord, ycord, d, c)
+        self.L = L
+        self.gx, self.gy, self.gz, self.il, self.ir, self.jl, self.jr, self.kl, self.kr, lbi = list(d)
+        self.boost_invariant = bool(lbi)
+        self.dx, self.dy, self.dz, self.tau0, self.ts, self.x_pos, self.flat, self.gevfm = list(c)
+        self.n = self.gx * self.gy * self.gz
+
+    def run(self):
+        """ginit at tau0 - ts, then at tau0; returns (state (18, n), x, y, eta)"""
+        self.L.ref_ginit_run(self.tau0, self.ts)
+        f = np.zeros((NF, self.n)); x = np.zeros(self.n); y = np.zeros(self.n); eta = np.zeros(self.n)
+        self.L.ref_ginit_state(_ptr(f), _ptr(x), _ptr(y), _ptr(eta))
+        return f, x, y, eta
+
+    def eos(self, e):
+        """P, dP/de, T, s of the block's EOS (s95p)"""
+        out = np.zeros(4)
+        self.L.ref_ginit_eos(e, _ptr(out))
+        return out
+
+    def e_at_0p4gev(self):
+        return self.L.ref_ginit_e_at_0p4gev()
+
+
 # ---------------------------------------------------------------- inputs
 
 

@@ -17,7 +17,9 @@ sums over the whole grid), so that the fixtures stay small.  A fifth
 fixture, cart_3d_shock, is the reference's own Cartesian scenario (the
 shock tube of its default TXYZ5 block) after 20 steps; a sixth, ns10_lbi,
 is NEWEST10's ten-component Navier-Stokes shear tensor (CalcNS); a
-seventh, bjorken, is the reference's Bjorken scenario run to tau = 10.  The CPU tests
+seventh, bjorken, is the reference's Bjorken scenario run to tau = 10; an
+eighth, cgc, the reference's Glasma initialisation (ginit.h) on one rank's
+window.  The CPU tests
 rebuild the same inputs and check the oracle against these numbers.
 """
 from __future__ import annotations
@@ -32,7 +34,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from pyoracle import Oracle, OracleConfig, RefBuild, RefNS10, grid_coords, smooth_state  # noqa: E402
+from pyoracle import Oracle, OracleConfig, RefBuild, RefGinit, RefNS10, grid_coords, smooth_state  # noqa: E402
 
 # reference scenario blocks (oracle/Makefile) and the EOS / transport they compile
 SCENARIOS = {
@@ -177,6 +179,30 @@ def make_bjorken() -> dict:
             "temp": np.array(temps), "final": R.get_state()[:, centre]}
 
 
+CGC_SAMPLE = 1000
+
+
+def make_cgc() -> dict:
+    """The reference's Glasma initialisation (NEWEST5/ginit.h with its GINIT
+    block: s95p EOS, tau0 = 0.1 fm/c, ts = 0.002), 3+1D with 61 eta cells, on
+    the window of rank (4, 4) of its 10 x 10 layout (x, y in [-3.3, 0.2] fm
+    with ghosts): the state at seeded interior cells, s95p's P there, T = 0.4
+    GeV's energy density, and an s95p table (e, P, dP/de, T) for the GPU."""
+    R = RefGinit(4, 4)
+    f, x, y, eta = R.run()
+    idx = np.arange(R.n)
+    i, j, k = idx % R.gx, (idx // R.gx) % R.gy, idx // (R.gx * R.gy)
+    inner = np.where((i >= R.il) & (i < R.ir) & (j >= R.jl) & (j < R.jr) & (k >= R.kl) & (k < R.kr))[0]
+    cells = np.sort(np.random.default_rng(321).choice(inner, size=CGC_SAMPLE, replace=False))
+    te = np.geomspace(1e-2, 1e4, 2000)
+    tab = np.array([R.eos(v) for v in te])
+    return {"cells": cells, "dims": np.array([R.gx, R.gy, R.gz, R.il, R.ir, R.kl, R.kr]),
+            "consts": np.array([R.dx, R.dy, R.dz, R.tau0, R.ts, R.x_pos, R.flat, R.gevfm]),
+            "e_at_0p4gev": R.e_at_0p4gev(), "state": f[:, cells], "x": x[cells], "y": y[cells], "eta": eta[cells],
+            "P": np.array([R.eos(v)[0] for v in f[0, cells]]),
+            "eos_table": np.array([te, tab[:, 0], tab[:, 1], tab[:, 2]])}
+
+
 NS10_TAU = 1.3
 NS10_SEED = 11
 
@@ -201,7 +227,7 @@ def make_ns10() -> dict:
 
 
 def main():
-    special = {"cart_3d_shock": make_shock, "ns10_lbi": make_ns10, "bjorken": make_bjorken}
+    special = {"cart_3d_shock": make_shock, "ns10_lbi": make_ns10, "bjorken": make_bjorken, "cgc": make_cgc}
     which = sys.argv[1:] or list(SCENARIOS) + list(special)
     for v in which:
         d = special[v]() if v in special else make(v)

@@ -54,8 +54,11 @@ def tmunu_of(p, tau, cart=False):
 
 @pytest.mark.parametrize("which", ["gubser", "glauber3d"])
 def test_init_tmunu_round_trip(which):
-    """T^{mu nu} of an evolved viscous state, matched back: e, u, pi and
-    T^{tau mu} of the state"""
+    """T^{mu nu} of an evolved viscous state, matched back: e and u of the
+    state; pi and T^{tau mu} of the state for the conformal EOS (Gubser),
+    and with the reference's trace correction otherwise: its pi is
+    T - T_id - PI (g - u u) with PI = -(e - 3P)/3, which adds (e - 3P)/3
+    (g - u u) to a fluid tensor's pi (NEWEST5/ginit.h:955-989)"""
     if which == "gubser":
         cfg = C.gubser_config(nx=33, ny=33)
         inp = C.gubser_inputs(cfg)
@@ -76,6 +79,21 @@ def test_init_tmunu_round_trip(which):
         assert H2.init_tmunu(tau, T) == 0
         s2 = H2.get_state()
         assert abs(H2.tau - tau) < 1e-15
+    if which != "gubser":
+        # the expected state: pi + (e - 3P)/3 (g - u u), T^{tau mu} by the
+        # oracle's closure of it
+        from helpers import oracle_config
+        from pyoracle import Oracle
+        t2 = tau * tau
+        gi = [1.0, -1.0, -1.0, -1.0 / t2]
+        u = s[1:5]
+        tr = (s[0] - 3 * p["P"]) / 3
+        for m, (a, b) in enumerate([(1, 1), (2, 2), (1, 2), (1, 3), (2, 3)]):
+            s[5 + m] = s[5 + m] + tr * ((gi[a] if a == b else 0.0) - u[a] * u[b])
+        O = Oracle(oracle_config(cfg))
+        O.set_state(s)
+        O.fill_tmunu(tau)
+        s = O.get_state()
     # interior cells (the Gubser test's mirrored ghosts hold a u^tau that is
     # not the normalisation of their u^x, u^y)
     m = interior_mask(cfg)

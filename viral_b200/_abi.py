@@ -107,6 +107,11 @@ SIGNATURES = [
     ("vh_batch_barrier_selftest", ctypes.c_int, [ctypes.c_int, _dp]),
     ("vh_get_ns_pi", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("vh_get_conserved", ctypes.c_int, [ctypes.c_void_p, _dp]),
+    ("vh_init_prevu_tmunu", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_longlong)]),
+    ("vh_profile_cgc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, _dp]),
     ("vh_save_checkpoint", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("vh_load_checkpoint", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _dp]),
     ("vh_batch_last_error", ctypes.c_char_p, [ctypes.c_void_p]),

@@ -425,6 +425,26 @@ extern "C" int vh_init_tmunu(vh_handle* h, double tau, const double* tmunu10, lo
   return VH_OK;
 }
 
+extern "C" int vh_init_prevu_tmunu(vh_handle* h, double tau_prev, const double* tmunu10, long long* nfail) {
+  if (!h || !tmunu10) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "vh_init_prevu_tmunu after the state is set");
+  if (!h->C.cart && !(tau_prev > 0)) return fail(h, VH_E_ARG, "Milne tau must be positive");
+  const long long n = h->C.n;
+  double* buf = h->stage;
+  VH_CUDA(h, cudaMemcpyAsync(buf, tmunu10, 10 * sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+  VH_CUDA(h, cudaMemsetAsync(h->red, 0, sizeof(unsigned long long), h->stream));
+  if (h->mixed) k_prevu_tmunu<float><<<grid1(n, 128), 128, 0, h->stream>>>(h->C, h->pf, tau_prev, buf, h->red);
+  else k_prevu_tmunu<double><<<grid1(n, 128), 128, 0, h->stream>>>(h->C, h->pd, tau_prev, buf, h->red);
+  VH_CUDA(h, cudaGetLastError());
+  unsigned long long bad = 0;
+  VH_CUDA(h, cudaMemcpyAsync(&bad, h->red, sizeof(bad), cudaMemcpyDeviceToHost, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (nfail) *nfail = (long long)bad;
+  if (bad) return fail(h, VH_E_ROOTFIND, "Landau matching found no timelike eigenvector in " + std::to_string(bad) +
+                                             " cell(s)");
+  return VH_OK;
+}
+
 extern "C" int vh_max_temperature(vh_handle* h, double* tmax_gev) {
   if (!h || !tmax_gev) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");

@@ -152,12 +152,35 @@ __global__ void k_init_tmunu(DevCfg C, DevPtrs<R> P, double tau, const double* T
   P.e()[c] = (R)e;
 #pragma unroll
   for (int l = 0; l < 4; l++) { P.u(l)[c] = (R)u[l]; P.pu(l)[c] = (R)u[l]; }
+  // NEWEST5/ginit.h:955-989: the ideal tensor tid, its trace e - 3P taken
+  // off as PI (g - u u) with PI = -trace/3, so that pi is traceless; PI
+  // itself is not evolved
+  double tid[4];
+#pragma unroll
+  for (int a = 0; a < 4; a++) tid[a] = (e + Pp) * u[a] * u[a] - Pp * gi[a];
+  const double PI = -(tid[0] - tid[1] - tid[2] - t2 * tid[3]) / 3.0;
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     const int a = a5[k], b = b5[k];
-    const double pi = t[q[k]] - (e + Pp) * u[a] * u[b] + (a == b ? Pp * gi[a] : 0.0);
-    P.A(4 + k)[c] = (R)pi;
+    const double id = (e + Pp) * u[a] * u[b] - (a == b ? Pp * gi[a] : 0.0);
+    const double pim = PI * ((a == b ? gi[a] : 0.0) - u[a] * u[b]);
+    P.A(4 + k)[c] = (R)(t[q[k]] - id - pim);
   }
+}
+
+// prevu from T^{mu nu} one step before the initial time (the reference's
+// ginit at tau - ts, NEWEST5/ginit.h:945-953): Landau matching, u only.
+template <class R>
+__global__ void k_prevu_tmunu(DevCfg C, DevPtrs<R> P, double tau, const double* T10, unsigned long long* nfail) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = C.n;
+  if (c >= n) return;
+  double t[10], e = 0, u[4] = {1, 0, 0, 0};
+#pragma unroll
+  for (int l = 0; l < 10; l++) t[l] = T10[(long long)l * n + c];
+  if (!landau_cell(t, tau, C.cart, e, u)) atomicAdd(nfail, 1ull);
+#pragma unroll
+  for (int l = 0; l < 4; l++) P.pu(l)[c] = (R)u[l];
 }
 
 // Velocity gradients with the coverage the reference's CalcDer4Vel has

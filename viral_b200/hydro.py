@@ -136,6 +136,13 @@ class Hydro:
         self._chk(A.lib().vh_init_tmunu(self.h, tau, A.ptr(t), ctypes.byref(nf)))
         return nf.value
 
+    def init_prevu_tmunu(self, tau_prev: float, tmunu10: np.ndarray) -> int:
+        """prevu from T^{mu nu} (10, n) at tau_prev by Landau matching"""
+        t = np.ascontiguousarray(tmunu10, dtype=np.float64).reshape(10, self.n)
+        nf = ctypes.c_longlong()
+        self._chk(A.lib().vh_init_prevu_tmunu(self.h, tau_prev, A.ptr(t), ctypes.byref(nf)))
+        return nf.value
+
     def init_profile(self, tau, e, ux, uy, ueta=None, prevu=None, pi_mode=A.PI_ZERO, pi5=None):
         c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
         self._chk(A.lib().vh_init_profile(self.h, tau, A.ptr(c(e)), A.ptr(c(ux)), A.ptr(c(uy)), A.ptr(c(ueta)),
@@ -237,6 +244,17 @@ def landau_match(tmunu10: np.ndarray, tau: float, cartesian: bool = False):
     nf = ctypes.c_longlong()
     A.check(A.lib().vh_landau_match(A.ptr(t), n, tau, int(cartesian), A.ptr(e), A.ptr(u), ctypes.byref(nf)))
     return e, u, nf.value
+
+
+def profile_cgc(nx, ny, nz=1, boost_invariant=True, dx=0.1, dy=0.1, dz=0.1, tau=0.1, e_peak=1.0, x_pos=3.0,
+                mass_number=197.0, ws_a=0.546, thickness_scale=12.2546, eta_flat=4.0, delta=100.0) -> np.ndarray:
+    """the optical-Glauber CGC T^{mu nu} (10, n) of the reference's Glasma
+    initialisation on the ghost-inclusive grid (host code)"""
+    gz = 1 if boost_invariant else nz + 6
+    out = np.zeros((10, (nx + 6) * (ny + 6) * gz))
+    A.check(A.lib().vh_profile_cgc(nx, ny, nz, int(boost_invariant), dx, dy, dz, tau, x_pos, mass_number, ws_a,
+                                   thickness_scale, e_peak, eta_flat, delta, A.ptr(out)))
+    return out
 
 
 def read_ideal_profile(eps_path: str, vx_path: str, vy_path: str, nx: int, ny: int):
