@@ -89,6 +89,9 @@ typedef struct {
   double minmod_theta;  /* generalized-minmod theta (NEWEST5/maindef.h:370) */
   double taupi_const;   /* VH_TAUPI_CONST: tau_pi in fm/c (the Bjorken block,
                            NEWEST5/maindef.h:228) */
+  int cold_plasma;      /* 1: the shear source without its relaxation term
+                           -pi/tau_pi (the reference's COLDPLASMA test of the
+                           Gubser flow, NEWEST5/Source.h:371-410) */
 } vh_config;
 
 typedef struct vh_handle vh_handle;
@@ -385,6 +388,17 @@ int vh_eos_table_synthetic(int n, double emin_gev, double emax_gev, double a, do
 int vh_profile_gubser(int nx, int ny, double dx, double dy, double q, double tau0, double dtau,
                       double t0_gev, double a, double hbarc, double* e, double* ux, double* uy,
                       double* prevu4);
+/* The viscous Gubser flow of the cold-plasma limit (the reference's
+ * COLDPLASMA initial state, NEWEST5/init.h:489-512): conformal e = a T^4
+ * with T = T^(rho)/tau, T^ = b sech(rho)^(2/3) cosh(k ln cosh rho)^(1/4),
+ * k = 4/(3 sqrt 5), sinh rho = -(1 - q^2 tau^2 + q^2 r^2)/(2 q tau); Gubser
+ * velocity; pi^{mu nu} from the de Sitter shear pi^eta_eta = -(4/3) a T^^4
+ * tanh(k ln cosh rho)/sqrt 5, scaled by tau^-4 into Milne coordinates.
+ * Writes e, u^x, u^y, pi5 (xx, yy, xy, x-eta, y-eta) at tau0 and prevu4 at
+ * tau0 - dtau on the 2+1D ghost-inclusive grid.  The reference's values:
+ * q = 1/fm, b = 1.21. */
+int vh_profile_gubser_cold(int nx, int ny, double dx, double dy, double q, double tau0, double dtau, double b,
+                           double a, double* e, double* ux, double* uy, double* pi5, double* prevu4);
 /* Monte-Carlo Glauber energy density (two Woods-Saxon nuclei): A nucleons
  * per nucleus, radius R, diffuseness aws, hard core dmin, impact parameter
  * b, sigma_nn (fm^2), Gaussian width w per participant, peak e in GeV/fm^3,

@@ -523,7 +523,9 @@ static void is_source_cell(const vho_config* C, double tau, double e, const doub
   static const int MU[5] = {1, 2, 1, 1, 2}, NU[5] = {1, 2, 2, 3, 3};
   for (int q = 0; q < 5; q++) {
     int m = MU[q], v = NU[q];
-    double rhs = -(pi[m][v] - 2.0 * eta * sig[m][v]) / tp - (4.0 / 3.0) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
+    /* COLDPLASMA (NEWEST5/Source.h:371-410) drops the relaxation -pi/tau_pi */
+    double relax = C->cold_plasma ? 0.0 : pi[m][v];
+    double rhs = -(relax - 2.0 * eta * sig[m][v]) / tp - (4.0 / 3.0) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
     double chr = 0;
     if (!cart) {
       /* Gamma^tau_{ee} = tau, Gamma^e_{tau e} = Gamma^e_{e tau} = 1/tau */

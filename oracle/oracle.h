@@ -51,6 +51,7 @@ typedef struct {
   int recon;            /* 0: WENO5 (reference); 1: generalized minmod */
   double minmod_theta;  /* generalized minmod theta (NEWEST5/maindef.h:370) */
   double taupi_const;   /* taupi_kind 2: constant tau_pi (NEWEST5/maindef.h:228) */
+  int cold_plasma;      /* shear source without -pi/tau_pi (NEWEST5/Source.h:371-410) */
 } vho_config;
 
 typedef struct vho_grid vho_grid;

@@ -37,6 +37,7 @@ class _Cfg(ctypes.Structure):
         ("hbarc", ctypes.c_double),
         ("taupi_kind", ctypes.c_int), ("gubser_mirror", ctypes.c_int),
         ("recon", ctypes.c_int), ("minmod_theta", ctypes.c_double), ("taupi_const", ctypes.c_double),
+        ("cold_plasma", ctypes.c_int),
     ]
 
 
@@ -59,6 +60,7 @@ class OracleConfig:
     hbarc: float = 0.19733
     taupi_kind: int = 0        # 0: 1.5 eta/P, 1: 5 eta/(e+P), 2: taupi_const
     taupi_const: float = 0.0
+    cold_plasma: bool = False  # shear source without -pi/tau_pi
     gubser_mirror: bool = False
     recon: int = 0             # 0 WENO5, 1 generalized minmod
     minmod_theta: float = 1.1
@@ -85,6 +87,7 @@ class OracleConfig:
         c.gubser_mirror = int(self.gubser_mirror)
         c.recon, c.minmod_theta = self.recon, self.minmod_theta
         c.taupi_const = self.taupi_const
+        c.cold_plasma = int(self.cold_plasma)
         return c
 
 

@@ -41,6 +41,7 @@ SCENARIOS = {
     "milne_lbi": dict(etas0=1 / (4 * math.pi), taupi_kind=0, cartesian=False, mirror=False, tau=1.3),
     "milne_3d": dict(etas0=1 / (4 * math.pi), taupi_kind=0, cartesian=False, mirror=False, tau=1.3),
     "gubser": dict(etas0=0.2, taupi_kind=1, cartesian=False, mirror=True, tau=1.3),
+    "gubser_cold": dict(etas0=0.2, taupi_kind=1, cartesian=False, mirror=True, tau=1.3, cold=True),
     "cart_3d": dict(etas0=0.01 / (4 * math.pi), taupi_kind=0, cartesian=True, mirror=False, tau=1.0),
 }
 TS = 0.01
@@ -52,7 +53,7 @@ def oracle_config(R: RefBuild, sc: dict) -> OracleConfig:
     return OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=(1 if R.boost_invariant else R.gz - 6),
                         boost_invariant=R.boost_invariant, cartesian=sc["cartesian"], dx=R.dx, dy=R.dy, dz=R.dz,
                         eos_kind=0, eos_a=R.factor, etas0=sc["etas0"], etas1=0.0, hbarc=R.gevfm,
-                        taupi_kind=sc["taupi_kind"], gubser_mirror=sc["mirror"])
+                        taupi_kind=sc["taupi_kind"], gubser_mirror=sc["mirror"], cold_plasma=sc.get("cold", False))
 
 
 def inputs(R: RefBuild, sc: dict) -> np.ndarray:

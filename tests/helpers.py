@@ -15,7 +15,8 @@ def oracle_config(cfg: Config) -> OracleConfig:
                         dx=cfg.dx, dy=cfg.dy, dz=cfg.dz, eos_kind=cfg.eos_kind, eos_a=cfg.eos_a,
                         eos_table=cfg.eos_table, etas0=cfg.etas0, etas1=cfg.etas1, etas_tc=cfg.etas_tc,
                         hbarc=cfg.hbarc, taupi_kind=cfg.taupi_kind, gubser_mirror=cfg.gubser_mirror,
-                        recon=cfg.recon, minmod_theta=cfg.minmod_theta, taupi_const=cfg.taupi_const)
+                        recon=cfg.recon, minmod_theta=cfg.minmod_theta, taupi_const=cfg.taupi_const,
+                        cold_plasma=cfg.cold_plasma)
 
 
 def canonical_state(cfg: Config, inp: dict) -> np.ndarray:

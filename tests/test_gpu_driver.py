@@ -104,6 +104,23 @@ def test_driver_bjorken_temperature_file(tmp_path):
     assert np.allclose(rows[:m, 1], g["temp"][:m] * 0.1973 / 1000, rtol=1e-5, atol=0)
 
 
+def test_driver_cold_plasma_snapshot(tmp_path):
+    """--scenario gubser --cold-plasma: the snapshot after 4 steps is the
+    Python path's (vh_profile_gubser_cold, the source without -pi/tau_pi)"""
+    from viral_b200.hydro import Hydro, profile_gubser_cold
+    out = run_driver(["--scenario", "gubser", "--cold-plasma", "--nx", "33", "--ny", "33", "--steps", "4",
+                      "--print-every", "0.04"], str(tmp_path))
+    cfg = C.gubser_config(nx=33, ny=33)
+    cfg.cold_plasma = True
+    with Hydro(cfg) as H:
+        e, ux, uy, pi5, pu = profile_gubser_cold(33, 33, cfg.dx, cfg.dy, 1.0, cfg.tau0, cfg.dtau, 1.21, cfg.eos_a)
+        H.init_profile(cfg.tau0, e, ux, uy, None, pu, A.PI_GIVEN, pi5)
+        H.step(4)
+        mine = os.path.join(str(tmp_path), "py.bin")
+        H.write(mine, A.WRITE_XY, 1)
+    assert open(mine, "rb").read() == open(os.path.join(out, "tau1.040fm.bin"), "rb").read()
+
+
 def test_get_primitive():
     cfg = C.gubser_config(nx=21, ny=21)
     with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:

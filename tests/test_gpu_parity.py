@@ -256,3 +256,32 @@ def test_get_conserved(cfgkw):
     assert np.array_equal(var[:4], t * s[10:14])
     assert np.array_equal(var[4:9], s[5:10])
     assert np.all(var[9] == 0)
+
+
+def test_cold_plasma_gubser_flow():
+    """the reference's cold-plasma test (the shear source without -pi/tau_pi):
+    the GPU against the oracle over 10 steps, and against the closed form
+    to tau = 1.5 fm/c on a 129 x 129 grid"""
+    from test_cold_plasma_cpu import A_CONF, closed_form_T, cold_config, radius, run_oracle
+    from viral_b200.hydro import profile_gubser_cold
+
+    def start(H, cfg):
+        e, ux, uy, pi5, pu = profile_gubser_cold(cfg.nx, cfg.ny, cfg.dx, cfg.dy, 1.0, cfg.tau0, cfg.dtau, 1.21, A_CONF)
+        H.init_profile(cfg.tau0, e, ux, uy, None, pu, A.PI_GIVEN, pi5)
+
+    cfg = cold_config(41, 0.1, 0.01)
+    ref, _ = run_oracle(cfg, 10)
+    with Hydro(cfg) as H:
+        start(H, cfg)
+        H.step(10)
+        compare_states(H.get_state(), ref, RUN_TOL, fields=range(18))
+    cfg = cold_config(129, 0.1, 0.01)
+    with Hydro(cfg) as H:
+        start(H, cfg)
+        H.step(50)
+        s, tau = H.get_state(), H.tau
+    r = radius(cfg)
+    m = r < 2.0
+    err = np.max(np.abs((s[0][m] / A_CONF) ** 0.25 / closed_form_T(r[m], tau) - 1))
+    print("cold plasma on the GPU to tau = %.2f: T within %.2e of the closed form" % (tau, err))
+    assert err <= 6e-4

@@ -26,6 +26,7 @@ VARIANTS = {
     "milne_lbi": dict(etas0=1 / (4 * math.pi), taupi_kind=0, cartesian=False, mirror=False),
     "milne_3d": dict(etas0=1 / (4 * math.pi), taupi_kind=0, cartesian=False, mirror=False),
     "gubser": dict(etas0=0.2, taupi_kind=1, cartesian=False, mirror=True),
+    "gubser_cold": dict(etas0=0.2, taupi_kind=1, cartesian=False, mirror=True, cold=True),
     "cart_3d": dict(etas0=0.01 / (4 * math.pi), taupi_kind=0, cartesian=True, mirror=False),
 }
 TOL = 1e-12
@@ -39,7 +40,8 @@ def setup(variant):
     sc = VARIANTS[variant]
     cfg = OracleConfig(nx=gx - 6, ny=gy - 6, nz=(1 if bi else gz - 6), boost_invariant=bool(bi),
                        cartesian=sc["cartesian"], dx=dx, dy=dy, dz=dz, eos_kind=0, eos_a=factor,
-                       etas0=sc["etas0"], hbarc=gevfm, taupi_kind=sc["taupi_kind"], gubser_mirror=sc["mirror"])
+                       etas0=sc["etas0"], hbarc=gevfm, taupi_kind=sc["taupi_kind"], gubser_mirror=sc["mirror"],
+                       cold_plasma=sc.get("cold", False))
     x, y, z = grid_coords(gx, gy, gz, dx, dy, dz, bool(bi))
     tau, ts = float(g["tau"]), float(g["ts"])
     f = smooth_state(x, y, z, tau, ts, seed=int(g["seed"]), cartesian=sc["cartesian"])

@@ -43,7 +43,7 @@ class VhConfig(ctypes.Structure):
         ("etas0", ctypes.c_double), ("etas1", ctypes.c_double), ("etas_tc", ctypes.c_double),
         ("hbarc", ctypes.c_double),
         ("taupi_kind", ctypes.c_int), ("gubser_mirror", ctypes.c_int), ("minmod_theta", ctypes.c_double),
-        ("taupi_const", ctypes.c_double),
+        ("taupi_const", ctypes.c_double), ("cold_plasma", ctypes.c_int),
     ]
 
 
@@ -107,6 +107,9 @@ SIGNATURES = [
     ("vh_batch_barrier_selftest", ctypes.c_int, [ctypes.c_int, _dp]),
     ("vh_get_ns_pi", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("vh_get_conserved", ctypes.c_int, [ctypes.c_void_p, _dp]),
+    ("vh_profile_gubser_cold", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_double, _dp, _dp, _dp, _dp, _dp]),
     ("vh_init_prevu_tmunu", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("vh_profile_cgc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,

@@ -824,7 +824,7 @@ extern "C" int vh_adjoint_eps_p(vh_handle* h, int nsteps, int checkpoint_every, 
   if (!h || nsteps < 1 || checkpoint_every < 1) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
   const DevCfg& C = h->C;
-  if (C.cart || !C.bi || C.mirror || C.recon != VH_RECON_WENO5)
+  if (C.cart || !C.bi || C.mirror || C.recon != VH_RECON_WENO5 || C.cold)
     return fail(h, VH_E_UNSUPPORTED,
                 "vh_adjoint_eps_p: boost-invariant Milne grids with WENO reconstruction and copy boundaries only");
   const size_t smem = h->mixed ? dir_smem<float>(C) : dir_smem<double>(C);

@@ -66,6 +66,7 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
   C.etas0 = cfg->etas0; C.etas1 = cfg->etas1; C.etas_tc = cfg->etas_tc; C.hbarc = cfg->hbarc;
   C.taupi_kind = cfg->taupi_kind;
   C.taupi_c = cfg->taupi_const;
+  C.cold = cfg->cold_plasma != 0;
   C.mm_theta = cfg->minmod_theta;
   h->tau = cfg->tau0;
 

@@ -338,7 +338,8 @@ extern "C" int vh_batch_create(const vh_config* cfg, int n_events, const int* nx
   C.dx = cfg->dx; C.dy = cfg->dy; C.dz = 1.0;
   C.eos_kind = cfg->eos_kind; C.eos_a = cfg->eos_a;
   C.etas0 = cfg->etas0; C.etas1 = cfg->etas1; C.etas_tc = cfg->etas_tc; C.hbarc = cfg->hbarc;
-  C.taupi_kind = cfg->taupi_kind; C.taupi_c = cfg->taupi_const; C.mm_theta = cfg->minmod_theta;
+  C.taupi_kind = cfg->taupi_kind; C.taupi_c = cfg->taupi_const; C.cold = cfg->cold_plasma != 0;
+  C.mm_theta = cfg->minmod_theta;
   auto fail = [&](const char* what) {
     g_batch_err = std::string("vh_batch_create: ") + what + ": " + b->err;
     vh_batch_destroy(b);

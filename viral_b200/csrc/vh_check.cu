@@ -28,6 +28,7 @@ HostCfg make_cfg(const vh_config* c) {
   C.etas0 = c->etas0; C.etas1 = c->etas1; C.etas_tc = c->etas_tc; C.hbarc = c->hbarc;
   C.taupi_kind = c->taupi_kind;
   C.taupi_c = c->taupi_const;
+  C.cold = c->cold_plasma != 0;
   C.dx = c->dx; C.dy = c->dy; C.dz = c->dz;
   if (c->eos_kind == VH_EOS_TABLE) {
     const int n = c->eos_n;

@@ -31,6 +31,7 @@ struct DevCfg {
   double etas0, etas1, etas_tc, hbarc;
   int taupi_kind;
   double taupi_c;               // tau_pi of VH_TAUPI_CONST
+  int cold;                     // cold-plasma test: no -pi/tau_pi relaxation
   double mm_theta;
 };
 
@@ -455,7 +456,8 @@ VH_HD inline void is_source_PT(const DevCfg& C, R tau, R e, R P, R T, const R* u
 #pragma unroll
   for (int q = 0; q < 5; q++) {
     const int m = MU[q], v = NU[q];
-    R rhs = -(pi[m][v] - (R)2 * eta * sig[m][v]) * itp - ((R)4 / (R)3) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
+    const R relax = C.cold ? (R)0 : pi[m][v];  // the cold-plasma limit keeps 2 eta sigma / tau_pi only
+    R rhs = -(relax - (R)2 * eta * sig[m][v]) * itp - ((R)4 / (R)3) * pi[m][v] * th - (u[m] * pa[v] + u[v] * pa[m]);
     R chr = 0;
     if (!cart) {
 #pragma unroll

@@ -117,6 +117,60 @@ extern "C" int vh_profile_gubser(int nx, int ny, double dx, double dy, double q,
   return VH_OK;
 }
 
+extern "C" int vh_profile_gubser_cold(int nx, int ny, double dx, double dy, double q, double tau0, double dtau,
+                                      double b, double a, double* e, double* ux, double* uy, double* pi5,
+                                      double* prevu4) {
+  if (nx < 1 || ny < 1 || !e || !ux || !uy || !pi5 || !(tau0 > dtau) || !(q > 0) || !(b > 0) || !(a > 0))
+    return VH_E_ARG;
+  std::vector<double> X, Y;
+  axis_coords(nx, 3, dx, X);
+  axis_coords(ny, 3, dy, Y);
+  const int gx = nx + 6, gy = ny + 6;
+  const long long n = (long long)gx * gy;
+  const double q2 = q * q, k = 4.0 / (3.0 * std::sqrt(5.0));
+  for (int j = 0; j < gy; j++)
+    for (int i = 0; i < gx; i++) {
+      const long long c = (long long)j * gx + i;
+      const double x = X[i], y = Y[j], r = std::sqrt(x * x + y * y);
+      for (int pass = 0; pass < 2; pass++) {
+        const double tau = pass ? tau0 - dtau : tau0;
+        const double kap = std::atanh(2 * q2 * tau * r / (1 + q2 * tau * tau + q2 * r * r));
+        const double sh = std::sinh(kap), ch = std::cosh(kap);
+        const double cphi = r > 0 ? x / r : 1.0, sphi = r > 0 ? y / r : 0.0;
+        if (pass) {
+          if (prevu4) {
+            prevu4[c] = ch; prevu4[n + c] = sh * cphi; prevu4[2 * n + c] = sh * sphi; prevu4[3 * n + c] = 0.0;
+          }
+          continue;
+        }
+        ux[c] = sh * cphi;
+        uy[c] = sh * sphi;
+        // de Sitter time rho and the cold-plasma solution there: the shear
+        // ratio pi^eta_eta / (e + P) relaxes nowhere and follows
+        // d(pibar)/d(ln cosh rho) = 4/15 - (4/3) pibar^2 from 0 at rho = 0
+        const double rho = std::asinh(-(1 - q2 * tau * tau + q2 * r * r) / (2 * q * tau));
+        const double lc = std::log(std::cosh(rho));
+        const double That = b * std::pow(std::cosh(k * lc), 0.25) / std::pow(std::cosh(rho), 2.0 / 3.0);
+        const double T = That / tau;
+        e[c] = a * T * T * T * T;
+        const double w_hat = (4.0 / 3.0) * a * That * That * That * That;
+        const double pihat = -w_hat * std::tanh(k * lc) / std::sqrt(5.0);
+        // Milne: the eta and phi directions carry pihat / tau^4 (mixed
+        // components, pi^theta_theta = pi^phi_phi = -pihat/2); the direction
+        // in the (tau, r) plane orthogonal to u, n = (sinh kap, cosh kap),
+        // carries pi^{ab} = (pihat / (2 tau^4)) n^a n^b
+        const double c0 = pihat / (2 * tau * tau * tau * tau);
+        const double prr = c0 * ch * ch, pff = c0;  // pi^{rr}, r^2 pi^{phi phi}
+        pi5[c] = cphi * cphi * prr + sphi * sphi * pff;          // xx
+        pi5[n + c] = sphi * sphi * prr + cphi * cphi * pff;      // yy
+        pi5[2 * n + c] = sphi * cphi * (prr - pff);              // xy
+        pi5[3 * n + c] = 0.0;                                    // x eta
+        pi5[4 * n + c] = 0.0;                                    // y eta
+      }
+    }
+  return VH_OK;
+}
+
 extern "C" int vh_profile_glauber(int nx, int ny, int nz, int boost_invariant, double dx, double dy, double dz, int A,
                                   double R, double aws, double dmin, double b, double sigma_nn, double w,
                                   double epeak_gev, double eta_flat, double eta_sigma, double efloor_gev,

@@ -73,6 +73,7 @@ int fill_cfg(const vh_config* c, const double* eos_dev, DevCfg& C) {
   if (c->nx < 3 || c->ny < 3 || (!c->boost_invariant && c->nz < 3) || (c->boost_invariant && c->nz != 1)) return VH_E_ARG;
   if (!(c->dx > 0 && c->dy > 0 && (c->boost_invariant || c->dz > 0) && c->dtau > 0)) return VH_E_ARG;
   if (c->taupi_kind != VH_TAUPI_15_ETA_OVER_P && c->taupi_kind != VH_TAUPI_5_ETA_OVER_EPP) return VH_E_ARG;
+  if (c->cold_plasma) return VH_E_ARG;  // the test mode runs through vh_step only
   C = DevCfg{};
   C.nx = c->nx; C.ny = c->ny; C.nz = c->boost_invariant ? 1 : c->nz;
   C.gx = c->nx + 2 * NG; C.gy = c->ny + 2 * NG; C.gz = c->boost_invariant ? 1 : c->nz + 2 * NG;

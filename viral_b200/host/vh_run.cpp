@@ -9,7 +9,9 @@
 //   gubser     2+1D Gubser test (maindef.h GUBSER block): 129x129, dx 0.1 fm,
 //              tau0 1 fm/c, dtau 0.01, conformal EOS, eta/s 0.2,
 //              tau_pi = 5 eta/(e+P), Navier-Stokes pi, mirrored ghosts;
-//              stops after tau > 9 fm/c (main.cpp:196-199)
+//              stops after tau > 9 fm/c (main.cpp:196-199); --cold-plasma
+//              runs the COLDPLASMA test instead (init.h:489-512, the shear
+//              source without -pi/tau_pi, Source.h:371-410)
 //   glauber    2+1D MC-Glauber event (b, seed), synthetic EOS table,
 //              eta/s 0.08, tau_pi = 1.5 eta/P, tau0 0.6, dtau 0.02;
 //              stops when max T < 120 MeV (main.cpp:201-204, GINIT block)
@@ -61,6 +63,7 @@ struct Options {
   std::string restart;      // resume from this restart file
   std::string checkpoint;   // write a restart file at the end
   bool ns = false;          // also write res/NStau%2.3ffm.bin beside each snapshot
+  bool cold = false;        // gubser: the cold-plasma test (COLDPLASMA)
 };
 
 void usage() {
@@ -68,7 +71,7 @@ void usage() {
       "usage: vh_run [--scenario gubser|glauber|glauber3d|shocktube|bjorken] [--nx N --ny N --nz N]\n"
       "              [--precision fp64|mixed] [--steps N] [--tau-end T] [--print-every T]\n"
       "              [--out DIR] [--every FREQ] [--b B] [--seed S] [--floor E_GeV_fm3] [--quiet]\n"
-      "              [--restart FILE] [--checkpoint FILE] [--ns]\n");
+      "              [--restart FILE] [--checkpoint FILE] [--ns] [--cold-plasma]\n");
 }
 
 bool parse(int argc, char** argv, Options& o) {
@@ -103,6 +106,7 @@ bool parse(int argc, char** argv, Options& o) {
     else if (a == "--restart") o.restart = next("--restart");
     else if (a == "--checkpoint") o.checkpoint = next("--checkpoint");
     else if (a == "--ns") o.ns = true;
+    else if (a == "--cold-plasma") o.cold = true;
     else { std::fprintf(stderr, "vh_run: unknown option %s\n", a.c_str()); usage(); return false; }
   }
   if (o.scenario != "gubser" && o.scenario != "glauber" && o.scenario != "glauber3d" && o.scenario != "shocktube" &&
@@ -153,6 +157,7 @@ int main(int argc, char** argv) {
     c.dx = c.dy = 0.1; c.dz = 1.0; c.tau0 = 1.0; c.dtau = 0.01;
     c.eos_kind = VH_EOS_CONFORMAL; c.eos_a = kAqgp;
     c.etas0 = 0.2; c.etas_tc = 0.154; c.taupi_kind = VH_TAUPI_5_ETA_OVER_EPP; c.gubser_mirror = 1;
+    c.cold_plasma = o.cold ? 1 : 0;
   } else {
     c.nx = o.nx ? o.nx : (three_d ? 161 : 128); c.ny = o.ny ? o.ny : c.nx;
     c.nz = three_d ? (o.nz ? o.nz : 41) : 1; c.boost_invariant = three_d ? 0 : 1;
@@ -185,6 +190,12 @@ int main(int argc, char** argv) {
   } else if (bjorken) {
     for (size_t q = 0; q < n; q++) e[q] = 30.0 / c.hbarc;
     r = vh_init_profile(h, c.tau0, e.data(), ux.data(), uy.data(), nullptr, nullptr, VH_PI_ZERO, nullptr);
+  } else if (gubser && o.cold) {
+    // NEWEST5/init.h:489-512: the cold-plasma solution (B = 1.21) with its pi
+    std::vector<double> pi5(5 * n);
+    r = vh_profile_gubser_cold(c.nx, c.ny, c.dx, c.dy, 1.0, c.tau0, c.dtau, 1.21, c.eos_a, e.data(), ux.data(),
+                               uy.data(), pi5.data(), prevu.data());
+    if (!r) r = vh_init_profile(h, c.tau0, e.data(), ux.data(), uy.data(), nullptr, prevu.data(), VH_PI_GIVEN, pi5.data());
   } else if (gubser) {
     r = vh_profile_gubser(c.nx, c.ny, c.dx, c.dy, 1.0, c.tau0, c.dtau, 0.6, c.eos_a, kHbarc, e.data(), ux.data(),
                           uy.data(), prevu.data());

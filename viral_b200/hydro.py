@@ -44,6 +44,7 @@ class Config:
     gubser_mirror: bool = False
     minmod_theta: float = 1.1
     taupi_const: float = 0.0  # tau_pi (fm/c) with TAUPI_CONST
+    cold_plasma: bool = False  # the shear source without -pi/tau_pi (COLDPLASMA test)
     _keep: list = field(default_factory=list, repr=False)
 
     def gdims(self):
@@ -67,6 +68,7 @@ class Config:
         c.gubser_mirror = int(self.gubser_mirror)
         c.minmod_theta = self.minmod_theta
         c.taupi_const = self.taupi_const
+        c.cold_plasma = int(self.cold_plasma)
         return c
 
 
@@ -244,6 +246,16 @@ def landau_match(tmunu10: np.ndarray, tau: float, cartesian: bool = False):
     nf = ctypes.c_longlong()
     A.check(A.lib().vh_landau_match(A.ptr(t), n, tau, int(cartesian), A.ptr(e), A.ptr(u), ctypes.byref(nf)))
     return e, u, nf.value
+
+
+def profile_gubser_cold(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, b=1.21, a=A_QGP):
+    """the cold-plasma viscous Gubser flow at tau0: e, u^x, u^y, pi5 and prevu
+    (at tau0 - dtau) on the 2+1D ghost-inclusive grid"""
+    n = (nx + 6) * (ny + 6)
+    e, ux, uy, pi5, pu = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros((5, n)), np.zeros((4, n))
+    A.check(A.lib().vh_profile_gubser_cold(nx, ny, dx, dy, q, tau0, dtau, b, a, A.ptr(e), A.ptr(ux), A.ptr(uy),
+                                           A.ptr(pi5), A.ptr(pu)))
+    return e, ux, uy, pi5, pu
 
 
 def profile_cgc(nx, ny, nz=1, boost_invariant=True, dx=0.1, dy=0.1, dz=0.1, tau=0.1, e_peak=1.0, x_pos=3.0,
