@@ -101,7 +101,9 @@ VH_HD inline bool landau_cell(const double* T10, double tau, bool cart, double& 
       u[a] = v;
     }
     sig = rayleigh(u);
-    if (d <= 1e-15 * fabs(u[0])) conv = true;
+    // the iteration converges cubically; a change of a few ulps is rounding
+    // noise, so 1e-14 (not 1e-15, where noise can keep it going) ends it
+    if (d <= 1e-14 * fabs(u[0])) conv = true;
   }
   if (!conv) return false;
   // the pair must be an eigenpair: |M u - e u| small against e u^tau
