@@ -248,6 +248,18 @@ MEASURED_TRAFFIC_PER_CELL = {
 }
 
 
+# the bound that does hold for the step kernels: the share of peak of the
+# pipe or issue rate that limits each, from the same ncu captures
+# (profiles/step_kernels_*.md, profiles/update_kernel_*.md)
+MEASURED_COMPUTE_BOUND = {
+    ("fp64", "k_dir_x"): ("fp64 pipe", 0.719), ("fp64", "k_dir_y"): ("fp64 pipe", 0.646),
+    ("fp64", "k_dir_eta"): ("fp64 pipe", 0.682), ("fp64", "k_update_stage1"): ("fp64 pipe", 0.369),
+    ("fp64", "k_update_stage2"): ("fp64 pipe", 0.273),
+    ("mixed", "k_dir_x"): ("fma pipe", 0.677), ("mixed", "k_dir_y"): ("fma pipe", 0.584),
+    ("mixed", "k_dir_eta"): ("fma pipe", 0.632), ("mixed", "k_update_stage2"): ("issue", 0.498),
+}
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -341,6 +353,9 @@ def run_ours(args, rank, world, dist):
                          "traffic": (MEASURED_TRAFFIC_PER_CELL[(args.precision, top)] * cells
                                      if (args.precision, top) in MEASURED_TRAFFIC_PER_CELL else None),
                          "algorithmic_bytes_per_cell": algorithmic_bytes(cfg, top),
+                         "compute_bound_ncu": (dict(zip(("limit", "active_frac_of_peak"),
+                                                        MEASURED_COMPUTE_BOUND[(args.precision, top)]))
+                                               if (args.precision, top) in MEASURED_COMPUTE_BOUND else None),
                          "kernel_ms_per_launch": per_launch, "kernel_share": share},
         }
     return out
