@@ -46,6 +46,13 @@ def test_create_rejects_bad_config_without_gpu():
     assert e.value.code == A.E_ARG
 
 
+def test_create_rejects_bad_relaxation_time_without_gpu():
+    for kw in (dict(taupi_kind=A.TAUPI_CONST, taupi_const=0.0), dict(taupi_kind=7)):
+        with pytest.raises(A.VhError) as e:
+            H.Hydro(H.Config(nx=10, ny=10, **kw))
+        assert e.value.code == A.E_ARG
+
+
 def test_eos_table_properties():
     t = H.eos_table_synthetic(2000, 1e-3, 500.0)
     e, p, cs2, T = t

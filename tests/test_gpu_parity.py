@@ -285,3 +285,25 @@ def test_cold_plasma_gubser_flow():
     err = np.max(np.abs((s[0][m] / A_CONF) ** 0.25 / closed_form_T(r[m], tau) - 1))
     print("cold plasma on the GPU to tau = %.2f: T within %.2e of the closed form" % (tau, err))
     assert err <= 6e-4
+
+
+@pytest.mark.parametrize("cfgkw", [
+    dict(nx=3, ny=3, nz=1, boost_invariant=True),
+    dict(nx=3, ny=4, nz=3),
+    dict(nx=3, ny=3, nz=3, coords=A.COORD_CARTESIAN, tau0=1.0),
+])
+def test_smallest_grids_match_oracle(cfgkw):
+    """three interior cells per axis, the minimum vh_create accepts: every
+    stencil reaches into the ghosts on both sides"""
+    cfg = milne3d(**cfgkw)
+    f = smooth_inputs(cfg, cfg.tau0, seed=9)
+    O = Oracle(oracle_config(cfg))
+    O.set_state(f)
+    tau = cfg.tau0
+    for _ in range(3):
+        assert O.step(tau, cfg.dtau) == 0
+        tau += cfg.dtau
+    with Hydro(cfg) as H:
+        H.set_state(f, cfg.tau0)
+        H.step(3)
+        compare_states(H.get_state(), O.get_state(), 1e-11, fields=range(18))
