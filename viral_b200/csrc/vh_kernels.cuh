@@ -449,21 +449,14 @@ __device__ __forceinline__ void rk_cell(const DevCfg& C, const DevPtrs<R>& P, do
     for (int l = 0; l < 5; l++) q9[4 + l] = Vn[4 + l];
 #pragma unroll
     for (int l = 0; l < 9; l++) P.S(out_b, l)[c] = q9[l];
-    // the root-find's start: e scaled by the change of T^{tau tau} and, at
-    // stage 1, the velocity extrapolated linearly from prevu (the root is
-    // the same; the start is closer to it)
-    const R rt = q9[0] / Tc[0];
-    e_out = (rt > (R)0.5 && rt < (R)2) ? e * rt : e;
-    u_out[0] = u[0];
-#pragma unroll
-    for (int l = 1; l < 4; l++) u_out[l] = STAGE == 1 ? (R)2 * u[l] - pu[l] : u[l];
     // previous velocity (NEWEST5/time.h:166, stage 1 only)
     if (STAGE == 1) {
 #pragma unroll
       for (int l = 0; l < 4; l++) { pu[l] = u[l]; P.pu(l)[c] = u[l]; }
     }
 #pragma unroll
-    for (int l = 0; l < 4; l++) pu_out[l] = pu[l];
+    for (int l = 0; l < 4; l++) { u_out[l] = u[l]; pu_out[l] = pu[l]; }
+    e_out = e;
   }
 }
 
