@@ -7,18 +7,22 @@
  * Test infrastructure only.
  *
  * What is the reference's code here: maindef.h, s95p.h, utils.h (WENO
- * derivative) and ginit.h (thickness, derivatives, T^{mu nu}, FindVar, the
- * pi and T^{tau mu} of the state).  What is ours: the single-rank MPI
- * declarations and a GSL stand-in (ref_shim/), the globals and coordinate
- * functions that init.h would declare (NEWEST5/init.h:18-80, restated for
- * the chosen rank coordinates), no-op MPI file output for ginit's WriteXY,
- * the grid allocation and the state export below.
+ * derivative), ginit.h (thickness, derivatives, T^{mu nu}, FindVar, the pi
+ * and T^{tau mu} of the state) and the step's headers (boundary.h,
+ * Source.h, multiroot.h, hydroKT.h, time.h), so that the window's state can
+ * also be evolved.  What is ours: the single-rank MPI declarations and the
+ * GSL stand-ins (ref_shim/), the globals and coordinate functions that
+ * init.h would declare (NEWEST5/init.h:18-80, restated for the chosen rank
+ * coordinates), no-op MPI file output for ginit's WriteXY, a no-op pack()
+ * and DebugMSG() as in ref_harness.cpp, the grid allocation and the state
+ * export below.
  *
  * Canonical state layout as the oracle's: structure of arrays over the
  * ghost-inclusive grid, index (k*YCM + j)*XCM + i; fields 0 En, 1..4 u,
  * 5..9 pi, 10..13 T^{tau mu}, 14..17 prevu.
  */
 #include <mpi.h>
+#include "gsl_multiroot_shim.h"
 #include "gsl_ginit_shim.h"
 
 #include <iostream>
@@ -75,7 +79,32 @@ inline double ZCORDWB(int) { return 0.0; }
 inline double ZCORDWB(int k) { return (-GRIDZMAX + (k - BORDER) * ZS); }
 #endif
 
+void NSInit(GRID HydroGrid, double tau, double ts);
+void ZeroInit(GRID HydroGrid, double tau, double ts);
+void CheckRoot(GRID HydroGrid, double tau);
+double DebugMSG(GRID HydroGrid, double tau);
+double MaxTempGev(GRID HydroGrid);
+#define BOUNDARY -1
+#define MYXLEFT BOUNDARY
+#define MYXRIGHT BOUNDARY
+#define MYYLEFT BOUNDARY
+#define MYYRIGHT BOUNDARY
+#define MYZLEFT BOUNDARY
+#define MYZRIGHT BOUNDARY
+
 #include "utils.h"
+
+/* one rank: nothing to exchange (every neighbour is BOUNDARY) */
+void pack(GRID) {}
+
+#include "boundary.h"
+
+double DebugMSG(GRID, double) { return 0.0; }
+
+#include "Source.h"
+#include "multiroot.h"
+#include "hydroKT.h"
+#include "time.h"
 #include "ginit.h"
 
 static const size_t NCELL = (size_t)XCM * YCM * ZCM;
@@ -129,6 +158,10 @@ void ref_ginit_run(double tau, double ts) {
   ginit(HydroGrid, tau - ts);
   ginit(HydroGrid, tau);
 }
+
+/* one TVDRK2 step of the reference from tau (NEWEST5/time.h:333-387), with
+ * this rank's window treated as the whole grid (outflow ghosts) */
+void ref_ginit_step(double tau, double ts) { TVDRK2(HydroGrid, tau, ts); }
 
 /* the canonical 18 fields of every cell, and X, Y, eta */
 void ref_ginit_state(double* f, double* x, double* y, double* eta) {

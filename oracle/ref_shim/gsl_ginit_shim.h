@@ -28,7 +28,9 @@
 #include <string.h>
 
 /* ---------------------------------------------------------------- matrices */
+#ifndef VH_REF_SHIM_GSL_H /* gsl_multiroot_shim.h declares the same matrix */
 typedef struct { size_t size1, size2; double* data; } gsl_matrix;
+#endif
 typedef struct { gsl_matrix matrix; } gsl_matrix_view;
 static inline gsl_matrix_view gsl_matrix_view_array(double* base, size_t n1, size_t n2) {
   gsl_matrix_view v;
