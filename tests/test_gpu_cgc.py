@@ -64,3 +64,43 @@ def test_glasma_initial_state(precision):
         print("pi component %d vs the reference (s95p P): %.1e of P" % (m, loose))
         assert loose <= 1e-4
     assert np.max(np.abs(s[10:14] - ref[10:14]) / np.abs(ref[10]).max()) <= 1e-4
+
+
+def test_glasma_evolution_against_the_reference():
+    """the reference's own Glasma state on one rank's window (compiled
+    ginit.h, oracle/_ref/libref_ginit.so) stepped three times by the
+    reference and by the FP64 GPU step, s95p as a 200,000-row table"""
+    import ctypes
+    from pyoracle import HERE as ORACLE_DIR
+    from pyoracle import NF, RefGinit, _ptr
+    if not os.path.exists(os.path.join(ORACLE_DIR, "_ref", "libref_ginit.so")):
+        pytest.skip("reference GINIT build not made")
+    R = RefGinit(4, 4)
+    R.L.ref_ginit_step.argtypes = [ctypes.c_double, ctypes.c_double]
+    f0, _, _, _ = R.run()
+    te = np.geomspace(1e-2, 1e4, 200000)
+    tab = np.array([R.eos(v)[:3] for v in te])
+    table = np.array([te, tab[:, 0], tab[:, 1], tab[:, 2]])
+    cfg = Config(nx=R.gx - 6, ny=R.gy - 6, nz=R.gz - 6, boost_invariant=False, dx=R.dx, dy=R.dy, dz=R.dz,
+                 tau0=R.tau0, dtau=R.ts, eos_kind=A.EOS_TABLE, eos_table=table, etas0=1 / (4 * np.pi), etas1=0.0,
+                 hbarc=R.gevfm)
+    tau = R.tau0
+    for _ in range(3):
+        R.L.ref_ginit_step(tau, R.ts)
+        tau += R.ts
+    fr = np.zeros((NF, R.n))
+    junk = [np.zeros(R.n) for _ in range(3)]
+    R.L.ref_ginit_state(_ptr(fr), *(_ptr(a) for a in junk))
+    with Hydro(cfg) as H:
+        H.set_state(f0, R.tau0)
+        H.step(3)
+        g = H.get_state()
+    idx = np.arange(R.n)
+    i, j, k = idx % R.gx, (idx // R.gx) % R.gy, idx // (R.gx * R.gy)
+    m = (i >= R.il) & (i < R.ir) & (j >= R.jl) & (j < R.jr) & (k >= R.kl) & (k < R.kr)
+    worst = 0.0
+    for grp in ((0,), (1, 2, 3, 4), (5, 6, 7, 8, 9), (10, 11, 12, 13), (14, 15, 16, 17)):
+        scale = max(np.abs(fr[q][m]).max() for q in grp)
+        worst = max(worst, max(np.abs(g[q][m] - fr[q][m]).max() for q in grp) / scale)
+    print("GINIT window, 3 steps: GPU vs reference %.2e (group-relative)" % worst)
+    assert worst <= 1e-9
