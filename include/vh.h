@@ -268,8 +268,9 @@ int vh_last_iterations(vh_handle* h, long long* iters);
  *            doubles) when cfg->eos_kind is VH_EOS_TABLE, else NULL;
  *            cfg->eos_e must still point to the host table
  *   stream:  cudaStream_t to launch on (NULL: the legacy stream)
- * cfg->precision must be VH_PREC_FP64 and the ghost-inclusive grid at most
- * VH_STATIC_MAX_CELLS cells, else VH_E_ARG.  The step's scratch is one
+ * cfg->precision must be VH_PREC_FP64, cfg->taupi_kind one of the two
+ * eta-proportional forms, cfg->cold_plasma 0, and the ghost-inclusive grid
+ * at most VH_STATIC_MAX_CELLS cells, else VH_E_ARG.  The step's scratch is one
  * file-scope device array of 16 MiB that every GPU loading the library holds
  * until exit; all calls share it and it keeps the last call's contents, so
  * calls that overlap on the GPU race (issue them one after another).  The
