@@ -449,14 +449,21 @@ __device__ __forceinline__ void rk_cell(const DevCfg& C, const DevPtrs<R>& P, do
     for (int l = 0; l < 5; l++) q9[4 + l] = Vn[4 + l];
 #pragma unroll
     for (int l = 0; l < 9; l++) P.S(out_b, l)[c] = q9[l];
+    // the root-find's first start: e scaled by the change of T^{tau tau}
+    // and, at stage 1, the velocity extrapolated linearly from prevu (the
+    // root is the same; root_cell falls back to the stage's primitives)
+    const R rt = q9[0] / Tc[0];
+    e_out = (rt > (R)0.5 && rt < (R)2) ? e * rt : e;
+    u_out[0] = u[0];
+#pragma unroll
+    for (int l = 1; l < 4; l++) u_out[l] = STAGE == 1 ? (R)2 * u[l] - pu[l] : u[l];
     // previous velocity (NEWEST5/time.h:166, stage 1 only)
     if (STAGE == 1) {
 #pragma unroll
       for (int l = 0; l < 4; l++) { pu[l] = u[l]; P.pu(l)[c] = u[l]; }
     }
 #pragma unroll
-    for (int l = 0; l < 4; l++) { u_out[l] = u[l]; pu_out[l] = pu[l]; }
-    e_out = e;
+    for (int l = 0; l < 4; l++) pu_out[l] = pu[l];
   }
 }
 
@@ -479,7 +486,20 @@ __device__ __forceinline__ unsigned root_cell(const DevCfg& C, const DevPtrs<R>&
     for (int l = 0; l < 4; l++) Tt[l] = (double)q9[l];
 #pragma unroll
     for (int l = 0; l < 5; l++) pd[l] = (double)q9[4 + l];
-    const int it = con2prim(C, Tt, pd, tau1, x, sizeof(R) == 4 ? 1e-10 : 1e-13, sizeof(R) == 4 ? 1e-6 : 1e-8);
+    const double rtol = sizeof(R) == 4 ? 1e-10 : 1e-13, qtol = sizeof(R) == 4 ? 1e-6 : 1e-8;
+    int it = -1;
+    // a second attempt starts from the stage's primitives, still in memory
+    // (near-vacuum cells, where the extrapolated start can lead Newton
+    // astray); one loop keeps a single copy of the solver in the kernel
+#pragma unroll 1
+    for (int attempt = 0; attempt < 2 && it < 0; attempt++) {
+      if (attempt) {
+        x[0] = (double)P.e()[c];
+#pragma unroll
+        for (int l = 1; l < 4; l++) x[l] = (double)P.u(l)[c];
+      }
+      it = con2prim(C, Tt, pd, tau1, x, rtol, qtol);
+    }
     if (it < 0) {
       atomicOr(P.status, ST_ROOT);
     } else {
