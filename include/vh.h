@@ -389,6 +389,22 @@ int vh_eos_table_synthetic(int n, double emin_gev, double emax_gev, double a, do
 int vh_profile_gubser(int nx, int ny, double dx, double dy, double q, double tau0, double dtau,
                       double t0_gev, double a, double hbarc, double* e, double* ux, double* uy,
                       double* prevu4);
+/* Isothermal freeze-out hypersurface of a boost-invariant run between two
+ * consecutive time slices (no counterpart in the reference, which only stops
+ * at the freeze-out temperature, NEWEST5/main.cpp:201-204).  t0, t1: the
+ * temperature on the ghost-inclusive nx x ny grid at tau0 < tau1 (any unit,
+ * the same as t_fo); u0, u1: u^tau, u^x, u^y there (3 fields).  The surface
+ * T = t_fo of the samples' piecewise-linear interpolant is found by marching
+ * tetrahedra over the space-time cubes between neighbouring interior cell
+ * centres (six tetrahedra per cube); each triangle gives 9 doubles: its centroid (tau, x, y), the
+ * covariant surface element dSigma_mu = tau eps_{mu nu lambda} dx^nu dx^lambda
+ * / 2 per unit rapidity (mu = tau, x, y), pointing from the hot side to the
+ * cold side, and u^tau, u^x, u^y interpolated there.  Writes at most cap
+ * elements into out; *count receives the number found (VH_E_ARG when it
+ * exceeds cap).  Host code. */
+int vh_freezeout_2d(int nx, int ny, double dx, double dy, double tau0, double tau1, const double* t0,
+                    const double* t1, const double* u0, const double* u1, double t_fo, double* out, long long cap,
+                    long long* count);
 /* The viscous Gubser flow of the cold-plasma limit (the reference's
  * COLDPLASMA initial state, NEWEST5/init.h:489-512): conformal e = a T^4
  * with T = T^(rho)/tau, T^ = b sech(rho)^(2/3) cosh(k ln cosh rho)^(1/4),

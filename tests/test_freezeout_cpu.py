@@ -1,0 +1,98 @@
+"""The isothermal freeze-out surface (vh_freezeout_2d, host code) on fields
+whose isotherm is known: a uniform cooling fluid (the surface is tau =
+tau_fo), a static Gaussian (a cylinder r = R_fo), and ideal Gubser flow (the
+analytic isotherm and its normal)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from viral_b200 import _abi as A
+from viral_b200.hydro import freezeout_2d
+
+
+def grid(nx, ny, dx, dy):
+    gx, gy = nx + 6, ny + 6
+    X = -(nx // 2) * dx + (np.arange(gx) - 3) * dx
+    Y = -(ny // 2) * dy + (np.arange(gy) - 3) * dy
+    YY, XX = np.meshgrid(Y, X, indexing="ij")
+    return XX.ravel(), YY.ravel()
+
+
+def at_rest(n):
+    u = np.zeros((3, n))
+    u[0] = 1.0
+    return u
+
+
+def test_uniform_cooling_gives_the_plane_tau_fo():
+    nx, ny, dx, dy = 20, 16, 0.1, 0.2
+    x, _ = grid(nx, ny, dx, dy)
+    n = x.size
+    t0, t1, tfo = 0.20, 0.14, 0.15
+    tau0, tau1 = 2.0, 2.1
+    el = freezeout_2d(nx, ny, dx, dy, tau0, tau1, np.full(n, t0), np.full(n, t1), at_rest(n), at_rest(n), tfo)
+    tau_fo = tau0 + (t0 - tfo) / (t0 - t1) * (tau1 - tau0)
+    assert np.allclose(el[:, 0], tau_fo, rtol=1e-14)
+    assert el[:, 3].sum() == pytest.approx(tau_fo * (nx - 1) * (ny - 1) * dx * dy, rel=1e-12)
+    assert np.all(el[:, 3] > 0)  # pointing to later times, where it is colder
+    assert np.abs(el[:, 4:6]).max() <= 1e-14
+    assert np.allclose(el[:, 6], 1.0) and np.abs(el[:, 7:9]).max() == 0
+
+
+def test_static_gaussian_gives_a_cylinder():
+    nx = ny = 81
+    dx = dy = 0.1
+    x, y = grid(nx, ny, dx, dy)
+    T = 0.3 * np.exp(-(x * x + y * y) / (2 * 1.5 ** 2))
+    tfo = 0.15
+    R = 1.5 * np.sqrt(2 * np.log(0.3 / tfo))
+    tau0, tau1 = 1.0, 1.05
+    el = freezeout_2d(nx, ny, dx, dy, tau0, tau1, T, T, at_rest(x.size), at_rest(x.size), tfo)
+    r = np.hypot(el[:, 1], el[:, 2])
+    assert np.abs(r - R).max() <= 5e-3  # the polygon of the linear interpolant
+    assert np.abs(el[:, 3]).max() <= 1e-14  # time-like normal absent: the surface does not move
+    assert np.all(el[:, 4] * el[:, 1] + el[:, 5] * el[:, 2] > 0)  # outwards, to the cold side
+    # tau eps dx dx / 2 summed: tau_mid * (circumference) * (tau1 - tau0)
+    area = np.hypot(el[:, 4], el[:, 5]).sum()
+    assert area == pytest.approx(0.5 * (tau0 + tau1) * 2 * np.pi * R * (tau1 - tau0), rel=2e-3)
+
+
+def gubser_T(tau, r, q=1.0, c=1.0):
+    return c / (tau ** (1 / 3) * (1 + 2 * q * q * (tau * tau + r * r) + q ** 4 * (tau * tau - r * r) ** 2) ** (1 / 3))
+
+
+def test_ideal_gubser_isotherm_and_normal():
+    nx = ny = 101
+    dx = dy = 0.08
+    x, y = grid(nx, ny, dx, dy)
+    r = np.hypot(x, y)
+    tau0, tau1 = 1.2, 1.21
+    tfo = 0.5 * gubser_T(1.2, 0.0)
+    el = freezeout_2d(nx, ny, dx, dy, tau0, tau1, gubser_T(tau0, r), gubser_T(tau1, r), at_rest(x.size),
+                      at_rest(x.size), tfo)
+    assert len(el) > 100
+    tc, rc = el[:, 0], np.hypot(el[:, 1], el[:, 2])
+    assert np.abs(gubser_T(tc, rc) / tfo - 1).max() <= 2e-3
+    # the normal against -grad T of the closed form (tau, x, y components)
+    h = 1e-6
+    gt = (gubser_T(tc + h, rc) - gubser_T(tc - h, rc)) / (2 * h)
+    gr = (gubser_T(tc, rc + h) - gubser_T(tc, rc - h)) / (2 * h)
+    g = -np.array([gt, gr * el[:, 1] / rc, gr * el[:, 2] / rc]).T
+    n = el[:, 3:6]
+    cosang = (n * g).sum(axis=1) / (np.linalg.norm(n, axis=1) * np.linalg.norm(g, axis=1))
+    assert cosang.min() >= 0.99
+
+
+def test_arguments_and_capacity():
+    L = A.lib()
+    nx = ny = 8
+    n = (nx + 6) * (ny + 6)
+    T0, T1, u = np.full(n, 0.2), np.full(n, 0.1), at_rest(n).ravel().copy()
+    out = np.zeros((4, 9))
+    cnt = ctypes.c_longlong()
+    rc = L.vh_freezeout_2d(nx, ny, 0.1, 0.1, 1.0, 1.1, A.ptr(T0), A.ptr(T1), A.ptr(u), A.ptr(u), 0.15, A.ptr(out), 4,
+                           ctypes.byref(cnt))
+    assert rc == A.E_ARG and cnt.value > 4  # the count is reported although it did not fit
+    assert L.vh_freezeout_2d(nx, ny, 0.1, 0.1, 1.1, 1.0, A.ptr(T0), A.ptr(T1), A.ptr(u), A.ptr(u), 0.15, A.ptr(out),
+                             4, ctypes.byref(cnt)) == A.E_ARG

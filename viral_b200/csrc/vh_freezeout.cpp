@@ -1,0 +1,112 @@
+// Isothermal freeze-out hypersurface of a boost-invariant run, host side:
+// the surface T = T_fo between two consecutive time slices of the
+// ghost-inclusive grid, as triangles of the linear interpolant in
+// (tau, x, y) found by marching tetrahedra (each space-time cube between
+// neighbouring cell centres split into six tetrahedra around its diagonal).
+// The reference stops at the freeze-out temperature (NEWEST5/main.cpp:201-204,
+// MaxTempGev in utils.h:263) and has no hypersurface; this is the step after
+// the path.
+#include <cmath>
+#include <vector>
+
+#include "vh.h"
+
+namespace {
+
+struct Pt {
+  double x[3];  // tau, x, y
+  double u[3];  // u^tau, u^x, u^y
+};
+
+// the six tetrahedra of the unit cube around its diagonal: vertex bits
+// (tau, x, y) in the order 0 -> e_a -> e_a + e_b -> (1, 1, 1)
+const int kTets[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7}, {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
+
+struct Emit {
+  double* out;
+  long long cap, count;
+  void triangle(const Pt& a, const Pt& b, const Pt& c, const double* cold, const double* hot) {
+    // dSigma_mu = (tau / 2) eps_{mu nu lambda} (b - a)^nu (c - a)^lambda per
+    // unit rapidity, oriented from the hot side to the cold side
+    double e1[3], e2[3], n[3];
+    for (int q = 0; q < 3; q++) { e1[q] = b.x[q] - a.x[q]; e2[q] = c.x[q] - a.x[q]; }
+    n[0] = 0.5 * (e1[1] * e2[2] - e1[2] * e2[1]);
+    n[1] = 0.5 * (e1[2] * e2[0] - e1[0] * e2[2]);
+    n[2] = 0.5 * (e1[0] * e2[1] - e1[1] * e2[0]);
+    double d = 0;
+    for (int q = 0; q < 3; q++) d += n[q] * (cold[q] - hot[q]);
+    const double s = d < 0 ? -1.0 : 1.0;
+    const double tc = (a.x[0] + b.x[0] + c.x[0]) / 3;
+    if (count < cap) {
+      double* o = out + 9 * count;
+      for (int q = 0; q < 3; q++) o[q] = (a.x[q] + b.x[q] + c.x[q]) / 3;
+      for (int q = 0; q < 3; q++) o[3 + q] = s * tc * n[q];
+      for (int q = 0; q < 3; q++) o[6 + q] = (a.u[q] + b.u[q] + c.u[q]) / 3;
+    }
+    count++;
+  }
+};
+
+Pt edge_point(const double* xa, const double* xb, const double* ua, const double* ub, double fa, double fb) {
+  const double w = fa / (fa - fb);
+  Pt p;
+  for (int q = 0; q < 3; q++) {
+    p.x[q] = xa[q] + w * (xb[q] - xa[q]);
+    p.u[q] = ua[q] + w * (ub[q] - ua[q]);
+  }
+  return p;
+}
+
+}  // namespace
+
+extern "C" int vh_freezeout_2d(int nx, int ny, double dx, double dy, double tau0, double tau1, const double* t0,
+                               const double* t1, const double* u0, const double* u1, double t_fo, double* out,
+                               long long cap, long long* count) {
+  if (nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0) || !(tau1 > tau0) || !t0 || !t1 || !u0 || !u1 || !count ||
+      (cap > 0 && !out) || cap < 0)
+    return VH_E_ARG;
+  const int G = 3, gx = nx + 2 * G, gy = ny + 2 * G;
+  const long long n = (long long)gx * gy;
+  const double x0 = -((double)(nx / 2) * dx), y0 = -((double)(ny / 2) * dy);
+  Emit em{out, cap, 0};
+  for (int j = G; j < G + ny - 1; j++)
+    for (int i = G; i < G + nx - 1; i++) {
+      double xs[8][3], us[8][3], f[8];
+      bool pos = false, neg = false;
+      for (int v = 0; v < 8; v++) {
+        const int bt = v & 1, bx = (v >> 1) & 1, by = (v >> 2) & 1;
+        const long long c = (long long)(j + by) * gx + (i + bx);
+        const double* T = bt ? t1 : t0;
+        const double* U = bt ? u1 : u0;
+        xs[v][0] = bt ? tau1 : tau0;
+        xs[v][1] = x0 + (i + bx - G) * dx;
+        xs[v][2] = y0 + (j + by - G) * dy;
+        for (int q = 0; q < 3; q++) us[v][q] = U[q * n + c];
+        f[v] = T[c] - t_fo;
+        if (f[v] > 0) pos = true; else neg = true;
+      }
+      if (!pos || !neg) continue;
+      for (const auto& tet : kTets) {
+        int hot[4], cold[4], nh = 0, nc = 0;
+        for (int q = 0; q < 4; q++) {
+          if (f[tet[q]] > 0) hot[nh++] = tet[q]; else cold[nc++] = tet[q];
+        }
+        if (!nh || !nc) continue;
+        const double* ph = xs[hot[0]];
+        const double* pc = xs[cold[0]];
+        auto P = [&](int a, int b) { return edge_point(xs[a], xs[b], us[a], us[b], f[a], f[b]); };
+        if (nh == 1 || nc == 1) {
+          const int lone = nh == 1 ? hot[0] : cold[0];
+          const int* other = nh == 1 ? cold : hot;
+          em.triangle(P(lone, other[0]), P(lone, other[1]), P(lone, other[2]), pc, ph);
+        } else {
+          // two against two: a quadrilateral a-b-c-d split into two triangles
+          const Pt a = P(hot[0], cold[0]), b = P(hot[0], cold[1]), c = P(hot[1], cold[1]), d = P(hot[1], cold[0]);
+          em.triangle(a, b, c, pc, ph);
+          em.triangle(a, c, d, pc, ph);
+        }
+      }
+    }
+  *count = em.count;
+  return em.count > cap ? VH_E_ARG : VH_OK;
+}

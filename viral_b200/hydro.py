@@ -248,6 +248,20 @@ def landau_match(tmunu10: np.ndarray, tau: float, cartesian: bool = False):
     return e, u, nf.value
 
 
+def freezeout_2d(nx, ny, dx, dy, tau0, tau1, T0, T1, u0, u1, t_fo):
+    """the isothermal surface T = t_fo between two time slices of a
+    boost-invariant run: (count, 9) rows of centroid (tau, x, y), dSigma_mu
+    per unit rapidity (tau, x, y) and u^tau, u^x, u^y"""
+    c = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    T0, T1, u0, u1 = c(T0), c(T1), c(np.asarray(u0)[:3]), c(np.asarray(u1)[:3])
+    cap = 12 * (nx - 1) * (ny - 1)
+    out = np.zeros((cap, 9))
+    cnt = ctypes.c_longlong()
+    A.check(A.lib().vh_freezeout_2d(nx, ny, dx, dy, tau0, tau1, A.ptr(T0), A.ptr(T1), A.ptr(u0), A.ptr(u1), t_fo,
+                                    A.ptr(out), cap, ctypes.byref(cnt)))
+    return out[:cnt.value]
+
+
 def profile_gubser_cold(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, b=1.21, a=A_QGP):
     """the cold-plasma viscous Gubser flow at tau0: e, u^x, u^y, pi5 and prevu
     (at tau0 - dtau) on the 2+1D ghost-inclusive grid"""
