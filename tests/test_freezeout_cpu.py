@@ -73,7 +73,7 @@ def test_ideal_gubser_isotherm_and_normal():
                       at_rest(x.size), tfo)
     assert len(el) > 100
     tc, rc = el[:, 0], np.hypot(el[:, 1], el[:, 2])
-    assert np.abs(gubser_T(tc, rc) / tfo - 1).max() <= 2e-3
+    assert np.abs(gubser_T(tc, rc) / tfo - 1).max() <= 1e-3
     # the normal against -grad T of the closed form (tau, x, y components)
     h = 1e-6
     gt = (gubser_T(tc + h, rc) - gubser_T(tc - h, rc)) / (2 * h)
@@ -81,7 +81,7 @@ def test_ideal_gubser_isotherm_and_normal():
     g = -np.array([gt, gr * el[:, 1] / rc, gr * el[:, 2] / rc]).T
     n = el[:, 3:6]
     cosang = (n * g).sum(axis=1) / (np.linalg.norm(n, axis=1) * np.linalg.norm(g, axis=1))
-    assert cosang.min() >= 0.99
+    assert cosang.min() >= 0.999  # within 2.6 degrees
 
 
 def test_arguments_and_capacity():
