@@ -405,6 +405,14 @@ int vh_profile_gubser(int nx, int ny, double dx, double dy, double q, double tau
 int vh_freezeout_2d(int nx, int ny, double dx, double dy, double tau0, double tau1, const double* t0,
                     const double* t1, const double* u0, const double* u1, double t_fo, double* out, long long cap,
                     long long* count);
+/* The same on a 3+1D Milne grid (nx x ny x nz cells of dx, dy, d eta):
+ * marching 4-simplices (24 per space-time hypercube) give tetrahedra; each
+ * gives 12 doubles: its centroid (tau, x, y, eta), dSigma_mu = tau
+ * eps_{mu nu lambda rho} dx^nu dx^lambda dx^rho / 6 (mu = tau, x, y, eta),
+ * hot to cold, and u^mu interpolated there (u0, u1: 4 fields). */
+int vh_freezeout_3d(int nx, int ny, int nz, double dx, double dy, double dz, double tau0, double tau1,
+                    const double* t0, const double* t1, const double* u0, const double* u1, double t_fo, double* out,
+                    long long cap, long long* count);
 /* The viscous Gubser flow of the cold-plasma limit (the reference's
  * COLDPLASMA initial state, NEWEST5/init.h:489-512): conformal e = a T^4
  * with T = T^(rho)/tau, T^ = b sech(rho)^(2/3) cosh(k ln cosh rho)^(1/4),

@@ -96,3 +96,50 @@ def test_arguments_and_capacity():
     assert rc == A.E_ARG and cnt.value > 4  # the count is reported although it did not fit
     assert L.vh_freezeout_2d(nx, ny, 0.1, 0.1, 1.1, 1.0, A.ptr(T0), A.ptr(T1), A.ptr(u), A.ptr(u), 0.15, A.ptr(out),
                              4, ctypes.byref(cnt)) == A.E_ARG
+
+
+def grid3(nx, ny, nz, dx, dy, dz):
+    gx, gy, gz = nx + 6, ny + 6, nz + 6
+    X = -(nx // 2) * dx + (np.arange(gx) - 3) * dx
+    Y = -(ny // 2) * dy + (np.arange(gy) - 3) * dy
+    Z = -(nz // 2) * dz + (np.arange(gz) - 3) * dz
+    ZZ, YY, XX = np.meshgrid(Z, Y, X, indexing="ij")
+    return XX.ravel(), YY.ravel(), ZZ.ravel()
+
+
+def test_3d_uniform_cooling_gives_the_plane_tau_fo():
+    from viral_b200.hydro import freezeout_3d
+    nx, ny, nz, dx, dy, dz = 6, 5, 4, 0.1, 0.2, 0.25
+    x, _, _ = grid3(nx, ny, nz, dx, dy, dz)
+    n = x.size
+    u = np.zeros((4, n))
+    u[0] = 1.0
+    t0, t1, tfo, tau0, tau1 = 0.2, 0.14, 0.15, 2.0, 2.1
+    el = freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, np.full(n, t0), np.full(n, t1), u, u, tfo)
+    tau_fo = tau0 + (t0 - tfo) / (t0 - t1) * (tau1 - tau0)
+    assert np.allclose(el[:, 0], tau_fo, rtol=1e-14)
+    assert el[:, 4].sum() == pytest.approx(tau_fo * (nx - 1) * (ny - 1) * (nz - 1) * dx * dy * dz, rel=1e-12)
+    assert np.all(el[:, 4] > 0) and np.abs(el[:, 5:8]).max() <= 1e-14
+
+
+def test_3d_static_ball_gives_a_sphere():
+    """a static Gaussian in (x, y, eta): the surface is a sphere of the
+    coordinate space; its dSigma (x, y, eta) point outwards and add up to
+    tau 4 pi R^2 (tau1 - tau0)"""
+    from viral_b200.hydro import freezeout_3d
+    nx = ny = nz = 33
+    d = 0.1
+    x, y, z = grid3(nx, ny, nz, d, d, d)
+    T = 0.3 * np.exp(-(x * x + y * y + z * z) / (2 * 0.6 ** 2))
+    tfo = 0.15
+    R = 0.6 * np.sqrt(2 * np.log(2.0))
+    u = np.zeros((4, x.size))
+    u[0] = 1.0
+    tau0, tau1 = 1.0, 1.05
+    el = freezeout_3d(nx, ny, nz, d, d, d, tau0, tau1, T, T, u, u, tfo)
+    r = np.linalg.norm(el[:, 1:4], axis=1)
+    assert np.abs(r - R).max() <= 6e-3
+    assert np.abs(el[:, 4]).max() <= 1e-14
+    assert np.all((el[:, 5:8] * el[:, 1:4]).sum(axis=1) > 0)
+    area = np.linalg.norm(el[:, 5:8], axis=1).sum()
+    assert area == pytest.approx(0.5 * (tau0 + tau1) * 4 * np.pi * R * R * (tau1 - tau0), rel=1e-2)

@@ -262,6 +262,20 @@ def freezeout_2d(nx, ny, dx, dy, tau0, tau1, T0, T1, u0, u1, t_fo):
     return out[:cnt.value]
 
 
+def freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, T0, T1, u0, u1, t_fo):
+    """the isothermal surface T = t_fo between two time slices of a 3+1D
+    run: (count, 12) rows of centroid (tau, x, y, eta), dSigma_mu (tau, x,
+    y, eta) and u^mu"""
+    c = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    T0, T1, u0, u1 = c(T0), c(T1), c(np.asarray(u0)[:4]), c(np.asarray(u1)[:4])
+    cap = 72 * (nx - 1) * (ny - 1) * (nz - 1)
+    out = np.zeros((cap, 12))
+    cnt = ctypes.c_longlong()
+    A.check(A.lib().vh_freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, A.ptr(T0), A.ptr(T1), A.ptr(u0), A.ptr(u1),
+                                    t_fo, A.ptr(out), cap, ctypes.byref(cnt)))
+    return out[:cnt.value]
+
+
 def profile_gubser_cold(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, b=1.21, a=A_QGP):
     """the cold-plasma viscous Gubser flow at tau0: e, u^x, u^y, pi5 and prevu
     (at tau0 - dtau) on the 2+1D ghost-inclusive grid"""
