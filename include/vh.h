@@ -405,6 +405,13 @@ int vh_profile_gubser(int nx, int ny, double dx, double dy, double q, double tau
 int vh_freezeout_2d(int nx, int ny, double dx, double dy, double tau0, double tau1, const double* t0,
                     const double* t1, const double* u0, const double* u1, double t_fo, double* out, long long cap,
                     long long* count);
+/* Boltzmann Cooper-Frye spectrum E dN/d^3p at mid-rapidity from count
+ * elements of vh_freezeout_2d (boost invariant, u^eta = 0; the rapidity
+ * integral done with K0, K1): out[a * nphi + b] at p_T = pt[a], azimuth
+ * phi[b], for a hadron of mass and degeneracy at the surface temperature
+ * t_fo (mass, momenta and t_fo in the same unit, e.g. fm^-1).  Host code. */
+int vh_cooper_frye_2d(const double* elements, long long count, double t_fo, double mass, double degeneracy,
+                      const double* pt, int npt, const double* phi, int nphi, double* out);
 /* The same on a 3+1D Milne grid (nx x ny x nz cells of dx, dy, d eta):
  * marching 4-simplices (24 per space-time hypercube) give tetrahedra; each
  * gives 12 doubles: its centroid (tau, x, y, eta), dSigma_mu = tau

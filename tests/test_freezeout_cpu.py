@@ -143,3 +143,48 @@ def test_3d_static_ball_gives_a_sphere():
     assert np.all((el[:, 5:8] * el[:, 1:4]).sum(axis=1) > 0)
     area = np.linalg.norm(el[:, 5:8], axis=1).sum()
     assert area == pytest.approx(0.5 * (tau0 + tau1) * 4 * np.pi * R * R * (tau1 - tau0), rel=1e-2)
+
+
+def test_cooper_frye_on_known_surfaces():
+    """Boltzmann spectra (vh_cooper_frye_2d): a plane tau = tau_fo of a fluid
+    at rest gives g A tau_fo 2 m_T K1(m_T/T) / (2 pi)^3 and, integrated, A
+    tau_fo times the equilibrium density; a uniformly moving fluid adds its
+    Lorentz factor and boost; a static closed cylinder emits nothing net"""
+    from scipy import integrate, special
+    from viral_b200.hydro import cooper_frye_2d
+    nx, ny, dx, dy = 20, 16, 0.1, 0.2
+    x, _ = grid(nx, ny, dx, dy)
+    n = x.size
+    tfo, m, g = 0.15 / 0.19733, 0.14 / 0.19733, 3.0  # fm^-1: 150 MeV, a pion-like mass
+    tau0, tau1 = 2.0, 2.1
+    el = freezeout_2d(nx, ny, dx, dy, tau0, tau1, np.full(n, 1.2 * tfo), np.full(n, 0.8 * tfo), at_rest(n), at_rest(n),
+                      tfo)
+    A_tau = el[:, 3].sum()
+    pt = np.array([0.5, 1.0, 2.0, 5.0])
+    phi = np.linspace(0, 2 * np.pi, 5, endpoint=False)
+    sp = cooper_frye_2d(el, tfo, m, g, pt, phi)
+    mt = np.sqrt(m * m + pt * pt)
+    want = g * A_tau * 2 * mt * special.k1(mt / tfo) / (2 * np.pi) ** 3
+    assert np.allclose(sp, want[:, None], rtol=1e-12)
+    dndy = integrate.quad(lambda p: 2 * np.pi * p * cooper_frye_2d(el, tfo, m, g, [p], [0.0])[0, 0], 0, 60 * tfo,
+                          epsrel=1e-10)[0]
+    n_eq = g * m * m * tfo * special.kn(2, m / tfo) / (2 * np.pi ** 2)
+    assert dndy == pytest.approx(A_tau * n_eq, rel=1e-7)
+    # a uniformly moving fluid: u = (gamma, gamma v, 0)
+    v = 0.4
+    gam = 1 / np.sqrt(1 - v * v)
+    u = np.zeros((3, n))
+    u[0], u[1] = gam, gam * v
+    el = freezeout_2d(nx, ny, dx, dy, tau0, tau1, np.full(n, 1.2 * tfo), np.full(n, 0.8 * tfo), u, u, tfo)
+    sp = cooper_frye_2d(el, tfo, m, g, pt, phi)
+    px = pt[:, None] * np.cos(phi)[None, :]
+    want = g * A_tau * 2 * mt[:, None] * special.k1(mt[:, None] * gam / tfo) * np.exp(px * gam * v / tfo) / (2 * np.pi) ** 3
+    assert np.allclose(sp, want, rtol=1e-12)
+    # a static cylinder at rest: the outgoing and incoming halves cancel
+    nx = ny = 41
+    x, y = grid(nx, ny, 0.1, 0.1)
+    T = 0.3 * np.exp(-(x * x + y * y) / (2 * 1.0 ** 2))
+    el = freezeout_2d(nx, ny, 0.1, 0.1, 1.0, 1.05, T, T, at_rest(x.size), at_rest(x.size), 0.15)
+    sp = cooper_frye_2d(el, 0.15, 0.3, 1.0, [0.2, 0.5], [0.0, 1.0])
+    scale = cooper_frye_2d(np.abs(el), 0.15, 0.3, 1.0, [0.2, 0.5], [0.0, 1.0])
+    assert np.abs(sp).max() <= 1e-12 * np.abs(scale).max()

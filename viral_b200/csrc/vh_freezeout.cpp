@@ -236,3 +236,34 @@ extern "C" int vh_freezeout_3d(int nx, int ny, int nz, double dx, double dy, dou
   *count = em.count;
   return em.count > cap ? VH_E_ARG : VH_OK;
 }
+
+// ------------------------------------------------------ Cooper-Frye spectra
+// Boltzmann spectrum at mid-rapidity from the surface elements of
+// vh_freezeout_2d (boost invariant, u^eta = 0): with p^mu dSigma_mu =
+// m_T cosh(y - eta) dSigma_tau + p_x dSigma_x + p_y dSigma_y and
+// p.u = m_T u^tau cosh(y - eta) - p_x u^x - p_y u^y, the rapidity integral
+// gives Bessel functions, int deta cosh(eta) e^{-a cosh eta} = 2 K1(a) and
+// int deta e^{-a cosh eta} = 2 K0(a):
+//   E dN/d^3p = g / (2 pi)^3 sum [2 m_T K1(a) dSigma_tau + 2 K0(a) (p_x dSigma_x
+//               + p_y dSigma_y)] exp((p_x u^x + p_y u^y) / T),  a = m_T u^tau / T.
+extern "C" int vh_cooper_frye_2d(const double* elements, long long count, double t_fo, double mass, double degeneracy,
+                                 const double* pt, int npt, const double* phi, int nphi, double* out) {
+  if (!elements || count < 0 || !(t_fo > 0) || mass < 0 || !pt || !phi || npt < 1 || nphi < 1 || !out)
+    return VH_E_ARG;
+  const double pref = degeneracy / (8 * M_PI * M_PI * M_PI);
+  for (int a = 0; a < npt; a++)
+    for (int b = 0; b < nphi; b++) {
+      const double mt = std::sqrt(mass * mass + pt[a] * pt[a]);
+      const double px = pt[a] * std::cos(phi[b]), py = pt[a] * std::sin(phi[b]);
+      double sum = 0;
+      for (long long e = 0; e < count; e++) {
+        const double* el = elements + 9 * e;
+        const double arg = mt * el[6] / t_fo;
+        const double boost = std::exp((px * el[7] + py * el[8]) / t_fo);
+        sum += (2 * mt * std::cyl_bessel_k(1.0, arg) * el[3] + 2 * std::cyl_bessel_k(0.0, arg) * (px * el[4] + py * el[5])) *
+               boost;
+      }
+      out[(long long)a * nphi + b] = pref * sum;
+    }
+  return VH_OK;
+}
