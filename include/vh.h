@@ -401,7 +401,7 @@ int vh_profile_gubser(int nx, int ny, double dx, double dy, double q, double tau
  * / 2 per unit rapidity (mu = tau, x, y), pointing from the hot side to the
  * cold side, and u^tau, u^x, u^y interpolated there.  Writes at most cap
  * elements into out; *count receives the number found (VH_E_ARG when it
- * exceeds cap).  Host code. */
+ * exceeds cap; cap = 0 with out = NULL only counts).  Host code. */
 int vh_freezeout_2d(int nx, int ny, double dx, double dy, double tau0, double tau1, const double* t0,
                     const double* t1, const double* u0, const double* u1, double t_fo, double* out, long long cap,
                     long long* count);

@@ -254,11 +254,11 @@ def freezeout_2d(nx, ny, dx, dy, tau0, tau1, T0, T1, u0, u1, t_fo):
     per unit rapidity (tau, x, y) and u^tau, u^x, u^y"""
     c = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
     T0, T1, u0, u1 = c(T0), c(T1), c(np.asarray(u0)[:3]), c(np.asarray(u1)[:3])
-    cap = 12 * (nx - 1) * (ny - 1)
-    out = np.zeros((cap, 9))
     cnt = ctypes.c_longlong()
-    A.check(A.lib().vh_freezeout_2d(nx, ny, dx, dy, tau0, tau1, A.ptr(T0), A.ptr(T1), A.ptr(u0), A.ptr(u1), t_fo,
-                                    A.ptr(out), cap, ctypes.byref(cnt)))
+    args = (nx, ny, dx, dy, tau0, tau1, A.ptr(T0), A.ptr(T1), A.ptr(u0), A.ptr(u1), t_fo)
+    A.lib().vh_freezeout_2d(*args, None, 0, ctypes.byref(cnt))  # counts the elements
+    out = np.zeros((max(cnt.value, 1), 9))
+    A.check(A.lib().vh_freezeout_2d(*args, A.ptr(out), cnt.value, ctypes.byref(cnt)))
     return out[:cnt.value]
 
 
@@ -280,11 +280,11 @@ def freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, T0, T1, u0, u1, t_fo):
     y, eta) and u^mu"""
     c = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
     T0, T1, u0, u1 = c(T0), c(T1), c(np.asarray(u0)[:4]), c(np.asarray(u1)[:4])
-    cap = 72 * (nx - 1) * (ny - 1) * (nz - 1)
-    out = np.zeros((cap, 12))
     cnt = ctypes.c_longlong()
-    A.check(A.lib().vh_freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, A.ptr(T0), A.ptr(T1), A.ptr(u0), A.ptr(u1),
-                                    t_fo, A.ptr(out), cap, ctypes.byref(cnt)))
+    args = (nx, ny, nz, dx, dy, dz, tau0, tau1, A.ptr(T0), A.ptr(T1), A.ptr(u0), A.ptr(u1), t_fo)
+    A.lib().vh_freezeout_3d(*args, None, 0, ctypes.byref(cnt))  # counts the elements
+    out = np.zeros((max(cnt.value, 1), 12))
+    A.check(A.lib().vh_freezeout_3d(*args, A.ptr(out), cnt.value, ctypes.byref(cnt)))
     return out[:cnt.value]
 
 
