@@ -412,6 +412,10 @@ int vh_freezeout_2d(int nx, int ny, double dx, double dy, double tau0, double ta
  * t_fo (mass, momenta and t_fo in the same unit, e.g. fm^-1).  Host code. */
 int vh_cooper_frye_2d(const double* elements, long long count, double t_fo, double mass, double degeneracy,
                       const double* pt, int npt, const double* phi, int nphi, double* out);
+/* The same at rapidity y from count elements of vh_freezeout_3d (each at
+ * its own eta; u^eta included).  Host code. */
+int vh_cooper_frye_3d(const double* elements, long long count, double t_fo, double mass, double degeneracy, double y,
+                      const double* pt, int npt, const double* phi, int nphi, double* out);
 /* The same on a 3+1D Milne grid (nx x ny x nz cells of dx, dy, d eta):
  * marching 4-simplices (24 per space-time hypercube) give tetrahedra; each
  * gives 12 doubles: its centroid (tau, x, y, eta), dSigma_mu = tau

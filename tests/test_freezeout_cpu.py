@@ -188,3 +188,25 @@ def test_cooper_frye_on_known_surfaces():
     sp = cooper_frye_2d(el, 0.15, 0.3, 1.0, [0.2, 0.5], [0.0, 1.0])
     scale = cooper_frye_2d(np.abs(el), 0.15, 0.3, 1.0, [0.2, 0.5], [0.0, 1.0])
     assert np.abs(sp).max() <= 1e-12 * np.abs(scale).max()
+
+
+def test_cooper_frye_3d_reduces_to_the_boost_invariant_result():
+    """a fluid at rest, uniform in x, y, eta over eta in [-6, 6] and cooling
+    through T_fo: the 3+1D sum over the surface's eta cells approaches the
+    rapidity integral of the boost-invariant formula (2 m_T K1) at y = 0
+    (the midpoint rule in eta converges geometrically for this integrand)"""
+    from scipy import special
+    from viral_b200.hydro import cooper_frye_3d, freezeout_3d
+    nx, ny, nz, dx, dy, dz = 4, 4, 121, 0.2, 0.2, 0.1
+    x, _, _ = grid3(nx, ny, nz, dx, dy, dz)
+    n = x.size
+    u = np.zeros((4, n))
+    u[0] = 1.0
+    tfo, m, g = 0.76, 0.71, 1.0
+    el = freezeout_3d(nx, ny, nz, dx, dy, dz, 2.0, 2.1, np.full(n, 1.1 * tfo), np.full(n, 0.9 * tfo), u, u, tfo)
+    A_tau = el[:, 4].sum() / ((nz - 1) * dz)  # per unit rapidity
+    pt = np.array([0.3, 1.0, 3.0])
+    sp = cooper_frye_3d(el, tfo, m, g, 0.0, pt, [0.0, 1.0])
+    mt = np.sqrt(m * m + pt * pt)
+    want = g * A_tau * 2 * mt * special.k1(mt / tfo) / (2 * np.pi) ** 3
+    assert np.allclose(sp, want[:, None], rtol=1e-10)

@@ -267,3 +267,31 @@ extern "C" int vh_cooper_frye_2d(const double* elements, long long count, double
     }
   return VH_OK;
 }
+
+// The same on the 3+1D surface of vh_freezeout_3d, at rapidity y: each
+// element sits at its own eta, so the sum runs over the elements directly,
+//   p^tau = m_T cosh(y - eta), p^eta = m_T sinh(y - eta) / tau,
+//   p.u = p^tau u^tau - p_x u^x - p_y u^y - tau^2 p^eta u^eta,
+//   E dN/d^3p = g / (2 pi)^3 sum p^mu dSigma_mu exp(-p.u / T).
+extern "C" int vh_cooper_frye_3d(const double* elements, long long count, double t_fo, double mass, double degeneracy,
+                                 double y, const double* pt, int npt, const double* phi, int nphi, double* out) {
+  if (!elements || count < 0 || !(t_fo > 0) || mass < 0 || !pt || !phi || npt < 1 || nphi < 1 || !out)
+    return VH_E_ARG;
+  const double pref = degeneracy / (8 * M_PI * M_PI * M_PI);
+  for (int a = 0; a < npt; a++)
+    for (int b = 0; b < nphi; b++) {
+      const double mt = std::sqrt(mass * mass + pt[a] * pt[a]);
+      const double px = pt[a] * std::cos(phi[b]), py = pt[a] * std::sin(phi[b]);
+      double sum = 0;
+      for (long long e = 0; e < count; e++) {
+        const double* el = elements + 12 * e;
+        const double tau = el[0], eta = el[3];
+        const double pt_ = mt * std::cosh(y - eta), pe = mt * std::sinh(y - eta) / tau;
+        const double pds = pt_ * el[4] + px * el[5] + py * el[6] + pe * el[7];
+        const double pu = pt_ * el[8] - px * el[9] - py * el[10] - tau * tau * pe * el[11];
+        sum += pds * std::exp(-pu / t_fo);
+      }
+      out[(long long)a * nphi + b] = pref * sum;
+    }
+  return VH_OK;
+}

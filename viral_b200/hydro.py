@@ -274,6 +274,18 @@ def cooper_frye_2d(elements, t_fo, mass, degeneracy, pt, phi):
     return out
 
 
+def cooper_frye_3d(elements, t_fo, mass, degeneracy, y, pt, phi):
+    """Boltzmann E dN/d^3p at rapidity y (len(pt), len(phi)) from the
+    elements of freezeout_3d"""
+    el = np.ascontiguousarray(elements, dtype=np.float64).reshape(-1, 12)
+    pt = np.ascontiguousarray(pt, dtype=np.float64).reshape(-1)
+    phi = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
+    out = np.zeros((pt.size, phi.size))
+    A.check(A.lib().vh_cooper_frye_3d(A.ptr(el), el.shape[0], t_fo, mass, degeneracy, y, A.ptr(pt), pt.size,
+                                      A.ptr(phi), phi.size, A.ptr(out)))
+    return out
+
+
 def freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, T0, T1, u0, u1, t_fo):
     """the isothermal surface T = t_fo between two time slices of a 3+1D
     run: (count, 12) rows of centroid (tau, x, y, eta), dSigma_mu (tau, x,
