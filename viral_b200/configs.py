@@ -9,6 +9,11 @@ glauber_161x161x41 3+1D Milne event: 161x161x41, dx = dy = 0.1 fm,
                   d eta = 0.25, tau0 = 0.6 -> 10 fm/c, dtau = 0.02 (470 steps),
                   MC-Glauber Pb+Pb b = 7 fm (seed 0), synthetic EOS table,
                   eta/s = 0.08, tau_pi = 1.5 eta/P, u = 0, pi = 0.
+bjorken           the reference's Bjorken block: a uniform fluid at rest in
+                  Milne coordinates, 10x10 cells, e = 30 GeV/fm^3 at 0.6 fm/c,
+                  eta = 0.2 s, tau_pi = 0.01 fm/c (bjorken_config/_inputs).
+The reference's cold-plasma Gubser test and its Glasma initial state come
+from the generators in hydro.py (profile_gubser_cold, profile_cgc).
 """
 from __future__ import annotations
 
