@@ -424,6 +424,32 @@ int vh_cooper_frye_3d(const double* elements, long long count, double t_fo, doub
 int vh_freezeout_3d(int nx, int ny, int nz, double dx, double dy, double dz, double tau0, double tau1,
                     const double* t0, const double* t1, const double* u0, const double* u1, double t_fo, double* out,
                     long long cap, long long* count);
+/* The surfaces of vh_freezeout_2d and vh_freezeout_3d computed on the GPU
+ * from device arrays (t0, t1: the ghost-inclusive slice, G doubles each;
+ * u0, u1: 3 x G or 4 x G) into device memory out (cap elements of 9 or 12
+ * doubles), element for element in the host functions' order: a count pass
+ * over the space-time cubes, an exclusive scan, an emit pass.  cap = 0 with
+ * out = NULL only counts.  Issued on stream (a cudaStream_t; NULL: the
+ * legacy stream), which is synchronised to return *count; scratch comes from
+ * the stream-ordered allocator.  Returns VH_E_ARG, with *count set, when
+ * the surface has more than cap elements (the first cap are written). */
+int vh_freezeout_2d_device(int nx, int ny, double dx, double dy, double tau0, double tau1, const double* t0,
+                           const double* t1, const double* u0, const double* u1, double t_fo, double* out,
+                           long long cap, long long* count, void* stream);
+int vh_freezeout_3d_device(int nx, int ny, int nz, double dx, double dy, double dz, double tau0, double tau1,
+                           const double* t0, const double* t1, const double* u0, const double* u1, double t_fo,
+                           double* out, long long cap, long long* count, void* stream);
+/* vh_cooper_frye_2d and vh_cooper_frye_3d on the GPU: elements in device
+ * memory (count x 9 or 12 doubles), momentum bins pt, phi and the result
+ * out (npt x nphi) on the host; one block per bin sums the elements in a
+ * fixed order.  The 2+1D form evaluates K0 and K1 by the trapezoidal rule
+ * on their integral representation (relative error within 4e-15).
+ * Synchronises stream before returning. */
+int vh_cooper_frye_2d_device(const double* elements, long long count, double t_fo, double mass, double degeneracy,
+                             const double* pt, int npt, const double* phi, int nphi, double* out, void* stream);
+int vh_cooper_frye_3d_device(const double* elements, long long count, double t_fo, double mass, double degeneracy,
+                             double y, const double* pt, int npt, const double* phi, int nphi, double* out,
+                             void* stream);
 /* The viscous Gubser flow of the cold-plasma limit (the reference's
  * COLDPLASMA initial state, NEWEST5/init.h:489-512): conformal e = a T^4
  * with T = T^(rho)/tau, T^ = b sech(rho)^(2/3) cosh(k ln cosh rho)^(1/4),

@@ -120,6 +120,21 @@ SIGNATURES = [
                                          ctypes.c_int, _dp, ctypes.c_int, _dp]),
     ("vh_cooper_frye_3d", ctypes.c_int, [_dp, ctypes.c_longlong, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp]),
+    ("vh_freezeout_2d_device", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                              ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p]),
+    ("vh_freezeout_3d_device", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong,
+                                              ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p]),
+    ("vh_cooper_frye_2d_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                                ctypes.c_void_p]),
+    ("vh_cooper_frye_3d_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int, _dp,
+                                                ctypes.c_int, _dp, ctypes.c_void_p]),
     ("vh_init_prevu_tmunu", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("vh_profile_cgc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,

@@ -8,6 +8,7 @@
 #include "vh.h"
 #include "vh_adjoint.cuh"
 #include "vh_aux.cuh"
+#include "vh_freezeout.cuh"
 
 using namespace vh;
 
@@ -101,4 +102,47 @@ void vhc_eos_d(const vh_config* c, double e, double* out4) {
   HostCfg h = make_cfg(c);
   eos_d<double>(h.C, e, out4[0], out4[1], out4[2], out4[3]);
 }
+
+// The algorithm of vh_freezeout_{2d,3d}_device run on the host with the same
+// per-cube functions: every cube's count, their exclusive scan, then each
+// cube's elements written from its offset, the cubes visited in the order
+// perm (a permutation of the cube indices: the device's threads keep no
+// order).  D = 3 (boost invariant) or 4.  Returns the element total, or -1
+// when some cube emits other than its count of elements.
+long long vhc_fo_emulate(int D, int nx, int ny, int nz, double dx, double dy, double dz, double tau0, double tau1,
+                         const double* t0, const double* t1, const double* u0, const double* u1, double t_fo,
+                         const long long* perm, double* out, long long cap) {
+  const vh_fo::Geo g = vh_fo::make_geo(nx, ny, nz, dx, dy, dz, tau0, tau1, t_fo, D == 3);
+  const long long nc = vh_fo::cubes(g, D);
+  std::vector<long long> counts(nc), offs(nc);
+  for (long long c = 0; c < nc; c++) {
+    int i, j, k;
+    vh_fo::cube_ijk(g, c, &i, &j, &k);
+    counts[c] = D == 3 ? vh_fo::count<3>(g, i, j, k, t0, t1) : vh_fo::count<4>(g, i, j, k, t0, t1);
+  }
+  long long total = 0;
+  for (long long c = 0; c < nc; c++) {
+    offs[c] = total;
+    total += counts[c];
+  }
+  for (long long q = 0; q < nc; q++) {
+    const long long c = perm[q];
+    if (counts[c] == 0) continue;
+    int i, j, k;
+    vh_fo::cube_ijk(g, c, &i, &j, &k);
+    vh_fo::Sink s{out, offs[c], cap};
+    if (D == 3) vh_fo::cube2(g, i, j, t0, t1, u0, u1, s);
+    else vh_fo::cube3(g, i, j, k, t0, t1, u0, u1, s);
+    if (s.at - offs[c] != counts[c]) return -1;
+  }
+  return total;
+}
+void vhc_bessel_k01e(double z, double* out2) { vh_fo::bessel_k01e(z, &out2[0], &out2[1]); }
+double vhc_cf2_term(const double* el, double mt, double px, double py, double t_fo) {
+  return vh_fo::cf2_term(el, mt, px, py, t_fo);
+}
+double vhc_cf3_term(const double* el, double mt, double px, double py, double y, double t_fo) {
+  return vh_fo::cf3_term(el, mt, px, py, y, t_fo);
+}
+void vhc_kuhn_simplex(int s, int m, int* v) { vh_fo::kuhn_simplex(s, m, v); }
 }

@@ -300,6 +300,82 @@ def freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, T0, T1, u0, u1, t_fo):
     return out[:cnt.value]
 
 
+def _cuda_f64(t, rows, n):
+    """rows x n float64 values of a CUDA tensor, contiguous (a copy only when
+    needed); rows = 0 for a flat array of n"""
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda):
+        raise TypeError("expected a CUDA tensor")
+    t = t.to(torch.float64).reshape(-1, n) if rows else t.to(torch.float64).reshape(-1)
+    if rows:
+        if t.shape[0] < rows:
+            raise ValueError(f"expected at least {rows} rows of {n}")
+        t = t[:rows]
+    elif t.numel() != n:
+        raise ValueError(f"expected {n} values")
+    return t.contiguous()
+
+
+def _stream(stream):
+    import torch
+    return torch.cuda.current_stream().cuda_stream if stream is None else stream
+
+
+def _surface_device(fn, width, rows, geo, n, T0, T1, u0, u1, t_fo, stream):
+    import torch
+    ts = [_cuda_f64(T0, 0, n), _cuda_f64(T1, 0, n), _cuda_f64(u0, rows, n), _cuda_f64(u1, rows, n)]
+    args = (*geo, *[t.data_ptr() for t in ts], t_fo)
+    cnt = ctypes.c_longlong()
+    st = _stream(stream)
+    rc = fn(*args, None, 0, ctypes.byref(cnt), st)  # counts the elements
+    if rc not in (A.OK, A.E_ARG) or cnt.value < 0:
+        A.check(rc)
+    out = torch.zeros((max(cnt.value, 1), width), dtype=torch.float64, device=ts[0].device)
+    A.check(fn(*args, out.data_ptr(), cnt.value, ctypes.byref(cnt), st))
+    return out[:cnt.value]
+
+
+def freezeout_2d_device(nx, ny, dx, dy, tau0, tau1, T0, T1, u0, u1, t_fo, stream=None):
+    """freezeout_2d on the GPU (vh_freezeout_2d_device): T0, T1 and u0, u1
+    (u^tau, u^x, u^y rows) as CUDA tensors on the ghost-inclusive grid; a
+    (count, 9) float64 CUDA tensor in freezeout_2d's element order"""
+    n = (nx + 6) * (ny + 6)
+    return _surface_device(A.lib().vh_freezeout_2d_device, 9, 3, (nx, ny, dx, dy, tau0, tau1), n, T0, T1, u0, u1,
+                           t_fo, stream)
+
+
+def freezeout_3d_device(nx, ny, nz, dx, dy, dz, tau0, tau1, T0, T1, u0, u1, t_fo, stream=None):
+    """freezeout_3d on the GPU (vh_freezeout_3d_device): a (count, 12)
+    float64 CUDA tensor in freezeout_3d's element order"""
+    n = (nx + 6) * (ny + 6) * (nz + 6)
+    return _surface_device(A.lib().vh_freezeout_3d_device, 12, 4, (nx, ny, nz, dx, dy, dz, tau0, tau1), n, T0, T1,
+                           u0, u1, t_fo, stream)
+
+
+def cooper_frye_2d_device(elements, t_fo, mass, degeneracy, pt, phi, stream=None):
+    """cooper_frye_2d from elements in a CUDA tensor (count, 9), summed on
+    the GPU (vh_cooper_frye_2d_device); a (len(pt), len(phi)) array"""
+    el = _cuda_f64(elements, 0, elements.numel())
+    pt = np.ascontiguousarray(pt, dtype=np.float64).reshape(-1)
+    phi = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
+    out = np.zeros((pt.size, phi.size))
+    A.check(A.lib().vh_cooper_frye_2d_device(el.data_ptr(), el.numel() // 9, t_fo, mass, degeneracy, A.ptr(pt),
+                                             pt.size, A.ptr(phi), phi.size, A.ptr(out), _stream(stream)))
+    return out
+
+
+def cooper_frye_3d_device(elements, t_fo, mass, degeneracy, y, pt, phi, stream=None):
+    """cooper_frye_3d from elements in a CUDA tensor (count, 12), summed on
+    the GPU (vh_cooper_frye_3d_device); a (len(pt), len(phi)) array"""
+    el = _cuda_f64(elements, 0, elements.numel())
+    pt = np.ascontiguousarray(pt, dtype=np.float64).reshape(-1)
+    phi = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
+    out = np.zeros((pt.size, phi.size))
+    A.check(A.lib().vh_cooper_frye_3d_device(el.data_ptr(), el.numel() // 12, t_fo, mass, degeneracy, y, A.ptr(pt),
+                                             pt.size, A.ptr(phi), phi.size, A.ptr(out), _stream(stream)))
+    return out
+
+
 def profile_gubser_cold(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, b=1.21, a=A_QGP):
     """the cold-plasma viscous Gubser flow at tau0: e, u^x, u^y, pi5 and prevu
     (at tau0 - dtau) on the 2+1D ghost-inclusive grid"""
