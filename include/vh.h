@@ -439,6 +439,20 @@ int vh_freezeout_2d_device(int nx, int ny, double dx, double dy, double tau0, do
 int vh_freezeout_3d_device(int nx, int ny, int nz, double dx, double dy, double dz, double tau0, double tau1,
                            const double* t0, const double* t1, const double* u0, const double* u1, double t_fo,
                            double* out, long long cap, long long* count, void* stream);
+/* The surface T = t_fo swept by the handle's state since the last call,
+ * on the GPU without host copies of the slices: T and u^mu of the current
+ * state against those this call kept from the previous one (at its tau),
+ * as vh_freezeout_2d_device (boost invariant) or vh_freezeout_3d_device
+ * write it into device memory out (cap elements of 9 or 12 doubles).  The
+ * first call after the state is set (vh_set_state, vh_init_profile,
+ * vh_init_tmunu, vh_load_checkpoint) only keeps the slice and returns
+ * *count = 0; a call between which no step ran returns VH_E_STATE.  When
+ * the surface has more than cap elements the call returns VH_E_ARG with
+ * *count set and keeps the previous slice, so that a call with a larger
+ * out gets the same surface.  Milne grids only (VH_E_UNSUPPORTED on
+ * Cartesian ones).  Call after each vh_step(h, 1) to follow the surface
+ * through a run. */
+int vh_freezeout_step(vh_handle* h, double t_fo, double* out, long long cap, long long* count);
 /* vh_cooper_frye_2d and vh_cooper_frye_3d on the GPU: elements in device
  * memory (count x 9 or 12 doubles), momentum bins pt, phi and the result
  * out (npt x nphi) on the host; one block per bin sums the elements in a

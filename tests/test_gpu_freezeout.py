@@ -103,3 +103,39 @@ def test_spectra_match_the_host():
         host3 = cooper_frye_3d(el3, 0.15, 0.7, 3.0, yy, pt, phi)
         got3 = cooper_frye_3d_device(dev(el3), 0.15, 0.7, 3.0, yy, pt, phi)
         assert np.allclose(got3, host3, rtol=1e-11, atol=0)
+
+
+def test_freezeout_step_follows_a_run():
+    """vh_freezeout_step during a viscous Gubser run: the surface between
+    consecutive steps from the handle's own slices equals the host surface
+    of the same slices read back with vh_get_primitive"""
+    from viral_b200 import configs as C
+    cfg = C.gubser_config(nx=33, ny=33)
+    with C.make_hydro(cfg, C.gubser_inputs(cfg)) as H:
+        p = H.get_primitive()
+        tfo = 0.85 * p["T"].max()
+        assert H.freezeout_step(tfo).shape == (0, 9)  # the first call keeps the slice
+        prev, total = (H.tau, p["T"], p["u"]), 0
+        for _ in range(6):
+            H.step(1)
+            got = H.freezeout_step(tfo)
+            q = H.get_primitive()
+            want = freezeout_2d(cfg.nx, cfg.ny, cfg.dx, cfg.dy, prev[0], H.tau, prev[1], q["T"], prev[2], q["u"], tfo)
+            same_elements(got, want)
+            total += len(want)
+            prev = (H.tau, q["T"], q["u"])
+        assert total > 50
+        with pytest.raises(A.VhError) as err:  # no step since the last slice
+            H.freezeout_step(tfo)
+        assert err.value.code == A.E_STATE
+
+        # too small an output: the count comes back and the slice is kept
+        H.step(1)
+        q = H.get_primitive()
+        want = freezeout_2d(cfg.nx, cfg.ny, cfg.dx, cfg.dy, prev[0], H.tau, prev[1], q["T"], prev[2], q["u"], tfo)
+        assert len(want) > 2
+        small = torch.zeros((2, 9), dtype=torch.float64, device="cuda")
+        cnt = ctypes.c_longlong()
+        assert A.lib().vh_freezeout_step(H.h, tfo, small.data_ptr(), 2, ctypes.byref(cnt)) == A.E_ARG
+        assert cnt.value == len(want)
+        same_elements(H.freezeout_step(tfo), want)

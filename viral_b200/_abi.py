@@ -129,6 +129,8 @@ SIGNATURES = [
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong,
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p]),
+    ("vh_freezeout_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong,
+                                         ctypes.POINTER(ctypes.c_longlong)]),
     ("vh_cooper_frye_2d_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_double, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp,
                                                 ctypes.c_void_p]),

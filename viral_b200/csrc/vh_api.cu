@@ -121,7 +121,7 @@ extern "C" int vh_destroy(vh_handle* h) {
   if (!h) return VH_OK;
   cudaFree(h->state); cudaFree(h->stage); cudaFree(h->eos_d); cudaFree(h->eos_f);
   cudaFree(h->status); cudaFree(h->iters); cudaFree(h->red); cudaFree(h->part);
-  cudaFree(h->adj_buf);
+  cudaFree(h->adj_buf); cudaFree(h->fo_prev);
   delete h;
   return VH_OK;
 }
@@ -164,6 +164,7 @@ extern "C" int vh_set_state_device(vh_handle* h, const double* dev, double tau) 
   if (r) return r;
   h->tau = tau;
   h->have_state = true;
+  h->fo_have = false;
   VH_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(unsigned int), h->stream));
   return VH_OK;
 }
@@ -326,6 +327,44 @@ extern "C" int vh_get_primitive(vh_handle* h, double* e, double* P, double* T, d
   return VH_OK;
 }
 
+extern "C" int vh_freezeout_step(vh_handle* h, double t_fo, double* out, long long cap, long long* count) {
+  if (!h || !count || cap < 0 || (cap > 0 && !out) || !(t_fo > 0)) return VH_E_ARG;
+  if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  const vh_config& c = h->cfg;
+  if (h->C.cart) return fail(h, VH_E_UNSUPPORTED, "freeze-out surfaces are built on Milne grids");
+  if (c.nx < 2 || c.ny < 2 || (!c.boost_invariant && c.nz < 2))
+    return fail(h, VH_E_ARG, "a freeze-out surface needs two cells along every axis");
+  const long long n = h->C.n;
+  const size_t nb = sizeof(double) * (size_t)n;
+  if (!h->fo_prev) VH_CUDA(h, cudaMalloc(&h->fo_prev, 5 * nb));
+  // T and u^mu of the current state: rows 2 (T) and 3..6 (u^mu) of the
+  // primitive fields, contiguous
+  double* buf = h->stage;
+  if (h->mixed) k_primitive<float><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pf, h->tau, buf);
+  else k_primitive<double><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pd, h->tau, buf);
+  VH_CUDA(h, cudaGetLastError());
+  const double* cur = buf + 2 * n;
+  *count = 0;
+  if (h->fo_have) {
+    if (!(h->tau > h->fo_tau)) return fail(h, VH_E_STATE, "no step since the last freeze-out slice");
+    const double* prev = h->fo_prev;
+    const int r = c.boost_invariant
+                      ? vh_freezeout_2d_device(c.nx, c.ny, c.dx, c.dy, h->fo_tau, h->tau, prev, cur, prev + n, cur + n,
+                                               t_fo, out, cap, count, h->stream)
+                      : vh_freezeout_3d_device(c.nx, c.ny, c.nz, c.dx, c.dy, c.dz, h->fo_tau, h->tau, prev, cur,
+                                               prev + n, cur + n, t_fo, out, cap, count, h->stream);
+    if (r == VH_E_ARG && *count > cap)
+      return fail(h, VH_E_ARG, "the surface has " + std::to_string(*count) + " elements, more than cap; the slice "
+                               "is kept for a call with room for them");
+    if (r) return fail(h, r, "freeze-out surface between two slices");
+  }
+  VH_CUDA(h, cudaMemcpyAsync(h->fo_prev, cur, 5 * nb, cudaMemcpyDeviceToDevice, h->stream));
+  VH_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->fo_tau = h->tau;
+  h->fo_have = true;
+  return VH_OK;
+}
+
 template <class R>
 static int ns_pi10(vh_handle* h, const DevPtrs<R>& P, double* out) {
   const DevCfg& C = h->C;
@@ -420,6 +459,7 @@ extern "C" int vh_init_tmunu(vh_handle* h, double tau, const double* tmunu10, lo
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
   h->tau = tau;
   h->have_state = true;
+  h->fo_have = false;
   if (nfail) *nfail = (long long)bad;
   if (bad) return fail(h, VH_E_ROOTFIND, "Landau matching found no timelike eigenvector in " + std::to_string(bad) +
                                              " cell(s)");

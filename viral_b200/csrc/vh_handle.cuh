@@ -38,6 +38,11 @@ struct vh_handle {
   void* adj_buf = nullptr;
   size_t adj_bytes = 0;
   double adj_ms[4] = {0, 0, 0, 0};
+  // the slice vh_freezeout_step saw last: T and u^mu (5 x n doubles) at
+  // fo_tau; forgotten whenever the state is set from outside
+  double* fo_prev = nullptr;
+  double fo_tau = 0;
+  bool fo_have = false;
   std::string err;
 };
 

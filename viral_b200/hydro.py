@@ -186,6 +186,23 @@ class Hydro:
         self._chk(A.lib().vh_cfl(self.h, ctypes.byref(a), ctypes.byref(d)))
         return a.value, d.value
 
+    def freezeout_step(self, t_fo: float):
+        """the surface T = t_fo swept since the last call, on the GPU
+        (vh_freezeout_step): a (count, 9) float64 CUDA tensor on
+        boost-invariant grids, (count, 12) in 3+1D; empty on the first call
+        after the state is set"""
+        import torch
+        width = 9 if self.cfg.boost_invariant else 12
+        cnt = ctypes.c_longlong()
+        rc = A.lib().vh_freezeout_step(self.h, t_fo, None, 0, ctypes.byref(cnt))  # counts (keeps the slice)
+        if rc == A.OK:
+            return torch.zeros((0, width), dtype=torch.float64, device="cuda")
+        if rc != A.E_ARG or cnt.value <= 0:
+            self._chk(rc)
+        out = torch.zeros((cnt.value, width), dtype=torch.float64, device="cuda")
+        self._chk(A.lib().vh_freezeout_step(self.h, t_fo, out.data_ptr(), cnt.value, ctypes.byref(cnt)))
+        return out[:cnt.value]
+
     def write(self, path: str, layout: int = A.WRITE_XY, every: int = 1):
         self._chk(A.lib().vh_write(self.h, path.encode(), layout, every))
 
