@@ -87,8 +87,10 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
     h->eos_host = t;
     if ((e = cudaMalloc(&h->eos_d, sizeof(double) * t.size())) != cudaSuccess) return bail(e, "eos table");
     if ((e = cudaMalloc(&h->eos_f, sizeof(float) * t.size())) != cudaSuccess) return bail(e, "eos table");
-    cudaMemcpy(h->eos_d, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(h->eos_f, tf.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice);
+    if ((e = cudaMemcpy(h->eos_d, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return bail(e, "eos table");
+    if ((e = cudaMemcpy(h->eos_f, tf.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return bail(e, "eos table");
     C.eos_n = n;
     C.eos_l0 = std::log(cfg->eos_e[0]);
     C.eos_idl = (n - 1) / (std::log(cfg->eos_e[n - 1]) - C.eos_l0);
@@ -104,8 +106,8 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
   if ((e = cudaMalloc(&h->red, sizeof(unsigned long long) * 4)) != cudaSuccess) return bail(e, "reduce");
   h->part_blocks = 296;
   if ((e = cudaMalloc(&h->part, sizeof(double) * 8 * h->part_blocks + 32)) != cudaSuccess) return bail(e, "reduce");
-  cudaMemset(h->status, 0, sizeof(unsigned int));
-  cudaMemset(h->iters, 0, sizeof(unsigned long long));
+  if ((e = cudaMemset(h->status, 0, sizeof(unsigned int))) != cudaSuccess) return bail(e, "status");
+  if ((e = cudaMemset(h->iters, 0, sizeof(unsigned long long))) != cudaSuccess) return bail(e, "iters");
   set_ptrs(h->pd, h->state, C.n, h->status, h->iters);
   set_ptrs(h->pf, h->state, C.n, h->status, h->iters);
   if ((h->mixed ? set_smem_attrs<float>(h) : set_smem_attrs<double>(h)) != VH_OK) {

@@ -345,15 +345,21 @@ extern "C" int vh_batch_create(const vh_config* cfg, int n_events, const int* nx
     vh_batch_destroy(b);
     return VH_E_CUDA;
   };
+  // a CUDA call's success, recording its error for fail()
+  auto ok = [&](cudaError_t ce) {
+    if (ce != cudaSuccess) b->err = cudaGetErrorString(ce);
+    return ce == cudaSuccess;
+  };
   if (cfg->eos_kind == VH_EOS_TABLE) {
     const int m = cfg->eos_n;
     std::vector<double> t(4 * (size_t)m);
     std::vector<float> tf(4 * (size_t)m);
     for (int i = 0; i < m; i++) { t[i] = cfg->eos_e[i]; t[m + i] = cfg->eos_p[i]; t[2 * m + i] = cfg->eos_cs2[i]; t[3 * m + i] = cfg->eos_t[i]; }
     for (size_t i = 0; i < t.size(); i++) tf[i] = (float)t[i];
-    if (cudaMalloc(&b->eos_d, sizeof(double) * t.size()) || cudaMalloc(&b->eos_f, sizeof(float) * t.size())) return fail("eos");
-    cudaMemcpy(b->eos_d, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(b->eos_f, tf.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice);
+    if (!ok(cudaMalloc(&b->eos_d, sizeof(double) * t.size())) || !ok(cudaMalloc(&b->eos_f, sizeof(float) * t.size())) ||
+        !ok(cudaMemcpy(b->eos_d, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice)) ||
+        !ok(cudaMemcpy(b->eos_f, tf.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice)))
+      return fail("eos");
     C.eos_n = m; C.eos_l0 = std::log(cfg->eos_e[0]); C.eos_idl = (m - 1) / (std::log(cfg->eos_e[m - 1]) - C.eos_l0);
     C.eos_d = b->eos_d; C.eos_f = b->eos_f;
   }
@@ -361,22 +367,23 @@ extern "C" int vh_batch_create(const vh_config* cfg, int n_events, const int* nx
   const size_t pool_bytes = (size_t)52 * tot * b->esz;
   cudaError_t ce = cudaMalloc(&b->pool, pool_bytes);
   if (ce != cudaSuccess) { b->err = cudaGetErrorString(ce); g_batch_err = "vh_batch_create: pool: " + b->err; vh_batch_destroy(b); return VH_E_NOMEM; }
-  cudaMemset(b->pool, 0, pool_bytes);
+  if (!ok(cudaMemset(b->pool, 0, pool_bytes))) return fail("pool");
   const int n = n_events;
-  if (cudaMalloc(&b->d_off, sizeof(long long) * n) || cudaMalloc(&b->d_nx, sizeof(int) * n) ||
-      cudaMalloc(&b->d_ny, sizeof(int) * n) || cudaMalloc(&b->d_state, sizeof(int) * n) ||
-      cudaMalloc(&b->d_steps, sizeof(int) * n) || cudaMalloc(&b->d_running, sizeof(int)) ||
-      cudaMalloc(&b->d_tau, sizeof(double) * n) || cudaMalloc(&b->d_dtau, sizeof(double) * n) ||
-      cudaMalloc(&b->d_taumax, sizeof(double) * n) || cudaMalloc(&b->d_tmax, sizeof(unsigned long long) * n) ||
-      cudaMalloc(&b->d_iters, sizeof(unsigned long long)) || cudaMalloc(&b->d_flag, sizeof(unsigned int) * n) ||
-      cudaMalloc(&b->d_bar, sizeof(unsigned int) * 4) ||
-      cudaMalloc(&b->stage, sizeof(double) * 18 * big))
+  if (!ok(cudaMalloc(&b->d_off, sizeof(long long) * n)) || !ok(cudaMalloc(&b->d_nx, sizeof(int) * n)) ||
+      !ok(cudaMalloc(&b->d_ny, sizeof(int) * n)) || !ok(cudaMalloc(&b->d_state, sizeof(int) * n)) ||
+      !ok(cudaMalloc(&b->d_steps, sizeof(int) * n)) || !ok(cudaMalloc(&b->d_running, sizeof(int))) ||
+      !ok(cudaMalloc(&b->d_tau, sizeof(double) * n)) || !ok(cudaMalloc(&b->d_dtau, sizeof(double) * n)) ||
+      !ok(cudaMalloc(&b->d_taumax, sizeof(double) * n)) ||
+      !ok(cudaMalloc(&b->d_tmax, sizeof(unsigned long long) * n)) ||
+      !ok(cudaMalloc(&b->d_iters, sizeof(unsigned long long))) || !ok(cudaMalloc(&b->d_flag, sizeof(unsigned int) * n)) ||
+      !ok(cudaMalloc(&b->d_bar, sizeof(unsigned int) * 4)) || !ok(cudaMalloc(&b->stage, sizeof(double) * 18 * big)))
     return fail("tables");
-  cudaMemcpy(b->d_off, b->off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_nx, b->nx.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_ny, b->ny.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_dtau, b->dtau.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_taumax, b->tau_max.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (!ok(cudaMemcpy(b->d_off, b->off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice)) ||
+      !ok(cudaMemcpy(b->d_nx, b->nx.data(), sizeof(int) * n, cudaMemcpyHostToDevice)) ||
+      !ok(cudaMemcpy(b->d_ny, b->ny.data(), sizeof(int) * n, cudaMemcpyHostToDevice)) ||
+      !ok(cudaMemcpy(b->d_dtau, b->dtau.data(), sizeof(double) * n, cudaMemcpyHostToDevice)) ||
+      !ok(cudaMemcpy(b->d_taumax, b->tau_max.data(), sizeof(double) * n, cudaMemcpyHostToDevice)))
+    return fail("tables");
   b->t_freeze_gev = t_freeze_gev;
   if (vh_batch_reset(b) != VH_OK) return fail("reset");
   if (build_items(b) != VH_OK) return fail("items");

@@ -138,8 +138,8 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
   FILE* fp = std::fopen(path, "wb");
   if (!fp) return VH_E_ARG;
   const size_t w = std::fwrite(file.data(), 1, file.size(), fp);
-  std::fclose(fp);
-  return w == file.size() ? VH_OK : VH_E_ARG;
+  const bool closed = std::fclose(fp) == 0;  // a delayed write error shows here
+  return w == file.size() && closed ? VH_OK : VH_E_ARG;
 }
 
 // NEWideal/init.h:296-345: interior values read row by row (x fastest),
