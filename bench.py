@@ -16,7 +16,10 @@ and the time the max over ranks.
 
 --impl reference times the reference's own CPU step (its NEWEST5 headers
 built in oracle/_ref, TVDRK2 on a 40x40x10 Milne grid, the compile-time grid
-of its default scenario block) in one process per host core.
+of its default scenario block) in one process per host core.  --ensemble N
+reports events/s of a batched ensemble; its cpu_baseline is the reference's
+boost-invariant step on the host cores, extrapolated to the ensemble's cell
+updates.
 """
 from __future__ import annotations
 
@@ -71,18 +74,25 @@ def parse():
 
 
 def _ref_worker(args):
-    """One process: the reference's TVDRK2 on its compile-time 3+1D grid for
+    """One process: the reference's TVDRK2 on the compile-time grid of a
+    build (milne_3d: 40x40x10 cells; milne_lbi: 40x40 boost invariant) for
     about `seconds` seconds; returns (interior cells x steps, seconds)."""
-    seconds, seed = args
+    seconds, seed, variant = (*args, "milne_3d")[:3]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
-    from pyoracle import Oracle, OracleConfig, RefBuild, smooth_state
-    R = RefBuild("milne_3d")
+    from pyoracle import F_PI, F_PU, F_U, Oracle, OracleConfig, RefBuild, smooth_state
+    R = RefBuild(variant)
     x, y, z = R.coords()
     tau, ts = 0.6, 0.02
     f = smooth_state(x, y, z, tau, ts, seed=seed)
-    O = Oracle(OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=R.gz - 6, boost_invariant=False, dx=R.dx, dy=R.dy,
-                            dz=R.dz, eos_kind=0, eos_a=R.factor, etas0=1 / (4 * math.pi), hbarc=R.gevfm))
+    if R.boost_invariant:  # no eta flow and no eta components of pi
+        for q in (F_U + 3, F_PI + 3, F_PI + 4, F_PU + 3):
+            f[q] = 0.0
+        for q in (F_U, F_PU):
+            f[q] = np.sqrt(1 + f[q + 1] ** 2 + f[q + 2] ** 2)
+    O = Oracle(OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=1 if R.boost_invariant else R.gz - 6,
+                            boost_invariant=R.boost_invariant, dx=R.dx, dy=R.dy, dz=R.dz, eos_kind=0,
+                            eos_a=R.factor, etas0=1 / (4 * math.pi), hbarc=R.gevfm))
     O.set_state(f)
     O.fill_tmunu(tau)
     R.set_state(O.get_state())
@@ -100,10 +110,10 @@ def _ref_worker(args):
     return cells * n, dt
 
 
-def cpu_reference(seconds: float, procs: int):
+def cpu_reference(seconds: float, procs: int, variant: str = "milne_3d"):
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(seconds, s) for s in range(procs)])
+        res = pool.map(_ref_worker, [(seconds, s, variant) for s in range(procs)])
     rate = sum(c / t for c, t in res)
     return rate, procs
 
@@ -487,11 +497,30 @@ def ensemble(args):
            "loop_fp64": {"events_per_s": n / loop_seconds, "seconds_per_event_by_side": per_side,
                          "sample": f"{args.loop_per_side} events per side, extrapolated by the side counts"},
            "speedup_vs_loop_fp64": loop_seconds / sec, "clocks": clk.summary(),
+           "cpu_baseline": ensemble_cpu_baseline(args.cpu_seconds, float(np.sum(cells * nst)), n),
            "config": {"workload": "glauber ensemble", "sides": [64, 96, 128, 160, 200], "dx_fm": 0.1,
                       "b_fm": [0, 12], "dtau_fm": dtau, "tau0_fm": tau0, "tau_max_fm": tau_max,
                       "t_freeze_gev": t_fo, "floor_gev_fm3": floor,
                       "precision": f"{args.ensemble_precision} (batch) / fp64 (loop)"}}
     print(json.dumps(out), flush=True)
+
+
+def ensemble_cpu_baseline(seconds: float, cell_steps: float, n_events: int) -> dict | None:
+    """events/s of the reference's CPU step on the host cores for an ensemble
+    of n_events that takes cell_steps interior cell updates in all: the
+    reference's 2+1D TVDRK2 (its boost-invariant build, 40x40 cells) timed in
+    one process per core for `seconds`, its aggregate cell-updates/s taken as
+    the rate of the ensemble's events (the step's cost per cell does not
+    depend on the grid side)"""
+    if seconds <= 0:
+        return None
+    procs = reference_procs()
+    rate, cores = cpu_reference(seconds, procs, "milne_lbi")
+    return {"value": n_events * rate / cell_steps, "unit": "events/s", "cores": cores, "kind": "reference",
+            "cell_updates_per_s": rate,
+            "sample": f"{cores} processes x reference TVDRK2 (NEWEST5 headers, boost invariant, 1 MPI rank each) on "
+                      f"40x40 cells for {seconds:.0f} s, extrapolated to the ensemble's {cell_steps:.4g} cell "
+                      f"updates; {cpu_model()}"}
 
 
 def adjoint_ratio(args):
