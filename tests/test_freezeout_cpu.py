@@ -210,3 +210,32 @@ def test_cooper_frye_3d_reduces_to_the_boost_invariant_result():
     mt = np.sqrt(m * m + pt * pt)
     want = g * A_tau * 2 * mt * special.k1(mt / tfo) / (2 * np.pi) ** 3
     assert np.allclose(sp, want[:, None], rtol=1e-10)
+
+
+def test_flow_coefficients_of_spectra():
+    """v_n and the event-plane angles of a spectrum with known harmonics, and
+    the elliptic flow of an elliptic fireball's spectrum: positive, rising
+    with p_T, its plane along the short axis (x)"""
+    from viral_b200.hydro import cooper_frye_2d, flow_coefficients
+    phi = np.arange(16) * 2 * np.pi / 16
+    pt = np.array([0.5, 1.0])
+    amp = np.array([[1.0], [0.3]])
+    S = amp * (1 + 2 * 0.1 * np.cos(2 * (phi - 0.3)) + 2 * 0.05 * np.cos(3 * (phi + 0.2)))[None, :]
+    v, psi = flow_coefficients(S, phi, orders=(1, 2, 3))
+    assert np.allclose(v[0], 0, atol=1e-15) and np.allclose(v[1], 0.1) and np.allclose(v[2], 0.05)
+    assert np.allclose(psi[1], 0.3) and np.allclose(psi[2], -0.2)
+    with pytest.raises(ValueError):
+        flow_coefficients(S, phi[:-1])
+
+    # an elliptic fireball expanding faster along x (its short axis)
+    nx = ny = 61
+    d = 0.1
+    x, y = grid(nx, ny, d, d)
+    T = 0.3 * np.exp(-(x * x / 1.0 + y * y / 2.0) / 2)
+    u = np.stack([np.sqrt(1 + (0.6 * x) ** 2 + (0.3 * y) ** 2), 0.6 * x, 0.3 * y])
+    el = freezeout_2d(nx, ny, d, d, 1.0, 1.05, T, 0.97 * T, u, u, 0.15)
+    pts = np.array([0.5, 1.0, 2.0])
+    v, psi = flow_coefficients(cooper_frye_2d(el, 0.15, 0.14, 1.0, pts, phi), phi, orders=(2,))
+    assert np.all(v[0] > 0) and np.all(np.diff(v[0]) > 0)
+    # the tetrahedra's diagonal breaks the x -> -x mirror symmetry slightly
+    assert np.allclose(psi[0], 0.0, atol=2e-3)

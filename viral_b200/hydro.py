@@ -317,6 +317,23 @@ def freezeout_3d(nx, ny, nz, dx, dy, dz, tau0, tau1, T0, T1, u0, u1, t_fo):
     return out[:cnt.value]
 
 
+def flow_coefficients(spectrum, phi, orders=(1, 2, 3, 4)):
+    """anisotropic flow of spectra (len(pt), len(phi)) on a uniform azimuth
+    grid over [0, 2 pi): v_n(p_T) = |sum_b S e^{i n phi_b}| / sum_b S and the
+    event-plane angle Psi_n = arg(sum_b S e^{i n phi_b}) / n, for each order
+    (exact for harmonics below len(phi) / 2); returns v, psi of shape
+    (len(orders), len(pt))"""
+    S = np.asarray(spectrum, dtype=np.float64)
+    phi = np.asarray(phi, dtype=np.float64).reshape(-1)
+    if S.ndim != 2 or S.shape[1] != phi.size:
+        raise ValueError("spectrum must be (len(pt), len(phi))")
+    step = 2 * np.pi / phi.size
+    if not np.allclose(np.diff(phi), step, rtol=0, atol=1e-12 * step):
+        raise ValueError("phi must be a uniform grid over [0, 2 pi)")
+    q = np.array([(S * np.exp(1j * n * phi)[None, :]).sum(axis=1) for n in orders]) / S.sum(axis=1)[None, :]
+    return np.abs(q), np.angle(q) / np.asarray(orders, dtype=np.float64)[:, None]
+
+
 def _cuda_f64(t, rows, n):
     """rows x n float64 values of a CUDA tensor, contiguous (a copy only when
     needed); rows = 0 for a flat array of n"""
