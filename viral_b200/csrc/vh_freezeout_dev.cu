@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(kThreads) k_cooper_frye(const double* __restri
                                                            const double* __restrict__ bins, double y, double t_fo,
                                                            double pref, double* __restrict__ out) {
   __shared__ double red[kThreads];
-  const int b = blockIdx.x;
+  const long long b = blockIdx.x;
   const double mt = bins[3 * b], px = bins[3 * b + 1], py = bins[3 * b + 2];
   double s = 0;
   for (long long e = threadIdx.x; e < count; e += kThreads)
