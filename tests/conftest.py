@@ -12,6 +12,8 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libvh.so")
+    config.addinivalue_line("markers", "late: runs after every other test, so that a failure there (under -x) "
+                                       "leaves the rest already run; for GPU paths not yet run on hardware")
 
 
 def _ensure_oracle():
@@ -42,6 +44,7 @@ def gpu_available() -> bool:
 
 
 def pytest_collection_modifyitems(config, items):
+    items.sort(key=lambda it: 1 if "late" in it.keywords else 0)  # stable: file order otherwise
     if gpu_available():
         return
     skip = pytest.mark.skip(reason="no CUDA GPU in this environment")

@@ -2,7 +2,8 @@
 (vh_freezeout_{2d,3d}_device, vh_cooper_frye_{2d,3d}_device) against the
 host functions on the same slices: the same element count and order, the
 values to rounding (the device contracts products into FMAs), the capacity
-contract, and the spectra summed per bin on the device."""
+contract, and the spectra summed per bin on the device.  Marked late: these
+device paths are newer than the rest of the GPU suite."""
 import ctypes
 
 import numpy as np
@@ -15,7 +16,7 @@ from viral_b200 import _abi as A
 from viral_b200.hydro import (cooper_frye_2d, cooper_frye_2d_device, cooper_frye_3d, cooper_frye_3d_device,
                               freezeout_2d, freezeout_2d_device, freezeout_3d, freezeout_3d_device)
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late]
 
 
 def dev(a):
