@@ -180,6 +180,39 @@ def make_bjorken() -> dict:
             "temp": np.array(temps), "final": R.get_state()[:, centre]}
 
 
+CART_BJORKEN_STEPS = 100
+
+
+def make_cart_bjorken() -> dict:
+    """The reference's Cartesian Bjorken block (TXYZ5/maindef.h:78-108,
+    init.h:221-283): e = 30 GeV/fm^3 at rest on its 10 x 10 x 41 grid of
+    0.1 fm from t = 0.6, CART_BJORKEN_STEPS steps of 0.01.  In (t, x, y, z) a
+    uniform fluid at rest is an equilibrium: the record is the final state of
+    the centre cell and the largest change of any field anywhere."""
+    R = RefBuild("cart_bjorken")
+    cfg = OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=R.gz - 6, boost_invariant=False, cartesian=True, dx=R.dx,
+                       dy=R.dy, dz=R.dz, eos_kind=0, eos_a=R.factor, etas0=0.2, etas1=0.0, hbarc=R.gevfm,
+                       taupi_kind=2, taupi_const=0.01)
+    f = np.zeros((18, R.n))
+    f[0] = 30.0 / R.gevfm
+    f[1] = 1.0
+    f[14] = 1.0
+    O = Oracle(cfg)
+    O.set_state(f)
+    O.fill_tmunu(0.6)
+    f = O.get_state()
+    R.set_state(f)
+    t = 0.6
+    for _ in range(CART_BJORKEN_STEPS):
+        R.step(t, 0.01)
+        t += 0.01
+    s = R.get_state()
+    centre = ((R.gz // 2) * R.gy + R.gy // 2) * R.gx + R.gx // 2
+    return {"t0": 0.6, "ts": 0.01, "steps": CART_BJORKEN_STEPS, "centre": centre,
+            "dims": np.array([R.gx, R.gy, R.gz, 0]), "consts": np.array([R.dx, R.dy, R.dz, R.factor, R.gevfm]),
+            "initial": f[:, centre], "final": s[:, centre], "max_change": np.abs(s - f).max(axis=1)}
+
+
 CGC_SAMPLE = 1000
 
 
@@ -228,7 +261,8 @@ def make_ns10() -> dict:
 
 
 def main():
-    special = {"cart_3d_shock": make_shock, "ns10_lbi": make_ns10, "bjorken": make_bjorken, "cgc": make_cgc}
+    special = {"cart_3d_shock": make_shock, "ns10_lbi": make_ns10, "bjorken": make_bjorken, "cgc": make_cgc,
+               "cart_bjorken": make_cart_bjorken}
     which = sys.argv[1:] or list(SCENARIOS) + list(special)
     for v in which:
         d = special[v]() if v in special else make(v)

@@ -243,6 +243,29 @@ def test_bjorken_scenario_matches_reference(precision):
         assert np.max(np.abs(final - g["final"])) <= 1e-12 * np.max(np.abs(g["final"]))
 
 
+@pytest.mark.late
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_cartesian_bjorken_block_stays_at_rest(precision):
+    """The reference's Cartesian Bjorken block (TXYZ5, 10x10x41, 100 steps
+    from t = 0.6; tests/golden/ref_cart_bjorken.npz): the compiled reference
+    keeps the uniform fluid at rest bitwise.  FP64 to 1e-12 (the root-find
+    may move e by an ulp per stage), the mixed mode to its FP32 state
+    (1e-6) (late: newer than the rest of this file)"""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_cart_bjorken.npz"))
+    cfg = C.cart_bjorken_config(precision=precision)
+    assert cfg.gdims() == tuple(int(v) for v in g["dims"][:3])
+    with C.make_hydro(cfg, C.cart_bjorken_inputs(cfg)) as H:
+        start = H.get_state()
+        H.step(int(g["steps"]))
+        end = H.get_state()
+        assert H.tau == pytest.approx(float(g["t0"]) + int(g["steps"]) * float(g["ts"]), abs=1e-12)
+    tol = 1e-12 if precision == A.PREC_FP64 else 1e-6
+    scale = np.abs(g["final"]).max()
+    assert np.abs(end[:, int(g["centre"])] - g["final"]).max() <= tol * scale
+    assert np.abs(end[:14] - start[:14]).max() <= tol * scale
+
+
 @pytest.mark.parametrize("cfgkw", [dict(), dict(coords=A.COORD_CARTESIAN, tau0=1.0)])
 def test_get_conserved(cfgkw):
     """the reference's Var: tau T^{tau mu} (T^{t mu} in Cartesian), pi, 0"""

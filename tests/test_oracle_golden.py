@@ -198,3 +198,30 @@ def test_bjorken_scenario():
     first_order = T0 * (t0 / taus) ** (1 / 3) * (1 + 2 * 0.2 * (1 - (t0 / taus) ** (2 / 3)) / (3 * t0 * T0))
     assert np.max(np.abs(temps / first_order - 1)) <= 2e-3
     assert temps[-1] / (T0 * (t0 / taus[-1]) ** (1 / 3)) - 1 > 0.09
+
+
+def test_cartesian_bjorken_block():
+    """The reference's Cartesian Bjorken block (TXYZ5, -DBJORKEN): a uniform
+    fluid at rest in (t, x, y, z) is an equilibrium, and the compiled
+    reference keeps it bitwise for 100 steps; so does the oracle"""
+    g = np.load(os.path.join(GOLD, "ref_cart_bjorken.npz"))
+    gx, gy, gz, _ = (int(v) for v in g["dims"])
+    dx, dy, dz, factor, gevfm = (float(v) for v in g["consts"])
+    cfg = OracleConfig(nx=gx - 6, ny=gy - 6, nz=gz - 6, boost_invariant=False, cartesian=True, dx=dx, dy=dy, dz=dz,
+                       eos_kind=0, eos_a=factor, etas0=0.2, etas1=0.0, hbarc=gevfm, taupi_kind=2, taupi_const=0.01)
+    f = np.zeros((18, gx * gy * gz))
+    f[0] = 30.0 / gevfm
+    f[1] = 1.0
+    f[14] = 1.0
+    O = Oracle(cfg)
+    O.set_state(f)
+    O.fill_tmunu(float(g["t0"]))
+    f = O.get_state()
+    assert np.array_equal(f[:, int(g["centre"])], g["initial"])
+    t = float(g["t0"])
+    for _ in range(int(g["steps"])):
+        assert O.step(t, float(g["ts"])) == 0
+        t += float(g["ts"])
+    s = O.get_state()
+    assert np.all(g["max_change"] == 0) and np.array_equal(s, f)
+    assert np.array_equal(s[:, int(g["centre"])], g["final"])

@@ -12,6 +12,9 @@ glauber_161x161x41 3+1D Milne event: 161x161x41, dx = dy = 0.1 fm,
 bjorken           the reference's Bjorken block: a uniform fluid at rest in
                   Milne coordinates, 10x10 cells, e = 30 GeV/fm^3 at 0.6 fm/c,
                   eta = 0.2 s, tau_pi = 0.01 fm/c (bjorken_config/_inputs).
+cart_bjorken      the reference's Cartesian Bjorken block: the same fluid at
+                  rest in (t, x, y, z), 10x10x41 cells of 0.1 fm from
+                  t = 0.6 (cart_bjorken_config/_inputs), an equilibrium.
 The reference's cold-plasma Gubser test and its Glasma initial state come
 from the generators in hydro.py (profile_gubser_cold, profile_cgc).
 """
@@ -46,6 +49,24 @@ def bjorken_config(nx=10, ny=10, precision=A.PREC_FP64) -> Config:
     return Config(nx=nx, ny=ny, nz=1, boost_invariant=True, precision=precision, dx=0.1, dy=0.1, tau0=0.6,
                   dtau=0.01, eos_kind=A.EOS_CONFORMAL, eos_a=BJORKEN_A, etas0=0.2, etas1=0.0,
                   hbarc=BJORKEN_GEVFM, taupi_kind=A.TAUPI_CONST, taupi_const=0.01)
+
+
+def cart_bjorken_config(precision=A.PREC_FP64) -> Config:
+    """The reference's Cartesian Bjorken block (TXYZ5/maindef.h:78-108): 10x10x41
+    cells of 0.1 fm, t0 = 0.6, dt = 0.01, the Milne block's EOS and transport."""
+    return Config(nx=10, ny=10, nz=41, boost_invariant=False, coords=A.COORD_CARTESIAN, precision=precision, dx=0.1,
+                  dy=0.1, dz=0.1, tau0=0.6, dtau=0.01, eos_kind=A.EOS_CONFORMAL, eos_a=BJORKEN_A, etas0=0.2,
+                  etas1=0.0, hbarc=BJORKEN_GEVFM, taupi_kind=A.TAUPI_CONST, taupi_const=0.01)
+
+
+def cart_bjorken_inputs(cfg: Config):
+    """TXYZ5/init.h:221-283: e = 30 GeV/fm^3 at rest on every cell, prevu = u,
+    pi = 0"""
+    gx, gy, gz = cfg.gdims()
+    n = gx * gy * gz
+    z = np.zeros(n)
+    return dict(tau=cfg.tau0, e=np.full(n, BJORKEN_E0), ux=z, uy=z.copy(), ueta=z.copy(), prevu=None,
+                pi_mode=A.PI_ZERO)
 
 
 def bjorken_inputs(cfg: Config):
