@@ -34,7 +34,7 @@ GROUPS = [(0,), (1, 2, 3, 4), (5, 6, 7, 8, 9), (10, 11, 12, 13), (14, 15, 16, 17
 
 def compare_states(a, b, tol, fields=range(14), mask=None):
     """Max |a-b| of each field over the largest |b| of its tensor group
-    (a component that stays near zero is judged on the scale of its tensor)."""
+    (a component that stays near zero is compared on the scale of its tensor)."""
     errs = {}
     for grp in GROUPS:
         scale = max(float(np.max(np.abs(b[q] if mask is None else b[q][mask]))) for q in grp)
