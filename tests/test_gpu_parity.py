@@ -266,6 +266,36 @@ def test_cartesian_bjorken_block_stays_at_rest(precision):
     assert np.abs(end[:14] - start[:14]).max() <= tol * scale
 
 
+@pytest.mark.late
+def test_bench_workload_matches_oracle():
+    """The benchmarked workload itself (bench.py's glauber_161x161x41: the
+    3+1D MC-Glauber event, 1,062,761 interior cells, FP64): two steps of the
+    GPU step against two oracle steps (about 10 s each on the host), every
+    field on the whole ghost-inclusive grid; and the mixed mode's two steps
+    against the FP64 ones (late: newer than the rest of this file)"""
+    import bench
+    cfg, inp, _ = bench.build_workload("glauber_161x161x41", "fp64")
+    O = oracle_from_inputs(cfg, inp)
+    with C.make_hydro(cfg, inp) as H:
+        compare_states(H.get_state(), O.get_state(), STAGE_TOL, fields=range(18))
+        tau = cfg.tau0
+        for _ in range(2):
+            assert O.step(tau, cfg.dtau) == 0
+            tau += cfg.dtau
+        H.step(2)
+        s64 = H.get_state()
+    worst = compare_states(s64, O.get_state(), RUN_TOL, fields=range(18))
+    print("161x161x41, 2 steps: max group-relative error against the oracle %.2e" % worst)
+    cfg32, inp32, _ = bench.build_workload("glauber_161x161x41", "mixed")
+    with C.make_hydro(cfg32, inp32) as H:
+        H.step(2)
+        s32 = H.get_state()
+    m = interior_mask(cfg)
+    assert rel_err(s32[0][m], s64[0][m]) < 1e-5
+    for q in (1, 2, 3, 4):
+        assert rel_err(s32[q][m], s64[q][m]) < 1e-4
+
+
 @pytest.mark.parametrize("cfgkw", [dict(), dict(coords=A.COORD_CARTESIAN, tau0=1.0)])
 def test_get_conserved(cfgkw):
     """the reference's Var: tau T^{tau mu} (T^{t mu} in Cartesian), pi, 0"""
