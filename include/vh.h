@@ -407,7 +407,9 @@ int vh_freezeout_2d(int nx, int ny, double dx, double dy, double tau0, double ta
                     long long* count);
 /* Boltzmann Cooper-Frye spectrum E dN/d^3p at mid-rapidity from count
  * elements of vh_freezeout_2d (boost invariant, u^eta = 0; the rapidity
- * integral done with K0, K1): out[a * nphi + b] at p_T = pt[a], azimuth
+ * integral done with e^a K0(a), e^a K1(a) by the trapezoidal rule on their
+ * integral representation, relative error within 4e-15, so that no factor
+ * overflows at large p_T): out[a * nphi + b] at p_T = pt[a], azimuth
  * phi[b], for a hadron of mass and degeneracy at the surface temperature
  * t_fo (mass, momenta and t_fo in the same unit, e.g. fm^-1).  Host code. */
 int vh_cooper_frye_2d(const double* elements, long long count, double t_fo, double mass, double degeneracy,
@@ -456,9 +458,7 @@ int vh_freezeout_step(vh_handle* h, double t_fo, double* out, long long cap, lon
 /* vh_cooper_frye_2d and vh_cooper_frye_3d on the GPU: elements in device
  * memory (count x 9 or 12 doubles), momentum bins pt, phi and the result
  * out (npt x nphi) on the host; one block per bin sums the elements in a
- * fixed order.  The 2+1D form evaluates K0 and K1 by the trapezoidal rule
- * on their integral representation (relative error within 4e-15).
- * Synchronises stream before returning. */
+ * fixed order.  Synchronises stream before returning. */
 int vh_cooper_frye_2d_device(const double* elements, long long count, double t_fo, double mass, double degeneracy,
                              const double* pt, int npt, const double* phi, int nphi, double* out, void* stream);
 int vh_cooper_frye_3d_device(const double* elements, long long count, double t_fo, double mass, double degeneracy,

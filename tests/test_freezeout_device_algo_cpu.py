@@ -133,23 +133,35 @@ def test_quadrature_bessel_functions(L):
     assert np.abs(got[:, 1] / special.k1e(z) - 1).max() <= 5e-15
 
 
-def test_quadrature_spectrum_matches_the_host_spectrum(L):
-    """the device's term (scaled quadrature K0, K1) summed here against the
-    host function (std::cyl_bessel_k)"""
+def test_spectrum_against_scipy_bessel_functions():
+    """the boost-invariant spectrum (quadrature K0, K1 in scaled form) against
+    the same sum written here with SciPy's K0, K1"""
     nx, ny, dx, dy = 31, 31, 0.2, 0.2
     T0, T1, u0, u1 = fields_2d(nx, ny, dx, dy, 7)
     el = freezeout_2d(nx, ny, dx, dy, 1.0, 1.1, np.abs(T0), np.abs(T1), u0, u1, 0.15)
     tfo, m, g = 0.15, 0.7, 3.0
     pt, phi = np.array([0.0, 0.3, 1.0, 2.5]), np.array([0.0, 0.7, 2.0])
-    host = cooper_frye_2d(el, tfo, m, g, pt, phi)
-    rows = np.ascontiguousarray(el)
-    mine = np.zeros_like(host)
+    got = cooper_frye_2d(el, tfo, m, g, pt, phi)
+    want = np.zeros_like(got)
     for a, p in enumerate(pt):
+        mt = np.sqrt(m * m + p * p)
+        arg = mt * el[:, 6] / tfo
         for b, f in enumerate(phi):
-            mt = np.sqrt(m * m + p * p)
-            mine[a, b] = g / (8 * np.pi ** 3) * sum(
-                L.vhc_cf2_term(ptr(rows[e]), mt, p * np.cos(f), p * np.sin(f), tfo) for e in range(len(rows)))
-    assert np.allclose(mine, host, rtol=1e-13, atol=0)
+            px, py = p * np.cos(f), p * np.sin(f)
+            terms = (2 * mt * special.k1(arg) * el[:, 3] + 2 * special.k0(arg) * (px * el[:, 4] + py * el[:, 5])) \
+                * np.exp((px * el[:, 7] + py * el[:, 8]) / tfo)
+            want[a, b] = g / (8 * np.pi ** 3) * terms.sum()
+    assert np.allclose(got, want, rtol=1e-13, atol=0)
+
+
+def test_spectrum_stays_finite_at_large_momentum():
+    """p_T u_perp / T far above the exponent range of a double: the scaled
+    Bessel functions keep the term finite (the product K1(a) e^b would be
+    0 times infinity)"""
+    el = np.zeros((1, 9))
+    el[0, 3], el[0, 6], el[0, 7] = 1.0, np.sqrt(1 + 4.0), 2.0  # u^x = 2
+    sp = cooper_frye_2d(el, 0.15, 0.14, 1.0, [60.0, 120.0], [0.0])
+    assert np.all(np.isfinite(sp)) and np.all(sp > 0)
 
 
 def test_device_entry_points_check_arguments_first():

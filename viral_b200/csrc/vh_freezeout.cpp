@@ -46,7 +46,9 @@ extern "C" int vh_freezeout_3d(int nx, int ny, int nz, double dx, double dy, dou
 // gives Bessel functions, int deta cosh(eta) e^{-a cosh eta} = 2 K1(a) and
 // int deta e^{-a cosh eta} = 2 K0(a):
 //   E dN/d^3p = g / (2 pi)^3 sum [2 m_T K1(a) dSigma_tau + 2 K0(a) (p_x dSigma_x
-//               + p_y dSigma_y)] exp((p_x u^x + p_y u^y) / T),  a = m_T u^tau / T.
+//               + p_y dSigma_y)] exp((p_x u^x + p_y u^y) / T),  a = m_T u^tau / T,
+// with e^a K0(a), e^a K1(a) by the quadrature of vh_freezeout.cuh and the
+// exponentials combined, so that neither factor overflows at large p_T.
 extern "C" int vh_cooper_frye_2d(const double* elements, long long count, double t_fo, double mass, double degeneracy,
                                  const double* pt, int npt, const double* phi, int nphi, double* out) {
   if (!elements || count < 0 || !(t_fo > 0) || !(mass >= 0) || !pt || !phi || npt < 1 || nphi < 1 || !out ||
@@ -58,13 +60,7 @@ extern "C" int vh_cooper_frye_2d(const double* elements, long long count, double
       const double mt = std::sqrt(mass * mass + pt[a] * pt[a]);
       const double px = pt[a] * std::cos(phi[b]), py = pt[a] * std::sin(phi[b]);
       double sum = 0;
-      for (long long e = 0; e < count; e++) {
-        const double* el = elements + 9 * e;
-        const double arg = mt * el[6] / t_fo;
-        const double boost = std::exp((px * el[7] + py * el[8]) / t_fo);
-        sum += (2 * mt * std::cyl_bessel_k(1.0, arg) * el[3] + 2 * std::cyl_bessel_k(0.0, arg) * (px * el[4] + py * el[5])) *
-               boost;
-      }
+      for (long long e = 0; e < count; e++) sum += vh_fo::cf2_term(elements + 9 * e, mt, px, py, t_fo);
       out[(long long)a * nphi + b] = pref * sum;
     }
   return VH_OK;
@@ -86,9 +82,7 @@ extern "C" int vh_cooper_frye_3d(const double* elements, long long count, double
       const double mt = std::sqrt(mass * mass + pt[a] * pt[a]);
       const double px = pt[a] * std::cos(phi[b]), py = pt[a] * std::sin(phi[b]);
       double sum = 0;
-      for (long long e = 0; e < count; e++) {
-        sum += vh_fo::cf3_term(elements + 12 * e, mt, px, py, y, t_fo);
-      }
+      for (long long e = 0; e < count; e++) sum += vh_fo::cf3_term(elements + 12 * e, mt, px, py, y, t_fo);
       out[(long long)a * nphi + b] = pref * sum;
     }
   return VH_OK;
