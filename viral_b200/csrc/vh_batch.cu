@@ -687,14 +687,27 @@ extern "C" int vh_batch_autotune(vh_batch* b, const char* cache_path, int probe_
   const size_t pool_bytes = (size_t)52 * b->ntot * b->esz;
   void* save = nullptr;
   VB_CUDA(b, cudaMalloc(&save, pool_bytes));
-  VB_CUDA(b, cudaMemcpy(save, b->pool, pool_bytes, cudaMemcpyDeviceToDevice));
+  // put the saved pool back; on failure free the copy and report
+  auto restore = [&]() {
+    const cudaError_t e = cudaMemcpy(b->pool, save, pool_bytes, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+      b->err = std::string("vh_batch_autotune: restoring the pool: ") + cudaGetErrorString(e);
+      cudaFree(save);
+    }
+    return e == cudaSuccess;
+  };
+  if (const cudaError_t e = cudaMemcpy(save, b->pool, pool_bytes, cudaMemcpyDeviceToDevice); e != cudaSuccess) {
+    b->err = std::string("vh_batch_autotune: saving the pool: ") + cudaGetErrorString(e);
+    cudaFree(save);
+    return VH_E_CUDA;
+  }
   double best = 1e300;
   int best_v = b->variant, best_s = b->steps_per_launch;
   for (int v = 0; v < kNumVariants; v++)
     for (int spl : kStepsChoices) {
       int blocks = 0;
       if (launch(b, v, 0, 0, true, &blocks) != VH_OK || blocks <= 0) continue;
-      VB_CUDA(b, cudaMemcpy(b->pool, save, pool_bytes, cudaMemcpyDeviceToDevice));
+      if (!restore()) return VH_E_CUDA;
       if (vh_batch_reset(b) != VH_OK) break;
       b->variant = v;
       b->steps_per_launch = spl;
@@ -702,13 +715,13 @@ extern "C" int vh_batch_autotune(vh_batch* b, const char* cache_path, int probe_
       const int steps = ((probe_steps + spl - 1) / spl) * spl;
       double sec = 0;
       if (vh_batch_run(b, spl, nullptr, nullptr) != VH_OK) continue;  // warm-up launch
-      VB_CUDA(b, cudaMemcpy(b->pool, save, pool_bytes, cudaMemcpyDeviceToDevice));
+      if (!restore()) return VH_E_CUDA;
       if (vh_batch_reset(b) != VH_OK) break;
       if (vh_batch_run(b, steps, &sec, nullptr) != VH_OK) continue;
       const double ms = 1e3 * sec / steps;
       if (ms < best) { best = ms; best_v = v; best_s = spl; }
     }
-  VB_CUDA(b, cudaMemcpy(b->pool, save, pool_bytes, cudaMemcpyDeviceToDevice));
+  if (!restore()) return VH_E_CUDA;
   cudaFree(save);
   vh_batch_reset(b);
   b->variant = best_v;
