@@ -95,12 +95,24 @@ struct Corners {
   VH_FO_HD double x(int v, int q) const { return ((v >> q) & 1) ? hi[q] : lo[q]; }
 };
 
-// loads the corners of cube (i, j, k); returns false when the isotherm
-// misses it (all corners on one side)
+// cell index of corner v of cube (i, j, k) in its time slice
+template <int D>
+VH_FO_HD long long corner_cell(const Geo& g, int i, int j, int k, int v) {
+  const int bx = (v >> 1) & 1, by = (v >> 2) & 1, bz = D == 4 ? (v >> 3) & 1 : 0;
+  return ((long long)(k + bz - (D == 4 ? 0 : kG)) * g.gy + (j + by)) * g.gx + (i + bx);
+}
+
+// loads the corners of cube (i, j, k); returns false, having read T alone,
+// when the isotherm misses it (all corners on one side)
 template <int D>
 VH_FO_HD bool load(const Geo& g, int i, int j, int k, const double* t0, const double* t1, const double* u0,
                    const double* u1, Corners<D>& K) {
   bool pos = false, neg = false;
+  for (int v = 0; v < (1 << D); v++) {
+    K.f[v] = ((v & 1) ? t1 : t0)[corner_cell<D>(g, i, j, k, v)] - g.t_fo;
+    if (K.f[v] > 0) pos = true; else neg = true;
+  }
+  if (!pos || !neg) return false;
   K.lo[0] = g.tau0;
   K.hi[0] = g.tau1;
   K.lo[1] = g.x0 + (i - kG) * g.dx;
@@ -112,15 +124,11 @@ VH_FO_HD bool load(const Geo& g, int i, int j, int k, const double* t0, const do
     K.hi[D - 1] = g.z0 + (k + 1 - kG) * g.dz;
   }
   for (int v = 0; v < (1 << D); v++) {
-    const int bt = v & 1, bx = (v >> 1) & 1, by = (v >> 2) & 1, bz = D == 4 ? (v >> 3) & 1 : 0;
-    const long long c = ((long long)(k + bz - (D == 4 ? 0 : kG)) * g.gy + (j + by)) * g.gx + (i + bx);
-    const double* T = bt ? t1 : t0;
-    const double* U = bt ? u1 : u0;
+    const long long c = corner_cell<D>(g, i, j, k, v);
+    const double* U = (v & 1) ? u1 : u0;
     for (int q = 0; q < D; q++) K.u[v][q] = U[q * g.n + c];
-    K.f[v] = T[c] - g.t_fo;
-    if (K.f[v] > 0) pos = true; else neg = true;
   }
-  return pos && neg;
+  return true;
 }
 
 // elements that cube (i, j, k) emits, from the signs of T - T_fo alone: per
@@ -129,11 +137,8 @@ VH_FO_HD bool load(const Geo& g, int i, int j, int k, const double* t0, const do
 template <int D>
 VH_FO_HD int count(const Geo& g, int i, int j, int k, const double* t0, const double* t1) {
   unsigned hot = 0;
-  for (int v = 0; v < (1 << D); v++) {
-    const int bt = v & 1, bx = (v >> 1) & 1, by = (v >> 2) & 1, bz = D == 4 ? (v >> 3) & 1 : 0;
-    const long long c = ((long long)(k + bz - (D == 4 ? 0 : kG)) * g.gy + (j + by)) * g.gx + (i + bx);
-    if ((bt ? t1 : t0)[c] - g.t_fo > 0) hot |= 1u << v;
-  }
+  for (int v = 0; v < (1 << D); v++)
+    if (((v & 1) ? t1 : t0)[corner_cell<D>(g, i, j, k, v)] - g.t_fo > 0) hot |= 1u << v;
   if (hot == 0 || hot == (1u << (1 << D)) - 1) return 0;
   int total = 0, nsim = D == 4 ? 24 : 6;
   for (int s = 0; s < nsim; s++) {
