@@ -201,3 +201,17 @@ def test_host_spectra_refuse_a_massless_hadron_at_zero_momentum():
     el3 = np.zeros((1, 12))
     el3[0, 0], el3[0, 4], el3[0, 8] = 1.0, 1.0, 1.0
     assert cooper_frye_3d(el3, 0.15, 0.0, 1.0, 0.0, [0.0], [0.0])[0, 0] == 0.0
+
+
+def test_device_wrappers_want_cuda_tensors():
+    """the Python wrappers of the device forms take CUDA tensors and check
+    their sizes before any call (so also here, without a GPU)"""
+    import torch
+    from viral_b200.hydro import _cuda_f64, cooper_frye_2d_device, freezeout_2d_device
+    n = 14 * 14
+    with pytest.raises(TypeError):
+        freezeout_2d_device(8, 8, 0.1, 0.1, 1.0, 1.1, np.zeros(n), np.zeros(n), np.zeros((3, n)), np.zeros((3, n)), 0.15)
+    with pytest.raises(TypeError):
+        cooper_frye_2d_device(torch.zeros((4, 9)), 0.15, 0.1, 1.0, [0.5], [0.0])
+    with pytest.raises(TypeError):
+        _cuda_f64(torch.zeros(n), 0, n)
