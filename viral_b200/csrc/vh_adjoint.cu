@@ -28,6 +28,7 @@
 #include "vh.h"
 #include "vh_adjoint.cuh"
 #include "vh_handle.cuh"
+#include "vh_nvtx.h"
 
 namespace {
 
@@ -823,6 +824,7 @@ extern "C" int vh_adjoint_eps_p(vh_handle* h, int nsteps, int checkpoint_every, 
                                 double* grad_e, double* grad_etas) {
   if (!h || nsteps < 1 || checkpoint_every < 1) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
+  VhNvtxRange range("discrete adjoint of eps_p");
   const DevCfg& C = h->C;
   if (C.cart || !C.bi || C.mirror || C.recon != VH_RECON_WENO5 || C.cold)
     return fail(h, VH_E_UNSUPPORTED,

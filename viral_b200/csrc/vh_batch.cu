@@ -22,6 +22,7 @@
 #include "vh.h"
 #include "vh_adjoint.cuh"
 #include "vh_aux.cuh"
+#include "vh_nvtx.h"
 
 using namespace vh;
 
@@ -554,6 +555,7 @@ static int launch(vh_batch* b, int variant, cudaStream_t s, int nsteps, bool que
 // replay.  Returns the device seconds in *seconds.
 extern "C" int vh_batch_run(vh_batch* b, int max_steps, double* seconds, int* graph_used) {
   if (!b || max_steps < 0) return VH_E_ARG;
+  VhNvtxRange range("batched ensemble run");
   const int block = kVariants[b->variant].nc * 32;
   if (int r = build_uitems(b, block)) return r;
   cudaStream_t s;

@@ -16,6 +16,7 @@
 
 #include "vh.h"
 #include "vh_freezeout.cuh"
+#include "vh_nvtx.h"
 
 namespace {
 
@@ -80,6 +81,7 @@ int surface(const vh_fo::Geo& g, const double* t0, const double* t1, const doubl
             long long cap, long long* count, cudaStream_t st) {
   const long long nc = vh_fo::cubes(g, D);
   if (nc > INT_MAX) return VH_E_ARG;  // one scan of int-counted items
+  VhNvtxRange range("freeze-out surface");
   size_t scan_bytes = 0;
   const long long* scan_in = nullptr;
   long long* scan_out = nullptr;
@@ -121,6 +123,7 @@ int spectrum(const double* el, long long count, double t_fo, double mass, double
              const double* pt, int npt, const double* phi, int nphi, double* out, cudaStream_t st) {
   const long long nb = (long long)npt * nphi;
   if (nb > INT_MAX) return VH_E_ARG;
+  VhNvtxRange range("Cooper-Frye spectrum");
   std::vector<double> bins(3 * (size_t)nb);
   for (int a = 0; a < npt; a++)
     for (int b = 0; b < nphi; b++) {

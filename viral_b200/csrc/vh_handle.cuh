@@ -10,6 +10,7 @@
 
 #include "vh.h"
 #include "vh_aux.cuh"
+#include "vh_nvtx.h"
 
 using namespace vh;
 
@@ -134,6 +135,7 @@ static int stage_update(vh_handle* h, const DevPtrs<R>& P, double tau, double ts
 
 template <class R>
 static int step_once(vh_handle* h, const DevPtrs<R>& P) {
+  VhNvtxRange range("TVDRK2 step");
   const double tau = h->tau, ts = h->cfg.dtau;
   int r;
   if ((r = stage_rhs<R>(h, P, 0, tau))) return r;
