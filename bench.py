@@ -1,25 +1,36 @@
-"""Benchmark of the viscous KT step (cell-updates per second).
+"""Benchmark of the viscous KT step: cell-updates/s, events/s, mixed vs FP64
+at stated error, adjoint/forward ratio.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload glauber_161x161x41] [--precision fp64|mixed]
+                    [--sub mixed,ensemble,adjoint]
 
 A step is one TVDRK2 time step (two RK stages) of the whole grid.  The
-default workload is the 3+1D Milne event of 161x161x41 cells (dx = dy = 0.1
+headline workload is the 3+1D Milne event of 161x161x41 cells (dx = dy = 0.1
 fm, d eta = 0.25, dtau = 0.02 fm/c from tau0 = 0.6 fm/c), MC-Glauber Pb+Pb at
 b = 7 fm (seed 0), synthetic EOS table, eta/s = 0.08, FP64.  The device state
 (52 arrays x 1.3 M cells, 545 MB in FP64) is larger than L2, so no flush is
 needed between steps.  value = interior cells x steps / device seconds.
 
+At N = 1 the same JSON line also carries, each with its own CUDA-event
+timing and clock record:
+  mixed     the precision form of the same event (FP32 state, FP64
+            root-find): ms per step, speed-up over the FP64 line, errors of
+            e, u^mu, pi^{mu nu} against FP64 at steps 10, 50 and W+K;
+  ensemble  2048 boost-invariant events in one persistent kernel under a CUDA
+            graph (mixed and FP64), completed events/s, failed events apart,
+            the looped single-event FP64 step and the reference's CPU step;
+  adjoint   the eps_p gradient of the 128x128 event: adjoint/forward device
+            time in FP64 and mixed, checked against central differences.
+
 One process per GPU; with N > 1 every rank evolves its own replica of the
 event (the step does not shard: replicas only), value is the sum over ranks
-and the time the max over ranks.
+and the time the max over ranks; the sub-records run at N = 1 only.
 
 --impl reference times the reference's own CPU step (its NEWEST5 headers
-built in oracle/_ref, TVDRK2 on a 40x40x10 Milne grid, the compile-time grid
-of its default scenario block) in one process per host core.  --ensemble N
-reports events/s of a batched ensemble; its cpu_baseline is the reference's
-boost-invariant step on the host cores, extrapolated to the ensemble's cell
-updates.
+built in oracle/_ref, the GINIT block's EOS hooks on the synthetic table) on
+30x30x41 windows cut from the same Glauber state, in one process per host
+core, and prints the same config.
 """
 from __future__ import annotations
 
@@ -52,70 +63,145 @@ def parse():
     p.add_argument("--precision-report", action="store_true",
                    help="run the workload to tau_end in FP64 and mixed precision; report errors and speedup")
     p.add_argument("--tau-end", type=float, default=10.0)
+    p.add_argument("--sub", default="mixed,ensemble,adjoint",
+                   help="sub-records of the N = 1 line (comma list of mixed, ensemble, adjoint; 'none')")
     p.add_argument("--ensemble", type=int, default=0,
-                   help="events/s of a batched ensemble of this many boost-invariant events")
-    p.add_argument("--ensemble-precision", default="mixed", choices=["fp64", "mixed"])
+                   help="standalone: events/s of a batched ensemble of this many boost-invariant events")
+    p.add_argument("--ensemble-events", type=int, default=2048, help="events of the ensemble sub-record")
+    p.add_argument("--ensemble-fp64", type=int, default=1, help="also run the ensemble batch in FP64 (1/0)")
     p.add_argument("--ensemble-floor", type=float, default=None,
                    help="initial energy-density floor of the ensemble events in GeV/fm^3 (default: the workload's)")
     p.add_argument("--loop-per-side", type=int, default=2,
                    help="events per grid side for the looped single-event FP64 baseline")
     p.add_argument("--adjoint", action="store_true",
-                   help="adjoint/forward device-time ratio of the eps_p gradient (128x128 Glauber, 330 steps)")
+                   help="standalone: adjoint/forward device-time ratio of the eps_p gradient (128x128 Glauber)")
     p.add_argument("--checkpoint-every", type=int, default=25)
     p.add_argument("--adjoint-steps", type=int, default=0,
                    help="steps of the adjoint workload (0: its 330 steps to tau = 7.2 fm/c); small values for profiling")
+    p.add_argument("--adjoint-reps", type=int, default=5, help="timed repetitions of forward and adjoint")
     p.add_argument("--adjoint-precision", default="both", choices=["both", "fp64", "mixed"])
     p.add_argument("--adjoint-fd", type=int, default=4,
                    help="unit directions of the finite-difference check in the adjoint mode (0: none)")
+    p.add_argument("--ref-sample-seconds", type=float, default=2.0,
+                   help="--impl reference: step seconds per process in one sample (one sample per step)")
     return p.parse_args()
 
 
 # ---------------------------------------------------------------- reference CPU
+#
+# The reference's own CPU step (its NEWEST5 headers compiled in oracle/_ref)
+# on windows cut from the benchmarked state.  Its grid is a compile-time
+# constant: the table-EOS builds (libref_window_3d / _lbi: the GINIT scenario
+# block with its EOS hooks on a run-time table) step 30 x 30 x nz cells of
+# one rank, so the 161 x 161 x 41 event is cut into 6 x 6 such windows (the
+# reference's own MPI decomposition, with copy boundaries where its halo
+# exchange would run).  Each host process steps its share of the windows in
+# turn; only the TVDRK2 calls are timed.
+
+REF_WINDOW = 30  # interior cells per window side (XL/XS of the GINIT block)
 
 
-def _ref_worker(args):
-    """One process: the reference's TVDRK2 on the compile-time grid of a
-    build (milne_3d: 40x40x10 cells; milne_lbi: 40x40 boost invariant) for
-    about `seconds` seconds; returns (interior cells x steps, seconds)."""
-    seconds, seed, variant = (*args, "milne_3d")[:3]
+def window_origins(n: int, w: int = REF_WINDOW) -> list:
+    """ghost-inclusive origins of w-wide windows covering n interior cells
+    (the last one flush with the far edge)"""
+    if n <= w:
+        return [0]
+    o = list(range(0, n - w + 1, w))
+    if o[-1] != n - w:
+        o.append(n - w)
+    return o
+
+
+def glauber_rest_state(cfg, inp) -> "np.ndarray":
+    """18-field state of a Glauber initial condition at rest with pi = 0:
+    T^{tau tau} = e, T^{tau i} = 0, prevu = u = (1, 0, 0, 0)"""
+    import numpy as np
+    gx, gy, gz = cfg.gdims()
+    n = gx * gy * gz
+    f = np.zeros((18, n))
+    f[0] = np.asarray(inp["e"]).reshape(n)
+    f[1] = 1.0
+    f[10] = f[0]
+    f[14] = 1.0
+    return f
+
+
+def _ref_window_worker(args):
+    """One process: the reference's TVDRK2 on its windows, round robin, for
+    n_samples samples of about `seconds` each (at least one window step per
+    sample); returns [(interior cells x steps, step seconds)] per sample."""
+    variant, state_path, dims, origins, seconds, n_samples, tau0, dtau, eos_path = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
-    from pyoracle import F_PI, F_PU, F_U, Oracle, OracleConfig, RefBuild, smooth_state
+    from pyoracle import RefBuild
     R = RefBuild(variant)
-    x, y, z = R.coords()
-    tau, ts = 0.6, 0.02
-    f = smooth_state(x, y, z, tau, ts, seed=seed)
-    if R.boost_invariant:  # no eta flow and no eta components of pi
-        for q in (F_U + 3, F_PI + 3, F_PI + 4, F_PU + 3):
-            f[q] = 0.0
-        for q in (F_U, F_PU):
-            f[q] = np.sqrt(1 + f[q + 1] ** 2 + f[q + 2] ** 2)
-    O = Oracle(OracleConfig(nx=R.gx - 6, ny=R.gy - 6, nz=1 if R.boost_invariant else R.gz - 6,
-                            boost_invariant=R.boost_invariant, dx=R.dx, dy=R.dy, dz=R.dz, eos_kind=0,
-                            eos_a=R.factor, etas0=1 / (4 * math.pi), hbarc=R.gevfm))
-    O.set_state(f)
-    O.fill_tmunu(tau)
-    R.set_state(O.get_state())
+    R.set_eos_table(np.load(eos_path))
+    gx, gy, gz = dims
+    F = np.load(state_path, mmap_mode="r").reshape(18, gz, gy, gx)
+    wins = []
+    for (i0, j0) in origins:
+        f = np.ascontiguousarray(F[:, :R.gz, j0:j0 + R.gy, i0:i0 + R.gx]).reshape(18, -1)
+        wins.append([f, tau0])
     cells = (R.ir - R.il) * (R.jr - R.jl) * (R.kr - R.kl)
-    R.step(tau, ts)  # warm-up
-    tau += ts
-    n, t0 = 0, time.perf_counter()
-    while True:
-        R.step(tau, ts)
-        tau += ts
-        n += 1
-        dt = time.perf_counter() - t0
-        if dt >= seconds:
-            break
-    return cells * n, dt
+    out, q = [], 0
+    for _ in range(n_samples):
+        done, t_step = 0, 0.0
+        while True:
+            w = wins[q % len(wins)]
+            R.set_state(w[0])
+            t0 = time.perf_counter()
+            R.step(w[1], dtau)
+            t_step += time.perf_counter() - t0
+            w[0] = R.get_state()
+            w[1] += dtau
+            done += cells
+            q += 1
+            if t_step >= seconds:
+                break
+        out.append((done, t_step))
+    return out
 
 
-def cpu_reference(seconds: float, procs: int, variant: str = "milne_3d"):
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(seconds, s, variant) for s in range(procs)])
-    rate = sum(c / t for c, t in res)
-    return rate, procs
+def reference_windows(workload: str, seconds: float, n_samples: int, procs: int):
+    """Aggregate cell-updates/s of the reference's CPU step over `procs` host
+    processes on windows of a Glauber state of `workload` (the benchmarked
+    161x161x41 event, or a boost-invariant event of the ensemble): one rate
+    per sample (sum over processes of cells / their step seconds)."""
+    import tempfile
+
+    import numpy as np
+    from viral_b200 import configs as C
+    if workload == "ensemble":
+        cfg = C.glauber_config(nx=128, ny=128, boost_invariant=True)
+        inp = C.glauber_inputs(cfg, b=7.0, seed=0, efloor_gev=C.ENSEMBLE_FLOOR_GEV)
+        variant = "window_lbi"
+    else:
+        nx, ny, nz = (int(v) for v in workload.split("_", 1)[1].split("x"))
+        if nz != 41:
+            raise SystemExit("the reference's 3+1D window build has 41 eta cells")
+        cfg = C.glauber_config(nx=nx, ny=ny, nz=nz)
+        inp = C.glauber_inputs(cfg, b=7.0, seed=0)
+        variant = "window_3d"
+    f = glauber_rest_state(cfg, inp)
+    gdims = cfg.gdims()
+    origins = [(i0, j0) for j0 in window_origins(cfg.ny) for i0 in window_origins(cfg.nx)]
+    with tempfile.TemporaryDirectory() as td:
+        sp, ep = os.path.join(td, "state.npy"), os.path.join(td, "eos.npy")
+        np.save(sp, f)
+        np.save(ep, np.asarray(cfg.eos_table))
+        procs = max(1, min(procs, len(origins)))
+        jobs = [(variant, sp, gdims, origins[p::procs], seconds, n_samples, cfg.tau0, cfg.dtau, ep)
+                for p in range(procs)]
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_ref_window_worker, jobs)
+    rates = [sum(r[k][0] / r[k][1] for r in res) for k in range(n_samples)]
+    desc = (f"{procs} processes x the reference's TVDRK2 (NEWEST5 headers, GINIT block with the synthetic EOS table, "
+            f"1 MPI rank each) on {len(origins)} windows of {REF_WINDOW}x{REF_WINDOW}"
+            f"{'' if cfg.boost_invariant else 'x' + str(cfg.nz)} cells cut from the "
+            f"{'boost-invariant 128x128 ensemble event' if workload == 'ensemble' else workload} Glauber state "
+            f"(eta/s = 1/4pi, d eta = 0.1 in that block; copy boundaries at window faces)")
+    return rates, procs, desc
 
 
 def cpu_model() -> str:
@@ -191,27 +277,41 @@ class ClockSampler:
 # ---------------------------------------------------------------- workload
 
 
-def build_workload(name: str, precision: str):
+def build_workload(name: str, precision: str, inputs: bool = True):
+    """(Config, inputs or None, description) of a named workload"""
     from viral_b200 import _abi as A
     from viral_b200 import configs as C
     prec = A.PREC_MIXED if precision == "mixed" else A.PREC_FP64
+    inp = None
     if name.startswith("glauber_"):
         nx, ny, nz = (int(v) for v in name.split("_", 1)[1].split("x"))
         cfg = C.glauber_config(nx=nx, ny=ny, nz=nz, boost_invariant=nz == 1, precision=prec)
-        inp = C.glauber_inputs(cfg, b=7.0, seed=0)
+        if inputs:
+            inp = C.glauber_inputs(cfg, b=7.0, seed=0)
         desc = {"workload": name, "grid": [nx, ny, nz], "coords": "milne", "dx_fm": 0.1,
                 "deta": 0.25, "dtau_fm": 0.02, "tau0_fm": 0.6, "eos": "synthetic table (2000 rows)",
                 "eta_over_s": 0.08, "ic": "MC-Glauber Pb+Pb b=7 fm seed 0, 208 nucleons, sigma_nn=6.4 fm^2",
                 "recon": "WENO5", "precision": precision}
     elif name == "gubser_129":
         cfg = C.gubser_config(precision=prec)
-        inp = C.gubser_inputs(cfg)
+        if inputs:
+            inp = C.gubser_inputs(cfg)
         desc = {"workload": "gubser_129", "grid": [129, 129, 1], "coords": "milne (boost invariant)",
                 "dx_fm": 0.1, "dtau_fm": 0.01, "tau0_fm": 1.0, "eos": "conformal", "eta_over_s": 0.2,
                 "recon": "WENO5", "precision": precision}
     else:
         raise SystemExit(f"unknown workload {name}")
     return cfg, inp, desc
+
+
+def line_config(name: str, precision: str, world: int) -> dict:
+    """the `config` of the JSON line: the same dict for both arms"""
+    cfg, _, desc = build_workload(name, precision, inputs=False)
+    gx, gy, gz = cfg.gdims()
+    cells = cfg.nx * cfg.ny * (1 if cfg.boost_invariant else cfg.nz)
+    mb = 52 * gx * gy * gz * (8 if precision == "fp64" else 4) / 1e6
+    return dict(desc, interior_cells=cells, parallelism=f"replicas x{world}",
+                l2="state (52 arrays, %.0f MB) larger than the 126 MB L2; no flush" % mb)
 
 
 def max_over_ranks(ms: float, dist, device: str) -> float:
@@ -279,6 +379,48 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def timed_steps(H, stream, k: int, dev: int):
+    """device ms of k steps of handle H on `stream` (CUDA events), with the
+    clocks sampled during them"""
+    import torch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        H.step(k)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), clk.summary()
+
+
+KERNELS = ["k_dir_x", "k_dir_y", "k_dir_eta", "k_update_stage1", "k_update_stage2"]
+
+
+def kernel_times(H, cfg):
+    """per-launch device ms and share of each step kernel over 2 steps
+    (vh_time_kernels: events around every launch, outside the timed region)"""
+    kt = H.time_kernels(2)
+    launches = {"k_dir_x": 4, "k_dir_y": 4, "k_dir_eta": 0 if cfg.boost_invariant else 4, "k_update_stage1": 2,
+                "k_update_stage2": 2}
+    per_launch = {nm: (kt[q] / launches[nm] if launches[nm] else 0.0) for q, nm in enumerate(KERNELS)}
+    share = {nm: kt[q] / max(sum(kt), 1e-30) for q, nm in enumerate(KERNELS)}
+    top = max(KERNELS, key=lambda nm: kt[KERNELS.index(nm)])
+    return per_launch, share, top
+
+
+def roofline(cfg, precision: str, cells: int, per_launch: dict, share: dict, top: str) -> dict:
+    peak, peak_kind = measured_peaks()
+    ach = algorithmic_bytes(cfg, top) * cells / (per_launch[top] / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_source": peak_kind,
+            "traffic": (MEASURED_TRAFFIC_PER_CELL[(precision, top)] * cells
+                        if (precision, top) in MEASURED_TRAFFIC_PER_CELL else None),
+            "algorithmic_bytes_per_cell": algorithmic_bytes(cfg, top),
+            "compute_bound_ncu": (dict(zip(("limit", "active_frac_of_peak"), MEASURED_COMPUTE_BOUND[(precision, top)]))
+                                  if (precision, top) in MEASURED_COMPUTE_BOUND else None),
+            "kernel_ms_per_launch": per_launch, "kernel_share": share}
+
+
 def run_ours(args, rank, world, dist):
     import numpy as np
     import torch
@@ -298,36 +440,20 @@ def run_ours(args, rank, world, dist):
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev) as clk:
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        H.step(args.steps)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
+    ms, clocks = timed_steps(H, stream, args.steps, dev)
+    ms = max_over_ranks(ms, dist, "cuda")
     value = whole_job_rate(cells, args.steps, world, ms)
 
-    # per-kernel device times (outside the timed region) for the roofline
-    kt = H.time_kernels(2)
-    names = ["k_dir_x", "k_dir_y", "k_dir_eta", "k_update_stage1", "k_update_stage2"]
-    launches = {"k_dir_x": 4, "k_dir_y": 4, "k_dir_eta": 0 if cfg.boost_invariant else 4, "k_update_stage1": 2,
-                "k_update_stage2": 2}
-    per_launch = {nm: (kt[q] / launches[nm] if launches[nm] else 0.0) for q, nm in enumerate(names)}
-    share = {nm: kt[q] / max(sum(kt), 1e-30) for q, nm in enumerate(names)}
-    top = max(names, key=lambda nm: kt[names.index(nm)])
-    peak, peak_kind = measured_peaks()
-    ach = algorithmic_bytes(cfg, top) * cells / (per_launch[top] / 1e3) / 1e9
+    per_launch, share, top = kernel_times(H, cfg)
 
     # end to end through the C ABI with pinned host buffers
     n18 = 18 * H.n
     if args.e2e_steps <= 0:
         H.close()
         return None if rank else {"metric": METRIC, "value": value, "ms_per_step": ms / args.steps,
-                                  "config": desc, "kernel_ms": dict(zip(names, kt.tolist()))}
+                                  "config": desc, "kernel_ms_per_launch": per_launch}
     host = torch.empty(n18, dtype=torch.float64, pin_memory=True).numpy()
-    H_state = H.get_state()
-    host[:] = H_state.reshape(-1)
+    host[:] = H.get_state().reshape(-1)
     tau_now = H.tau
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -343,39 +469,107 @@ def run_ours(args, rank, world, dist):
     e2e_value = cells * args.e2e_steps * world / (e2e_ms / 1e3)
     H.close()
 
-    out = None
-    if rank == 0:
-        clocks = clk.summary()
-        out = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if cfg.precision == 0 else "f32 state / f64 root-find",
-            "data": "synthetic (seeded MC-Glauber initial state)",
-            "config": dict(desc, interior_cells=cells, parallelism=f"replicas x{world}",
-                           l2="state (52 arrays, %.0f MB) larger than the 126 MB L2; no flush" %
-                              (52 * H_state.shape[1] * (8 if cfg.precision == 0 else 4) / 1e6)),
-            "clocks": clocks,
-            "gpu_launches": launches_per_step * args.steps,
-            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n18 * 8, "d2h_bytes_per_step": n18 * 8,
-                    "what": "vh_set_state (pinned host) + vh_step(1) + vh_get_state per step"},
-            "roofline": {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "peak_source": peak_kind,
-                         "traffic": (MEASURED_TRAFFIC_PER_CELL[(args.precision, top)] * cells
-                                     if (args.precision, top) in MEASURED_TRAFFIC_PER_CELL else None),
-                         "algorithmic_bytes_per_cell": algorithmic_bytes(cfg, top),
-                         "compute_bound_ncu": (dict(zip(("limit", "active_frac_of_peak"),
-                                                        MEASURED_COMPUTE_BOUND[(args.precision, top)]))
-                                               if (args.precision, top) in MEASURED_COMPUTE_BOUND else None),
-                         "kernel_ms_per_launch": per_launch, "kernel_share": share},
-        }
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if cfg.precision == 0 else "f32 state / f64 root-find",
+        "data": "synthetic (seeded MC-Glauber initial state)",
+        "config": line_config(args.workload, args.precision, world),
+        "clocks": clocks,
+        "gpu_launches": launches_per_step * args.steps,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n18 * 8, "d2h_bytes_per_step": n18 * 8,
+                "what": "vh_set_state (pinned host) + vh_step(1) + vh_get_state per step"},
+        "roofline": roofline(cfg, args.precision, cells, per_launch, share, top),
+    }
+
+
+# ---------------------------------------------------------------- mixed precision
+
+
+def interior(cfg):
+    import numpy as np
+    gx, gy, gz = cfg.gdims()
+    idx = np.arange(gx * gy * gz)
+    i, j, k = idx % gx, (idx // gx) % gy, idx // (gx * gy)
+    kl, kr = (0, 1) if cfg.boost_invariant else (3, 3 + cfg.nz)
+    return (i >= 3) & (i < 3 + cfg.nx) & (j >= 3) & (j < 3 + cfg.ny) & (k >= kl) & (k < kr)
+
+
+def state_errors(a, b, m) -> dict:
+    """max and L2 relative differences of a against b over the interior mask
+    m, per group: e; u^mu; pi^{mu nu}"""
+    import numpy as np
+    out = {}
+    for g, qs in {"e": [0], "u": [1, 2, 3, 4], "pi": [5, 6, 7, 8, 9]}.items():
+        x, y = a[qs][:, m], b[qs][:, m]
+        d = x - y
+        out[g] = {"max_rel": float(np.max(np.abs(d)) / np.max(np.abs(y))),
+                  "l2_rel": float(np.sqrt(np.sum(d * d)) / np.sqrt(np.sum(y * y)))}
     return out
+
+
+ERROR_NORMS = ("max_rel = max|a-b| / max|b| over the group's components and the interior cells; "
+               "l2_rel = ||a-b||_2 / ||b||_2; groups e, u^mu (4), pi^{mu nu} (5 stored)")
+
+
+def mixed_record(args, fp64_ms_per_step: float) -> dict:
+    """The precision form on the same event: FP32 state, fluxes,
+    reconstruction and sources, FP64 root-find and conservation sums.  Device
+    ms per step over --steps steps after --warmup (as the FP64 line), the
+    speed-up over the FP64 line, and the errors of e, u^mu, pi^{mu nu}
+    against an FP64 run from the same initial state at step 10, step 50 and
+    the step the timed run ended on; beside them, the same errors of an FP64
+    run whose initial e was perturbed by 1e-7 (relative, seeded), the size of
+    FP32 rounding: where that baseline is large the event's trajectories
+    have separated, which no reduced-precision step can avoid."""
+    import numpy as np
+    import torch
+    from viral_b200 import _abi as A
+    from viral_b200 import configs as C
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    stream = torch.cuda.current_stream()
+    cfg32, inp, desc = build_workload(args.workload, "mixed")
+    cfg64, _, _ = build_workload(args.workload, "fp64", inputs=False)
+    cells = cfg32.nx * cfg32.ny * (1 if cfg32.boost_invariant else cfg32.nz)
+    H = C.make_hydro(cfg32, inp)
+    A.check(A.lib().vh_set_stream(H.h, ctypes_void_p(stream.cuda_stream)), H.h)
+    H.step(args.warmup)
+    torch.cuda.synchronize()
+    ms, clocks = timed_steps(H, stream, args.steps, dev)
+    per_launch, share, top = kernel_times(H, cfg32)
+    H.close()
+    m = interior(cfg64)
+    marks = sorted({10, 50, args.warmup + args.steps})
+    rng = np.random.default_rng(7)
+    inp_p = dict(inp, e=np.asarray(inp["e"]) * (1 + 1e-7 * rng.uniform(-1, 1, size=np.asarray(inp["e"]).shape)))
+    errs, base = {}, {}
+    with C.make_hydro(cfg64, inp) as H64, C.make_hydro(cfg32, inp) as H32, C.make_hydro(cfg64, inp_p) as Hp:
+        done = 0
+        for k in marks:
+            for h in (H64, H32, Hp):
+                h.step(k - done)
+            done = k
+            ref = H64.get_state()
+            errs[str(k)] = state_errors(H32.get_state(), ref, m)
+            base[str(k)] = state_errors(Hp.get_state(), ref, m)
+        tau_end = H64.tau
+    ms_step = ms / args.steps
+    return {"metric": METRIC, "value": cells * args.steps / (ms / 1e3), "unit": METRIC, "ms_per_step": ms_step,
+            "steps": args.steps, "warmup": args.warmup, "speedup_vs_fp64": fp64_ms_per_step / ms_step,
+            "dtype": "f32 state, fluxes, reconstruction, sources / f64 root-find, EOS inversion, conservation sums",
+            "errors_vs_fp64": errs, "fp64_perturbed_1e-7_vs_fp64": base, "error_steps": marks,
+            "error_tau_end_fm": tau_end, "error_norms": ERROR_NORMS, "clocks": clocks,
+            "gpu_launches": 2 * ((2 if cfg32.boost_invariant else 3) + 1) * args.steps,
+            "roofline": roofline(cfg32, "mixed", cells, per_launch, share, top),
+            "config": dict(desc, workload=args.workload + " (precision form)")}
 
 
 def precision_report(args):
     """Both precisions from the same initial state to tau_end: max and L2
     relative errors of e, u^mu, pi^{mu nu} of the mixed step against the FP64
     step over the interior, and the device-time ratio."""
-    import numpy as np
     import torch
     from viral_b200 import configs as C
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
@@ -394,147 +588,183 @@ def precision_report(args):
         res[prec] = {"ms": e0.elapsed_time(e1), "steps": nsteps, "tau": H.tau, "tmax_gev": H.max_temperature()}
         states[prec] = H.get_state()
         H.close()
-    gx, gy, gz = cfg.gdims()
-    idx = np.arange(gx * gy * gz)
-    i, j, k = idx % gx, (idx // gx) % gy, idx // (gx * gy)
-    kl, kr = (0, 1) if cfg.boost_invariant else (3, 3 + cfg.nz)
-    m = (i >= 3) & (i < 3 + cfg.nx) & (j >= 3) & (j < 3 + cfg.ny) & (k >= kl) & (k < kr)
-    a, b = states["mixed"][:, m], states["fp64"][:, m]
-    groups = {"e": [0], "u": [1, 2, 3, 4], "pi": [5, 6, 7, 8, 9]}
-    err = {}
-    for g, qs in groups.items():
-        d = a[qs] - b[qs]
-        scale = np.max(np.abs(b[qs]))
-        err[g] = {"max_rel": float(np.max(np.abs(d)) / scale),
-                  "l2_rel": float(np.sqrt(np.sum(d * d)) / np.sqrt(np.sum(b[qs] * b[qs])))}
+    err = state_errors(states["mixed"], states["fp64"], interior(cfg))
     out = {"report": "mixed vs fp64", "workload": args.workload, "tau_end": res["fp64"]["tau"],
            "steps": res["fp64"]["steps"], "ms_fp64": res["fp64"]["ms"], "ms_mixed": res["mixed"]["ms"],
            "speedup": res["fp64"]["ms"] / res["mixed"]["ms"], "errors": err,
            "tmax_gev": {"fp64": res["fp64"]["tmax_gev"], "mixed": res["mixed"]["tmax_gev"]},
-           "error_norms": "max_rel = max|mixed-fp64| / max|fp64| over the group's components; "
-                          "l2_rel = ||mixed-fp64||_2 / ||fp64||_2"}
+           "error_norms": ERROR_NORMS}
     print(json.dumps(out), flush=True)
 
 
-def ensemble(args):
-    """Batched ensemble of boost-invariant MC-Glauber events (grid side drawn
-    from {64,96,128,160,200}, dx = 0.1 fm, b uniform in [0,12] fm, seeds
-    0..N-1, dtau = 0.02 fm/c from tau0 = 0.6 fm/c, mixed precision), each
-    stopping when its maximum temperature falls below 0.15 GeV or at
-    tau = 15 fm/c; one persistent kernel under a CUDA graph with the tuned
-    variant.  Compared with looping the single-event FP64 step (one event at
-    a time, maximum temperature read after every step as the reference's
-    main loop does) on a stratified sample, extrapolated per grid side."""
+# ---------------------------------------------------------------- ensemble
+
+
+def ensemble_events(n: int):
+    """the ensemble's grid sides (from {64, 96, 128, 160, 200}) and impact
+    parameters (uniform in [0, 12] fm), seeded"""
+    import numpy as np
+    rng = np.random.default_rng(0)
+    sides = rng.choice(np.array([64, 96, 128, 160, 200]), size=n)
+    bimp = rng.uniform(0.0, 12.0, size=n)
+    return sides, bimp
+
+
+ENS_TAU0, ENS_DTAU, ENS_TAU_MAX, ENS_T_FO = 0.6, 0.02, 15.0, 0.15
+
+
+def batch_run(n: int, precision: str, floor: float, dev: int) -> dict:
+    """One batched run of the ensemble: init, autotune, run; events/s counts
+    events that completed (froze out or reached tau_max), failed events are
+    reported apart."""
     import tempfile
 
     import numpy as np
-    import torch
     from viral_b200 import _abi as A
     from viral_b200 import configs as C
     from viral_b200.batch import Batch
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    n = args.ensemble
-    rng = np.random.default_rng(0)
-    sides_all = np.array([64, 96, 128, 160, 200])
-    sides = rng.choice(sides_all, size=n)
-    bimp = rng.uniform(0.0, 12.0, size=n)
-    tau0, dtau, tau_max, t_fo = 0.6, 0.02, 15.0, 0.15
-    max_steps = C.steps_between(tau0, tau_max, dtau)
-    prec = A.PREC_MIXED if args.ensemble_precision == "mixed" else A.PREC_FP64
+    sides, bimp = ensemble_events(n)
+    max_steps = C.steps_between(ENS_TAU0, ENS_TAU_MAX, ENS_DTAU)
+    prec = A.PREC_MIXED if precision == "mixed" else A.PREC_FP64
     cfg = C.glauber_config(nx=8, ny=8, boost_invariant=True, precision=prec)
     t_init = time.perf_counter()
-    B = Batch(cfg, sides, tau0=tau0, dtau=dtau, tau_max=tau_max, t_freeze_gev=t_fo)
-    floor = C.ENSEMBLE_FLOOR_GEV if args.ensemble_floor is None else args.ensemble_floor
+    B = Batch(cfg, sides, tau0=ENS_TAU0, dtau=ENS_DTAU, tau_max=ENS_TAU_MAX, t_freeze_gev=ENS_T_FO)
     npart = B.init_glauber(seeds=np.arange(n), bimp=bimp, efloor_gev=floor)
     t_init = time.perf_counter() - t_init
     _, ecc2_initial = B.observables()
     cache = os.path.join(tempfile.gettempdir(), "vh_batch_tuning.txt")
+    t_tune = time.perf_counter()
     tune_ms = B.autotune(cache, probe_steps=16)
+    t_tune = time.perf_counter() - t_tune
     tuning = B.tuning()
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+    with ClockSampler(dev) as clk:
         sec, graph = B.run(max_steps)
     tau, nst, st = B.events()
     eps_p_final, _ = B.observables()
     B.close()
     okev = st != 3
-    observables = {"eps2_initial_mean": float(np.mean(ecc2_initial)),
-                   "eps_p_final_mean": float(np.mean(eps_p_final[okev])),
-                   "corr_eps2_eps_p": float(np.corrcoef(ecc2_initial[okev], eps_p_final[okev])[0, 1]),
-                   "what": "eccentricity of the initial energy density and momentum anisotropy where each event "
-                           "stopped (failed events excluded), vh_batch_observables"}
-    cells = (sides.astype(np.int64) ** 2)
-    batch_events_s = n / sec
-    batch_cells_s = float(np.sum(cells * nst)) / sec
-    # looped single-event FP64 baseline on a stratified sample
-    per_side = {}
-    for side in (sides_all if args.loop_per_side > 0 else []):
+    done = int(np.sum((st == 1) | (st == 2)))
+    cells = sides.astype(np.int64) ** 2
+    return {"events_per_s": done / sec, "completed": done, "failed": int(np.sum(st == 3)),
+            "running": int(np.sum(st == 0)), "frozen_out": int(np.sum(st == 1)), "tau_max": int(np.sum(st == 2)),
+            "seconds": sec, "total_steps": int(np.sum(nst)), "cell_updates": float(np.sum(cells * nst)),
+            "cell_updates_per_s": float(np.sum(cells * nst)) / sec,
+            "steps_per_event": {"mean": float(np.mean(nst)), "min": int(nst.min()), "max": int(nst.max())},
+            "graph": graph, "tuning": tuning, "autotune_ms_per_step": tune_ms, "autotune_seconds": t_tune,
+            "init_seconds": t_init, "npart_mean": float(np.mean(npart)), "clocks": clk.summary(),
+            "observables": {"eps2_initial_mean": float(np.mean(ecc2_initial)),
+                            "eps_p_final_mean": float(np.mean(eps_p_final[okev])),
+                            "corr_eps2_eps_p": float(np.corrcoef(ecc2_initial[okev], eps_p_final[okev])[0, 1])},
+            "failed_events": [int(e) for e in np.where(st == 3)[0][:64]]}
+
+
+def loop_fp64(n: int, per_side: int, floor: float) -> dict:
+    """the single-event FP64 step looped over the ensemble's events one at a
+    time, the maximum temperature read after every step as the reference's
+    main loop does (NEWEST5/main.cpp:188-205); wall seconds per event on a
+    stratified sample of `per_side` events per grid side, extrapolated by the
+    side counts"""
+    import numpy as np
+    import torch
+    from viral_b200 import configs as C
+    sides, bimp = ensemble_events(n)
+    max_steps = C.steps_between(ENS_TAU0, ENS_TAU_MAX, ENS_DTAU)
+    per = {}
+    for side in (64, 96, 128, 160, 200):
         ts = []
-        for q in range(args.loop_per_side):
-            ev = int(np.where(sides == side)[0][q]) if np.sum(sides == side) > q else q
-            c = C.glauber_config(nx=int(side), ny=int(side), boost_invariant=True)
+        for q in range(per_side):
+            idx = np.where(sides == side)[0]
+            ev = int(idx[q]) if len(idx) > q else q
+            c = C.glauber_config(nx=side, ny=side, boost_invariant=True)
             inp = C.glauber_inputs(c, b=float(bimp[ev]), seed=ev, efloor_gev=floor)
             H = C.make_hydro(c, inp)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for _ in range(max_steps):
                 H.step(1)
-                if H.max_temperature() < t_fo or H.tau >= tau_max - 1e-9:
+                if H.max_temperature() < ENS_T_FO or H.tau >= ENS_TAU_MAX - 1e-9:
                     break
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t0)
             H.close()
-        per_side[int(side)] = float(np.mean(ts))
-    loop_seconds = float(sum(per_side[int(s_)] for s_ in sides)) if per_side else float("nan")
-    out = {"metric": "events/s", "value": batch_events_s, "unit": "events/s", "n_events": n,
-           "batch_seconds": sec, "cell_updates_per_s": batch_cells_s, "graph": graph, "tuning": tuning,
-           "autotune_ms_per_step": tune_ms, "init_seconds": t_init,
-           "steps": {"mean": float(np.mean(nst)), "min": int(nst.min()), "max": int(nst.max())},
-           "stopped": {"frozen_out": int(np.sum(st == 1)), "tau_max": int(np.sum(st == 2)),
-                       "failed": int(np.sum(st == 3)), "running": int(np.sum(st == 0))},
-           "npart_mean": float(np.mean(npart)), "observables": observables,
-           "failed_events": [{"event": int(e), "side": int(sides[e]), "b": round(float(bimp[e]), 3),
-                              "steps": int(nst[e])} for e in np.where(st == 3)[0][:64]],
-           "loop_fp64": {"events_per_s": n / loop_seconds, "seconds_per_event_by_side": per_side,
-                         "sample": f"{args.loop_per_side} events per side, extrapolated by the side counts"},
-           "speedup_vs_loop_fp64": loop_seconds / sec, "clocks": clk.summary(),
-           "cpu_baseline": ensemble_cpu_baseline(args.cpu_seconds, float(np.sum(cells * nst)), n),
+        per[side] = float(np.mean(ts))
+    seconds = float(sum(per[int(s_)] for s_ in sides))
+    return {"events_per_s": n / seconds, "seconds_per_event_by_side": {str(k): v for k, v in per.items()},
+            "extrapolated_seconds": seconds,
+            "sample": f"{per_side} events per side, wall time, extrapolated by the side counts"}
+
+
+def ensemble_record(args) -> dict:
+    """c3: the batched ensemble of boost-invariant MC-Glauber events (grid side
+    from {64,96,128,160,200}, dx = 0.1 fm, b uniform in [0,12] fm, seeds
+    0..N-1, dtau = 0.02 fm/c from tau0 = 0.6 fm/c), each stopping when its
+    maximum temperature falls below 0.15 GeV or at tau = 15 fm/c; one
+    persistent kernel under a CUDA graph with the tuned variant, in mixed
+    precision and in FP64, next to the single-event FP64 step looped over the
+    events and the reference's CPU step on the host cores."""
+    from viral_b200 import configs as C
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    n = args.ensemble_events
+    floor = C.ENSEMBLE_FLOOR_GEV if args.ensemble_floor is None else args.ensemble_floor
+    mixed = batch_run(n, "mixed", floor, dev)
+    fp64 = batch_run(n, "fp64", floor, dev) if args.ensemble_fp64 else None
+    loop = loop_fp64(n, args.loop_per_side, floor) if args.loop_per_side > 0 else None
+    out = {"metric": "events/s", "value": mixed["events_per_s"], "unit": "events/s", "n_events": n,
+           "what": "completed events (frozen out or tau_max) per device second of the batched run; failed events "
+                   "(root-find or causality in the near-vacuum edge) counted apart",
+           "batch_mixed": mixed, "batch_fp64": fp64, "loop_fp64": loop,
+           "speedup_mixed_batch_vs_fp64_batch": (mixed["events_per_s"] / fp64["events_per_s"]) if fp64 else None,
+           "speedup_mixed_batch_vs_fp64_loop": (mixed["events_per_s"] / loop["events_per_s"]) if loop else None,
            "config": {"workload": "glauber ensemble", "sides": [64, 96, 128, 160, 200], "dx_fm": 0.1,
-                      "b_fm": [0, 12], "dtau_fm": dtau, "tau0_fm": tau0, "tau_max_fm": tau_max,
-                      "t_freeze_gev": t_fo, "floor_gev_fm3": floor,
-                      "precision": f"{args.ensemble_precision} (batch) / fp64 (loop)"}}
-    print(json.dumps(out), flush=True)
+                      "b_fm": [0, 12], "seeds": [0, n - 1], "dtau_fm": ENS_DTAU, "tau0_fm": ENS_TAU0,
+                      "tau_max_fm": ENS_TAU_MAX, "t_freeze_gev": ENS_T_FO, "floor_gev_fm3": floor,
+                      "eos": "synthetic table (2000 rows)", "eta_over_s": 0.08}}
+    if args.cpu_seconds > 0:
+        rates, procs, desc = reference_windows("ensemble", args.cpu_seconds, 1, reference_procs())
+        cpu_seconds_total = mixed["cell_updates"] / rates[0]
+        out["cpu_baseline"] = {"value": mixed["completed"] / cpu_seconds_total, "unit": "events/s", "cores": procs,
+                               "kind": "reference", "cell_updates_per_s": rates[0],
+                               "sample": f"{desc}, {args.cpu_seconds:.0f} s; the ensemble's "
+                                         f"{mixed['cell_updates']:.4g} cell updates at that rate; {cpu_model()}"}
+    return out
+
+
+def ensemble(args):
+    """standalone: the ensemble record alone (--ensemble N)"""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    args.ensemble_events = args.ensemble
+    print(json.dumps(ensemble_record(args)), flush=True)
 
 
 def ensemble_cpu_baseline(seconds: float, cell_steps: float, n_events: int) -> dict | None:
     """events/s of the reference's CPU step on the host cores for an ensemble
     of n_events that takes cell_steps interior cell updates in all: the
-    reference's 2+1D TVDRK2 (its boost-invariant build, 40x40 cells) timed in
-    one process per core for `seconds`, its aggregate cell-updates/s taken as
-    the rate of the ensemble's events (the step's cost per cell does not
-    depend on the grid side)"""
+    reference's boost-invariant step on windows of an ensemble event, its
+    aggregate cell-updates/s taken as the rate of the ensemble's events (the
+    step's cost per cell does not depend on the grid side)"""
     if seconds <= 0:
         return None
-    procs = reference_procs()
-    rate, cores = cpu_reference(seconds, procs, "milne_lbi")
-    return {"value": n_events * rate / cell_steps, "unit": "events/s", "cores": cores, "kind": "reference",
-            "cell_updates_per_s": rate,
-            "sample": f"{cores} processes x reference TVDRK2 (NEWEST5 headers, boost invariant, 1 MPI rank each) on "
-                      f"40x40 cells for {seconds:.0f} s, extrapolated to the ensemble's {cell_steps:.4g} cell "
-                      f"updates; {cpu_model()}"}
+    rates, cores, desc = reference_windows("ensemble", seconds, 1, reference_procs())
+    return {"value": n_events * rates[0] / cell_steps, "unit": "events/s", "cores": cores, "kind": "reference",
+            "cell_updates_per_s": rates[0], "sample": f"{desc}, {seconds:.0f} s; {cpu_model()}"}
 
 
-def adjoint_ratio(args):
-    """Discrete adjoint of the momentum anisotropy eps_p at tau = 7.2 fm/c of
-    the boost-invariant 128x128 MC-Glauber event (dx = 0.1 fm, b = 7 fm, seed
-    0, floor 0.5 GeV/fm^3; 330 steps of 0.02 fm/c from 0.6 fm/c; eta/s =
+# ---------------------------------------------------------------- adjoint
+
+
+def adjoint_record(args) -> dict:
+    """c4: discrete adjoint of the momentum anisotropy eps_p at tau = 7.2 fm/c
+    of the boost-invariant 128x128 MC-Glauber event (dx = 0.1 fm, b = 7 fm,
+    seed 0, floor 0.5 GeV/fm^3; 330 steps of 0.02 fm/c from 0.6 fm/c; eta/s =
     0.08 + 1.0 GeV^-1 max(T - 0.154 GeV, 0)), checkpoints every 25 steps, in
     FP64 and mixed precision.  The forward is vh_step(330) + vh_eps_p; the
     adjoint is one vh_adjoint_eps_p call (forward with checkpoints, segment
     recomputation, reverse steps, gradient export).  Device time from CUDA
-    events on the handle's stream, median of --steps repetitions after
-    --warmup.  The FP64 gradient is also checked against central differences
-    of the FP64 forward (h = 1e-6) along 4 seeded unit directions in e0 and
-    relative perturbations of (c0, c1)."""
+    events on the handle's stream, median of the repetitions.  Both
+    gradients are checked against central differences of the FP64 forward
+    (h = 1e-6) along seeded unit directions in e0 and relative perturbations
+    of (c0, c1)."""
     import numpy as np
     import torch
     from viral_b200 import _abi as A
@@ -543,7 +773,9 @@ def adjoint_ratio(args):
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
     nsteps = args.adjoint_steps if args.adjoint_steps > 0 else C.ADJOINT_STEPS
-    res = {}
+    reps = max(3, args.adjoint_reps)
+    res, grads = {}, {}
+    inp = None
     with ClockSampler(dev) as clk:
         modes = [("fp64", A.PREC_FP64), ("mixed", A.PREC_MIXED)]
         modes = [m_ for m_ in modes if args.adjoint_precision in ("both", m_[0])]
@@ -567,68 +799,96 @@ def adjoint_ratio(args):
                 return e0.elapsed_time(e1), out
 
             fwd, adj = [], []
-            for rep in range(args.warmup + args.steps):
+            for rep in range(2 + reps):  # two untimed warm-up repetitions
                 reinit()
                 tf, eps_f = timed(lambda: (H.step(nsteps), H.eps_p())[1])
                 reinit()
                 ta, out = timed(lambda: H.adjoint_eps_p(nsteps, args.checkpoint_every, want_state=False))
-                if rep >= args.warmup:
+                if rep >= 2:
                     fwd.append(tf)
                     adj.append(ta)
             phases = H.adjoint_phase_times()
             res[name] = {"forward_ms": statistics.median(fwd), "adjoint_ms": statistics.median(adj),
-                         "ratio": statistics.median(adj) / statistics.median(fwd), "eps_p": out[0],
+                         "ratio": statistics.median(adj) / statistics.median(fwd), "repetitions": reps,
+                         "eps_p": out[0], "eps_p_forward": eps_f,
                          "adjoint_phases_ms": {"forward_with_checkpoints": phases[0], "recompute_with_records": phases[1],
                                                "reverse": phases[2], "rest": phases[3]},
-                         "eps_p_forward": eps_f, "grad_etas": out[3].tolist(),
-                         "grad_e0_norm": float(np.linalg.norm(out[2]))}
-            if name == "fp64" and args.adjoint_fd > 0:
-                ge, gc = out[2], out[3]
-
-                def eps_of(e0, c):
-                    cfg2 = C.adjoint_config(128, prec, c[0], c[1])
-                    with C.make_hydro(cfg2, dict(inp, e=e0)) as H2:
-                        H2.step(nsteps)
-                        return H2.eps_p()
-
-                g = 134
-                m = np.zeros((g, g), bool)
-                m[3:131, 3:131] = True
-                m = m.reshape(-1)
-                rng = np.random.default_rng(1234)
-                h = 1e-6
-                c = np.array([0.08, 1.0])
-                errs = []
-                for _ in range(args.adjoint_fd):
-                    v = rng.normal(size=128 * 128)
-                    d = np.zeros_like(inp["e"])
-                    d[m] = v / np.linalg.norm(v)
-                    fd = (eps_of(inp["e"] + h * d, c) - eps_of(inp["e"] - h * d, c)) / (2 * h)
-                    errs.append(abs(float(np.dot(ge, d)) - fd) / abs(fd))
-                cerr = []
-                for k in range(2):
-                    cp = c.copy(); cm = c.copy()
-                    cp[k] *= 1 + h; cm[k] *= 1 - h
-                    fd = (eps_of(inp["e"], cp) - eps_of(inp["e"], cm)) / (2 * h * c[k])
-                    cerr.append(abs(gc[k] - fd) / abs(fd))
-                res[name]["fd_check"] = {"h": h, "e0_unit_directions_rel_err": errs, "c0_c1_rel_err": cerr}
+                         "grad_etas": out[3].tolist(), "grad_e0_norm": float(np.linalg.norm(out[2]))}
+            grads[name] = (out[2], out[3])
             H.close()
+        if args.adjoint_fd > 0 and inp is not None:
+            def eps_of(e0, c):
+                cfg2 = C.adjoint_config(128, A.PREC_FP64, c[0], c[1])
+                with C.make_hydro(cfg2, dict(inp, e=e0)) as H2:
+                    H2.step(nsteps)
+                    return H2.eps_p()
+
+            g = 134
+            m = np.zeros((g, g), bool)
+            m[3:131, 3:131] = True
+            m = m.reshape(-1)
+            rng = np.random.default_rng(1234)
+            h = 1e-6
+            c = np.array([0.08, 1.0])
+            fd_dirs, dirs = [], []
+            for _ in range(args.adjoint_fd):
+                v = rng.normal(size=128 * 128)
+                d = np.zeros_like(inp["e"])
+                d[m] = v / np.linalg.norm(v)
+                dirs.append(d)
+                fd_dirs.append((eps_of(inp["e"] + h * d, c) - eps_of(inp["e"] - h * d, c)) / (2 * h))
+            fd_c = []
+            for k in range(2):
+                cp = c.copy(); cm = c.copy()
+                cp[k] *= 1 + h; cm[k] *= 1 - h
+                fd_c.append((eps_of(inp["e"], cp) - eps_of(inp["e"], cm)) / (2 * h * c[k]))
+            for name, (ge, gc) in grads.items():
+                res[name]["fd_check"] = {
+                    "h": h, "against": "central differences of the FP64 forward",
+                    "e0_unit_directions_rel_err": [abs(float(np.dot(ge, d)) - f) / abs(f) for d, f in zip(dirs, fd_dirs)],
+                    "c0_c1_rel_err": [abs(gc[k] - fd_c[k]) / abs(fd_c[k]) for k in range(2)]}
     first = "fp64" if "fp64" in res else "mixed"
-    out = {"metric": "adjoint/forward time ratio", "value": res[first]["ratio"], "unit": "x",
-           "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-           "dtype": "f64" if first == "fp64" else "f32 (FP64 implicit-function solve)",
-           "data": "synthetic (seeded MC-Glauber initial state)", "vs_baseline": None,
-           "mixed_ratio": res["mixed"]["ratio"] if "mixed" in res else None, "detail": res, "clocks": clk.summary(),
-           "config": {"workload": "glauber_128x128 adjoint", "grid": [128, 128, 1], "b_fm": 7.0, "seed": 0,
-                      "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "tau_fm": [0.6, 0.6 + 0.02 * nsteps],
-                      "eta_over_s": "0.08 + 1.0 max(T - 0.154, 0)", "checkpoint_every": args.checkpoint_every,
-                      "observable": "eps_p"}}
+    return {"metric": "adjoint/forward time ratio", "value": res[first]["ratio"], "unit": "x",
+            "higher_is_better": False, "dtype": "f64" if first == "fp64" else "f32 (FP64 implicit-function solve)",
+            "mixed_ratio": res["mixed"]["ratio"] if "mixed" in res else None, "detail": res, "clocks": clk.summary(),
+            "config": {"workload": "glauber_128x128 adjoint", "grid": [128, 128, 1], "b_fm": 7.0, "seed": 0,
+                       "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "tau_fm": [0.6, 0.6 + 0.02 * nsteps],
+                       "eta_over_s": "0.08 + 1.0 max(T - 0.154, 0)", "checkpoint_every": args.checkpoint_every,
+                       "observable": "eps_p"}}
+
+
+def adjoint_ratio(args):
+    """standalone: the adjoint record alone (--adjoint)"""
+    out = adjoint_record(args)
+    out.update({"n_gpus": 1, "data": "synthetic (seeded MC-Glauber initial state)", "vs_baseline": None})
     print(json.dumps(out), flush=True)
 
 
 def ctypes_void_p(v):
     import ctypes
     return ctypes.c_void_p(v)
+
+
+# ---------------------------------------------------------------- arms
+
+
+def reference_arm(args, world):
+    """the reference's CPU step on the benchmarked workload (windows of its
+    Glauber state, all host cores); rank 0 only"""
+    t0 = time.perf_counter()
+    procs = reference_procs()
+    rates, procs, desc = reference_windows(args.workload, args.ref_sample_seconds, args.warmup + args.steps, procs)
+    timed = rates[args.warmup:]
+    value = statistics.mean(timed)
+    sample = f"{desc}; each step a sample of about {args.ref_sample_seconds:.1f} s per process; {cpu_model()}"
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded MC-Glauber initial state)",
+           "config": line_config(args.workload, "fp64", world),
+           "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample},
+           "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "sample_rates": timed, "wall_s": time.perf_counter() - t0}
+    print(json.dumps(out), flush=True)
 
 
 def main():
@@ -648,26 +908,8 @@ def main():
             adjoint_ratio(args)
         return
     if args.impl == "reference":
-        if rank != 0:
-            return
-        t0 = time.perf_counter()
-        procs = reference_procs()
-        rates = []
-        for s in range(args.warmup + args.steps):
-            r, _ = cpu_reference(max(1.0, args.cpu_seconds / max(1, args.steps + args.warmup)), procs)
-            if s >= args.warmup:
-                rates.append(r)
-        value = statistics.mean(rates)
-        out = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
-               "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded smooth viscous state)",
-               "config": {"workload": args.workload, "sample": "reference TVDRK2 on its compile-time 40x40x10 grid"},
-               "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference",
-                                "sample": f"{procs} processes x reference TVDRK2 (NEWEST5 headers, 1 MPI rank "
-                                          f"each) on 40x40x10 cells; {cpu_model()}"},
-               "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-               "wall_s": time.perf_counter() - t0}
-        print(json.dumps(out), flush=True)
+        if rank == 0:
+            reference_arm(args, world)
         return
 
     dist = None
@@ -677,13 +919,19 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     out = run_ours(args, rank, world, dist)
+    if rank == 0 and world == 1 and "e2e" in out:
+        subs = set(x for x in args.sub.split(",") if x and x != "none")
+        if "mixed" in subs and args.precision == "fp64":
+            out["mixed"] = mixed_record(args, out["ms_per_step"])
+        if "ensemble" in subs:
+            out["ensemble"] = ensemble_record(args)
+        if "adjoint" in subs:
+            out["adjoint"] = adjoint_record(args)
+        if args.cpu_seconds > 0:
+            rates, procs, desc = reference_windows(args.workload, args.cpu_seconds, 1, reference_procs())
+            out["cpu_baseline"] = {"value": rates[0], "unit": METRIC, "cores": procs, "kind": "reference",
+                                   "sample": f"{desc}; {args.cpu_seconds:.0f} s; {cpu_model()}"}
     if rank == 0:
-        if world == 1 and args.cpu_seconds > 0 and "e2e" in out:
-            procs = reference_procs()
-            rate, cores = cpu_reference(args.cpu_seconds, procs)
-            out["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference",
-                                   "sample": f"{cores} processes x reference TVDRK2 (NEWEST5 headers, 1 MPI rank "
-                                             f"each) on 40x40x10 cells for {args.cpu_seconds:.0f} s; {cpu_model()}"}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

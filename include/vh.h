@@ -259,23 +259,25 @@ int vh_last_iterations(vh_handle* h, long long* iters);
 
 /* Step without allocating: the FP64 step of vh_step on device memory the
  * caller owns, for callers that must not call cudaMalloc where they step the
- * fluid (a device memory pool owned by another framework, or launches being
- * recorded into a CUDA stream capture).  No counterpart in the reference,
+ * fluid (a device memory pool owned by another framework, whose budget a
+ * cudaMalloc behind its back would break).  No counterpart in the reference,
  * which steps host memory it allocated itself.
  *   state:   device pointer to the 18 canonical fields (18 x G doubles),
  *            read and advanced in place by nsteps steps from tau
  *   eos_dev: device copy of the EOS table [e | P | cs2 | T] (4 x eos_n
  *            doubles) when cfg->eos_kind is VH_EOS_TABLE, else NULL;
- *            cfg->eos_e must still point to the host table
+ *            cfg->eos_e must still point to the host table (positive and
+ *            strictly increasing)
  *   stream:  cudaStream_t to launch on (NULL: the legacy stream)
  * cfg->precision must be VH_PREC_FP64, cfg->taupi_kind one of the two
- * eta-proportional forms, cfg->cold_plasma 0, and the ghost-inclusive grid
- * at most VH_STATIC_MAX_CELLS cells, else VH_E_ARG.  The step's scratch is one
- * file-scope device array of 16 MiB that every GPU loading the library holds
- * until exit; all calls share it and it keeps the last call's contents, so
- * calls that overlap on the GPU race (issue them one after another).  The
- * first call on a device looks up that array's address; make it before any
- * stream capture begins.  Returns as vh_step, after synchronising stream. */
+ * eta-proportional forms, cfg->cold_plasma 0, tau > 0 on Milne grids, and the
+ * ghost-inclusive grid at most VH_STATIC_MAX_CELLS cells, else VH_E_ARG.  The
+ * step's scratch is one file-scope device array of 16 MiB that every GPU
+ * loading the library holds until exit; all calls share it and it keeps the
+ * last call's contents, so calls that overlap on the GPU race (issue them one
+ * after another).  The first call on a device looks up that array's address.
+ * Each call copies its status word to the host and synchronises stream before
+ * it returns; the return codes are vh_step's. */
 #define VH_STATIC_MAX_CELLS 61680
 int vh_step_static(const vh_config* cfg, double* state, const double* eos_dev, double tau, int nsteps,
                    void* stream);

@@ -228,6 +228,14 @@ class RefBuild:
         self.dx, self.dy, self.dz, self.factor, self.gevfm = list(c)
         self.n = self.gx * self.gy * self.gz
 
+    def set_eos_table(self, table):
+        """the run-time EOS table (4, n: e, P, cs2, T) of the table-EOS
+        builds (libref_window_*.so)"""
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        self.L.ref_set_eos_table.argtypes = [ctypes.c_int, _dp]
+        if self.L.ref_set_eos_table(t.shape[1], _ptr(t)) != 0:
+            raise ValueError("bad EOS table")
+
     def coords(self):
         x = np.zeros(self.n); y = np.zeros(self.n); e = np.zeros(self.n)
         self.L.ref_coords(_ptr(x), _ptr(y), _ptr(e))

@@ -18,7 +18,10 @@
  *
  * The scenario (grid, dx, EOS, transport) is the reference's compile-time
  * block selected by -D flags; ZCM/ZCMA, which NEWEST5's default block leaves
- * undefined, are passed on the command line.
+ * undefined, are passed on the command line.  With -DGINIT -DVH_REF_EOS_TABLE
+ * the GINIT block (30 x 30 cells of 0.1 fm per rank, eta = s/4pi,
+ * tau_pi = 1.5 eta/P) runs on a tabulated EOS set at run time
+ * (ref_shim/eos_table_s95p.h): the windows of the benchmark workloads.
  *
  * Canonical state layout shared with the oracle: structure of arrays over
  * the ghost-inclusive grid, index (k*YCM + j)*XCM + i (x fastest).
@@ -42,6 +45,10 @@
 using namespace std;
 
 #ifdef VH_REF_TXYZ5
+#include "maindef.h"
+#elif defined(VH_REF_EOS_TABLE)
+/* the GINIT block's EOS hooks on a run-time table instead of s95p */
+#include "eos_table_s95p.h"
 #include "maindef.h"
 #else
 #include "s95p.h"

@@ -44,7 +44,9 @@ def gpu_available() -> bool:
 
 
 def pytest_collection_modifyitems(config, items):
-    items.sort(key=lambda it: 1 if "late" in it.keywords else 0)  # stable: file order otherwise
+    # stable: file order otherwise; the allocation-free step's file runs after everything, late tests included
+    items.sort(key=lambda it: 2 if os.path.basename(str(it.fspath)).startswith("test_zz_")
+               else (1 if "late" in it.keywords else 0))
     if gpu_available():
         return
     skip = pytest.mark.skip(reason="no CUDA GPU in this environment")

@@ -8,9 +8,10 @@ import shutil
 import subprocess
 
 import pytest
+from refpath import reference_root  # oracle/ is on sys.path via conftest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("VH_REFERENCE", "/root/reference")
+REF = reference_root()
 
 PRELUDE = """#include <cstdio>
 #include <cstdlib>

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from viral_b200 import _abi as A
+from refpath import reference_root  # noqa: E402  (oracle/ is on sys.path via conftest)
 from viral_b200.hydro import read_ideal_profile
 
 
@@ -56,7 +57,7 @@ def test_reader_errors(tmp_path):
         read_ideal_profile(str(tmp_path / "missing.dat"), p, p, 2, 2)
 
 
-REF_INIT = "/root/reference/NEWideal/init"
+REF_INIT = os.path.join(reference_root(), "NEWideal", "init")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_INIT), reason="the reference tree is not present")

@@ -2,78 +2,135 @@
 
 vh_step_static serves callers that must not call cudaMalloc where they
 advance the fluid: a code whose device memory belongs to another framework's
-pool, or one recording its launches into a CUDA stream capture.  They own
-the state and lend it to the call; the step's scratch sits in a static
-device array inside the library.  This file runs last so that a failure here
-leaves every other test already run.
+pool allocator, where an allocation behind the pool's back would break the
+budget it was given.  They own the state and lend it to the call; the step's
+scratch sits in a static device array inside the library.  This file runs
+last so that a failure here leaves every other test already run.
 
 Two calls in a row on the same state must match two vh_step calls on a
 handle, to the FP64 tolerance of the other GPU tests (1e-12 relative), for
-both EOS kinds; the first call's leftovers in the shared scratch must not
-leak into the second.
+boost-invariant and 3+1D Milne grids, a Cartesian grid, both EOS kinds and a
+grid of exactly the largest size; the first call's leftovers in the shared
+scratch must not leak into the second, and the second call must leave the
+device's free memory unchanged.
 """
 import ctypes
+import os
+import sys
 
 import numpy as np
 import pytest
 
-from conftest import rel_err
-from viral_b200 import _abi as A
-from viral_b200 import configs as C
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from conftest import rel_err  # noqa: E402
+from helpers import smooth_inputs  # noqa: E402
+from viral_b200 import _abi as A  # noqa: E402
+from viral_b200 import configs as C  # noqa: E402
+from viral_b200.hydro import Config, Hydro  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
+MAX_CELLS = 61680  # VH_STATIC_MAX_CELLS in include/vh.h
 
 
-def _run_pair(cfg, inp, steps=(3, 2)):
+def _static(cfg, dev, eos_dev, tau, n, stream):
+    c = cfg.to_c()
+    return A.lib().vh_step_static(ctypes.byref(c), ctypes.c_void_p(dev.data_ptr()),
+                                  ctypes.c_void_p(eos_dev.data_ptr()) if eos_dev is not None else None,
+                                  tau, n, ctypes.c_void_p(stream))
+
+
+def _run_pair(cfg, f0, tau0, steps=(3, 2)):
+    """vh_step on a handle and vh_step_static on a device copy of the same
+    18-field state, `steps` steps per call; also the device's free memory
+    before and after the second static call"""
     import torch
-    with C.make_hydro(cfg, inp) as H:
-        f0 = H.get_state()
-        tau0 = H.tau
+    with Hydro(cfg) as H:
+        H.set_state(f0, tau0)
         ref = []
         for n in steps:
             H.step(n)
             ref.append(H.get_state())
-    dev = torch.from_numpy(f0.reshape(-1).copy()).cuda()
+    dev = torch.from_numpy(np.ascontiguousarray(f0).reshape(-1).copy()).cuda()
     eos_dev = None
     if cfg.eos_kind == A.EOS_TABLE:
         eos_dev = torch.from_numpy(np.ascontiguousarray(cfg.eos_table).reshape(-1).copy()).cuda()
-    c = cfg.to_c()
     stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
     tau = tau0
-    got = []
-    for n in steps:
-        rc = A.lib().vh_step_static(ctypes.byref(c), ctypes.c_void_p(dev.data_ptr()),
-                                    ctypes.c_void_p(eos_dev.data_ptr()) if eos_dev is not None else None,
-                                    tau, n, ctypes.c_void_p(stream))
+    got, free = [], []
+    for q, n in enumerate(steps):
+        if q == len(steps) - 1:
+            free.append(torch.cuda.mem_get_info()[0])
+        rc = _static(cfg, dev, eos_dev, tau, n, stream)
         assert rc == A.OK, A.STATUS_NAMES.get(rc, rc)
+        if q == len(steps) - 1:
+            free.append(torch.cuda.mem_get_info()[0])
         tau += n * cfg.dtau
         got.append(dev.cpu().numpy().reshape(A.NFIELDS, -1).copy())
-    return ref, got
+    return ref, got, free
 
 
-@pytest.mark.parametrize("which", ["gubser", "glauber_table"])
-def test_static_step_matches_handle_step_twice(which):
+def _from_inputs(cfg, inp):
+    with C.make_hydro(cfg, inp) as H:
+        return H.get_state(), H.tau
+
+
+def _case(which):
     if which == "gubser":
         cfg = C.gubser_config(nx=65, ny=65)
-        inp = C.gubser_inputs(cfg)
-    else:
+        return (cfg, *_from_inputs(cfg, C.gubser_inputs(cfg)))
+    if which == "glauber_table":
         cfg = C.glauber_config(nx=96, ny=96, boost_invariant=True)
-        inp = C.glauber_inputs(cfg, b=5.0, seed=4)
-    ref, got = _run_pair(cfg, inp)
+        return (cfg, *_from_inputs(cfg, C.glauber_inputs(cfg, b=5.0, seed=4)))
+    if which == "glauber_3d_table":
+        cfg = C.glauber_config(nx=24, ny=22, nz=12)
+        return (cfg, *_from_inputs(cfg, C.glauber_inputs(cfg, b=5.0, seed=2)))
+    if which == "cartesian_3d":
+        cfg = Config(nx=20, ny=18, nz=12, boost_invariant=False, coords=A.COORD_CARTESIAN, dx=0.1, dy=0.1, dz=0.1,
+                     tau0=1.0, dtau=0.01, eos_kind=A.EOS_CONFORMAL, eos_a=13.899692864867510, etas0=1 / (4 * np.pi))
+        return cfg, smooth_inputs(cfg, cfg.tau0, seed=5), cfg.tau0
+    if which == "largest_grid":
+        # 240 x 257 ghost-inclusive cells: exactly VH_STATIC_MAX_CELLS
+        cfg = C.glauber_config(nx=234, ny=251, boost_invariant=True)
+        return (cfg, *_from_inputs(cfg, C.glauber_inputs(cfg, b=3.0, seed=1)))
+    raise ValueError(which)
+
+
+@pytest.mark.parametrize("which", ["gubser", "glauber_table", "glauber_3d_table", "cartesian_3d", "largest_grid"])
+def test_static_step_matches_handle_step_twice(which):
+    cfg, f0, tau0 = _case(which)
+    gx, gy, gz = cfg.gdims()
+    assert gx * gy * gz <= MAX_CELLS
+    ref, got, free = _run_pair(cfg, f0, tau0)
     for r, g in zip(ref, got):
         for q in range(A.NFIELDS):
             assert rel_err(g[q], r[q]) <= TOL, f"field {q}"
+    assert free[0] == free[1], f"device free memory changed by {free[0] - free[1]} bytes"
 
 
-def test_static_step_rejects_oversized_and_mixed():
+def test_static_step_rejects_bad_arguments():
     import torch
-    big = C.glauber_config(nx=161, ny=161, nz=41)
-    c = big.to_c()
     buf = torch.zeros(8, dtype=torch.float64, device="cuda")
-    rc = A.lib().vh_step_static(ctypes.byref(c), ctypes.c_void_p(buf.data_ptr()), None, 0.6, 1, None)
-    assert rc == A.E_ARG
-    mixed = C.gubser_config(nx=33, ny=33, precision=A.PREC_MIXED).to_c()
-    rc = A.lib().vh_step_static(ctypes.byref(mixed), ctypes.c_void_p(buf.data_ptr()), None, 1.0, 1, None)
-    assert rc == A.E_ARG
+    tab = torch.zeros(8, dtype=torch.float64, device="cuda")
+
+    def rc(cfg, tau=0.6, eos=None):
+        c = cfg.to_c()
+        return A.lib().vh_step_static(ctypes.byref(c), ctypes.c_void_p(buf.data_ptr()),
+                                      ctypes.c_void_p(eos.data_ptr()) if eos is not None else None, tau, 1, None)
+
+    # 87 x 709 = 61683 ghost-inclusive cells, the smallest grid above the limit
+    assert rc(C.glauber_config(nx=81, ny=703, boost_invariant=True), eos=tab) == A.E_ARG
+    assert rc(C.glauber_config(nx=161, ny=161, nz=41), eos=tab) == A.E_ARG
+    assert rc(C.gubser_config(nx=33, ny=33, precision=A.PREC_MIXED), tau=1.0) == A.E_ARG
+    # Milne sources divide by tau
+    g = C.gubser_config(nx=33, ny=33)
+    assert rc(g, tau=0.0) == A.E_ARG
+    assert rc(g, tau=-1.0) == A.E_ARG
+    # the table lookup needs increasing energy densities
+    t = C.glauber_config(nx=20, ny=20, boost_invariant=True)
+    bad = np.array(t.eos_table, copy=True)
+    bad[0, 10] = bad[0, 9]
+    t.eos_table = bad
+    assert rc(t, eos=tab) == A.E_ARG

@@ -592,8 +592,14 @@ extern "C" int vh_batch_run(vh_batch* b, int max_steps, double* seconds, int* gr
       if ((rc = launch(b, b->variant, s, k))) break;
       done_steps += k;
     }
+    // the running count and the sticky barrier time-out flag together: after
+    // a time-out every later launch returns at its first barrier, so the
+    // loop stops at once instead of launching until max_steps
+    unsigned int flag = 0;
     if (cudaMemcpyAsync(&running, b->d_running, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(&flag, b->d_bar + 2, sizeof(flag), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) { rc = VH_E_CUDA; b->err = cudaGetErrorString(cudaGetLastError()); break; }
+    if (flag) break;
   }
   cudaEventRecord(e1, s);
   cudaEventSynchronize(e1);

@@ -3,13 +3,12 @@
 // allocates nothing.
 //
 // Who needs it: callers that must not call cudaMalloc on the device at the
-// point where they step the fluid.  Typical cases are a host code whose
-// device memory is owned by another framework's pool allocator (cudaMalloc
-// behind its back fragments or exceeds the pool's budget), and a host code
-// that records its launches into a CUDA stream capture, where allocation
-// calls are not allowed.  Such a caller keeps the 18-field state in memory
-// it owns and lends it to this call; the scratch the step needs (the stage-1
-// conserved set, the RK2 buffer, the flux-divergence and velocity-gradient
+// point where they step the fluid.  The typical case is a host code whose
+// device memory is owned by another framework's pool allocator: a cudaMalloc
+// behind the pool's back fragments the device or exceeds the budget the pool
+// was given.  Such a caller keeps the 18-field state in memory it owns and
+// lends it to this call; the scratch the step needs (the stage-1 conserved
+// set, the RK2 buffer, the flux-divergence and velocity-gradient
 // accumulators and two status words) lives in g_vh_static_scratch below.
 //
 // Limits and sharing rules:
@@ -23,8 +22,10 @@
 //    them one after another.
 //  - The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current) and sets the kernels'
-//    shared-memory attributes; make that first call before any stream
-//    capture begins.
+//    shared-memory attributes.
+//  - Each call ends by copying the status word to the host and
+//    synchronising the stream it was given, so it returns only once its
+//    steps have finished on the GPU.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -66,8 +67,11 @@ int static_setup(int dev, double** out) {
   return VH_OK;
 }
 
-int fill_cfg(const vh_config* c, const double* eos_dev, DevCfg& C) {
+int fill_cfg(const vh_config* c, const double* eos_dev, double tau, DevCfg& C) {
   if (!c || c->precision != VH_PREC_FP64) return VH_E_ARG;
+  // Milne sources divide by tau (the time is a call argument here, not
+  // cfg->tau0)
+  if (!std::isfinite(tau) || (c->coords == VH_COORD_MILNE && !(tau > 0))) return VH_E_ARG;
   if (c->coords != VH_COORD_MILNE && c->coords != VH_COORD_CARTESIAN) return VH_E_ARG;
   if (c->recon != VH_RECON_WENO5 && c->recon != VH_RECON_MINMOD) return VH_E_ARG;
   if (c->nx < 3 || c->ny < 3 || (!c->boost_invariant && c->nz < 3) || (c->boost_invariant && c->nz != 1)) return VH_E_ARG;
@@ -93,6 +97,9 @@ int fill_cfg(const vh_config* c, const double* eos_dev, DevCfg& C) {
     if (!(c->eos_a > 0)) return VH_E_ARG;
   } else if (c->eos_kind == VH_EOS_TABLE) {
     if (c->eos_n < 2 || !c->eos_e || !eos_dev) return VH_E_ARG;
+    // the table lookup brackets e by its logarithm: the rows must increase
+    for (int i = 1; i < c->eos_n; i++)
+      if (!(c->eos_e[i] > c->eos_e[i - 1]) || !(c->eos_e[i - 1] > 0)) return VH_E_ARG;
     C.eos_n = c->eos_n;
     C.eos_l0 = std::log(c->eos_e[0]);
     C.eos_idl = (c->eos_n - 1) / (std::log(c->eos_e[c->eos_n - 1]) - C.eos_l0);
@@ -129,7 +136,7 @@ extern "C" int vh_step_static(const vh_config* cfg, double* state, const double*
                               void* stream) {
   DevCfg C;
   if (!state || nsteps < 0) return VH_E_ARG;
-  if (fill_cfg(cfg, eos_dev, C) != VH_OK) return VH_E_ARG;
+  if (fill_cfg(cfg, eos_dev, tau, C) != VH_OK) return VH_E_ARG;
   if (C.n > kStaticCells) return VH_E_ARG;  // grid larger than the static scratch
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return VH_E_CUDA;
