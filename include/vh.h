@@ -477,6 +477,23 @@ int vh_cooper_frye_3d_device(const double* elements, long long count, double t_f
  * q = 1/fm, b = 1.21. */
 int vh_profile_gubser_cold(int nx, int ny, double dx, double dy, double q, double tau0, double dtau, double b,
                            double a, double* e, double* ux, double* uy, double* pi5, double* prevu4);
+/* Israel-Stewart Gubser flow (the reference's viscous Gubser test, whose
+ * initial table init/tempbin-23F.dat it reads at NEWEST5/init.h:419-459 and
+ * does not ship): conformal e = a T^4, eta/s constant, tau_pi = 5 eta/(e+P)
+ * (NEWEST5/maindef.h:338-339).  T^ = tau T and P = tau^2 pi^{eta eta}/(e+P)
+ * solve, in the de Sitter time rho (sinh rho = -(1 - q^2 tau^2 +
+ * q^2 r^2)/(2 q tau)),
+ *   d ln T^/d rho = -(2/3) tanh rho + (1/3) P tanh rho,
+ *   dP/d rho = -(4/3) P^2 tanh rho - P T^/(5 eta/s) + (4/15) tanh rho,
+ * fixed by T = t0_gev and P = p0 at the grid centre at tau0 (RK4, step 1e-3
+ * in rho).  Writes e, u^x, u^y (Gubser velocity) and pi5 (xx, yy, xy,
+ * x-eta, y-eta: w P along eta, -w P/2 along the two transverse rest-frame
+ * directions) at tau0 and prevu4 at tau0 - dtau on the 2+1D ghost-inclusive
+ * grid.  The reference's shipped table (init/tempbin-8.7z: q = 1/fm,
+ * T = 1.2 fm^-1 and P = 0 at tau0 = 1 fm/c, eta/s = 0.2) is this solution. */
+int vh_profile_gubser_is(int nx, int ny, double dx, double dy, double q, double tau0, double dtau, double t0_gev,
+                         double p0, double etas, double a, double hbarc, double* e, double* ux, double* uy,
+                         double* pi5, double* prevu4);
 /* Monte-Carlo Glauber energy density (two Woods-Saxon nuclei): A nucleons
  * per nucleus, radius R, diffuseness aws, hard core dmin, impact parameter
  * b, sigma_nn (fm^2), Gaussian width w per participant, peak e in GeV/fm^3,

@@ -6,6 +6,10 @@
  * that the oracle and the compiled reference agree to a few ulps; the
  * Israel-Stewart source is our own covariant derivation (the reference
  * evaluates machine-generated polynomials of the same expression).
+ *
+ * The cell loops run on OpenMP threads (OMP_NUM_THREADS): every cell is
+ * written by one thread and nothing is summed across cells in floating
+ * point, so the results do not depend on the number of threads.
  */
 #include "oracle.h"
 
@@ -286,6 +290,7 @@ static void centre_flux(const vho_grid* g, size_t c, double tau, double* fx, dou
 /* Var = tau T^{tau mu} and pi on every cell (NEWEST5/hydroKT.h:349-367) */
 static void fill_var(vho_grid* g, double tau) {
   const double tf = g->c.cartesian ? 1.0 : tau;
+#pragma omp parallel for schedule(static)
   for (size_t c = 0; c < g->n; c++) {
     for (int l = 0; l < 4; l++) g->var[l * g->n + c] = g->c.cartesian ? g->f[F_T + l][c] : tf * g->f[F_T + l][c];
     for (int l = 0; l < 5; l++) g->var[(4 + l) * g->n + c] = g->f[F_PI + l][c];
@@ -314,7 +319,10 @@ static void kt_direction(vho_grid* g, int dir, double tau) {
   (void)n_along;
   const double* F = g->flux + (size_t)dir * 9 * g->n;
   const double* A = g->spd + (size_t)dir * g->n;
+#pragma omp parallel
+  {
   double* H = (double*)malloc(sizeof(double) * 9 * (hi - lo + 1));
+#pragma omp for collapse(2) schedule(static)
   for (int b = o2lo; b < o2hi; b++)
     for (int a = o1lo; a < o1hi; a++) {
       size_t base = (size_t)a * s1 + (size_t)b * s2;
@@ -357,12 +365,14 @@ static void kt_direction(vho_grid* g, int dir, double tau) {
       }
     }
   free(H);
+  }
 }
 
 /* centre fluxes on every cell, speeds on the interior only, Var, and the
  * flux divergence summed over the directions (NEWEST5/hydroKT.h:391-421) */
 static void hydro_explicit(vho_grid* g, double tau) {
   const int cart = g->c.cartesian;
+#pragma omp parallel for schedule(static)
   for (size_t c = 0; c < g->n; c++) {
     double fx[9], fy[9], fz[9];
     centre_flux(g, c, tau, fx, fy, fz);
@@ -373,6 +383,7 @@ static void hydro_explicit(vho_grid* g, double tau) {
     }
   }
   memset(g->spd, 0, sizeof(double) * 3 * g->n);
+#pragma omp parallel for collapse(2) schedule(static)
   for (int k = g->kl; k < g->kr; k++)
     for (int j = g->jl; j < g->jr; j++)
       for (int i = g->il; i < g->ir; i++) {
@@ -398,6 +409,7 @@ static void hydro_explicit(vho_grid* g, double tau) {
  * which is zero unless set by an earlier call. */
 static void calc_du(vho_grid* g, double ts) {
   const size_t n = g->n;
+#pragma omp parallel for collapse(3) schedule(static)
   for (int l = 0; l < 4; l++)
     for (int k = g->kl; k < g->kr; k++)
       for (int j = g->jl; j < g->jr; j++)
@@ -407,6 +419,7 @@ static void calc_du(vho_grid* g, double ts) {
         }
   for (int l = 0; l < 4; l++) {
     const double* u = g->f[F_U0 + l];
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = g->kl; k < g->kr; k++)
       for (int j = g->jl; j < g->jr; j++)
         for (int i = 2; i < g->gx - 2; i++) {
@@ -414,6 +427,7 @@ static void calc_du(vho_grid* g, double ts) {
           double q[5] = {u[c - 2], u[c - 1], u[c], u[c + 1], u[c + 2]};
           g->du[(size_t)(l * 4 + 1) * n + c] = weno_der(q, g->c.dx);
         }
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = g->kl; k < g->kr; k++)
       for (int i = g->il; i < g->ir; i++)
         for (int j = 2; j < g->gy - 2; j++) {
@@ -425,6 +439,7 @@ static void calc_du(vho_grid* g, double ts) {
     if (!g->c.boost_invariant) {
       size_t s = (size_t)g->gx * g->gy;
       int Z = g->gz;
+#pragma omp parallel for collapse(2) schedule(static)
       for (int i = g->il; i < g->ir; i++)
         for (int j = g->jl; j < g->jr; j++)
           for (int k = 0; k < Z; k++) {
@@ -549,6 +564,7 @@ static void calc_source(vho_grid* g, double tau, double ts) {
   const vho_config* C = &g->c;
   const size_t n = g->n;
   calc_du(g, ts);
+#pragma omp parallel for collapse(2) schedule(static)
   for (int k = g->kl; k < g->kr; k++)
     for (int j = g->jl; j < g->jr; j++)
       for (int i = g->il; i < g->ir; i++) {
@@ -704,6 +720,8 @@ static int root_find(vho_grid* g, double tau) {
   const vho_config* C = &g->c;
   double t2 = C->cartesian ? 1.0 : tau * tau;
   int status = 0;
+  long long iters = 0;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4) reduction(|:status) reduction(+:iters)
   for (int k = g->kl; k < g->kr; k++)
     for (int j = g->jl; j < g->jr; j++)
       for (int i = g->il; i < g->ir; i++) {
@@ -714,7 +732,7 @@ static int root_find(vho_grid* g, double tau) {
         x[0] = g->f[F_E][c]; x[1] = g->f[F_U0 + 1][c]; x[2] = g->f[F_U0 + 2][c]; x[3] = g->f[F_U0 + 3][c];
         int it = vho_con2prim(g, Tt, p, tau, x);
         if (it < 0) { status |= 1; continue; }
-        g->iters += it;
+        iters += it;
         double u1 = x[1], u2 = x[2], u3 = x[3];
         double u0 = sqrt(1 + u1 * u1 + u2 * u2 + u3 * u3 * (C->cartesian ? 1.0 : tau) * (C->cartesian ? 1.0 : tau));
         g->f[F_E][c] = x[0];
@@ -722,6 +740,7 @@ static int root_find(vho_grid* g, double tau) {
         double vx = u1 / u0, vy = u2 / u0, ve = u3 / u0;
         if (sqrt(vx * vx + vy * vy + t2 * ve * ve) >= 1 || x[0] <= 0) status |= 2;
       }
+  g->iters += iters;
   return status;
 }
 
@@ -778,6 +797,7 @@ static void stage_rhs(vho_grid* g, double tau, double ts) {
 
 static void unpack_var(vho_grid* g, const double* v, double tau) {
   const size_t n = g->n;
+#pragma omp parallel for collapse(2) schedule(static)
   for (int k = g->kl; k < g->kr; k++)
     for (int j = g->jl; j < g->jr; j++)
       for (int i = g->il; i < g->ir; i++) {
@@ -795,6 +815,7 @@ int vho_step(vho_grid* g, double tau, double ts) {
   g->iters = 0;
   double t1 = tau + ts;
   stage_rhs(g, tau, ts);
+#pragma omp parallel for collapse(2) schedule(static)
   for (int k = g->kl; k < g->kr; k++)
     for (int j = g->jl; j < g->jr; j++)
       for (int i = g->il; i < g->ir; i++) {
@@ -816,6 +837,7 @@ int vho_step(vho_grid* g, double tau, double ts) {
   status |= root_find(g, t1);
   vho_boundary(g);
   stage_rhs(g, t1, ts);
+#pragma omp parallel for collapse(2) schedule(static)
   for (int k = g->kl; k < g->kr; k++)
     for (int j = g->jl; j < g->jr; j++)
       for (int i = g->il; i < g->ir; i++) {

@@ -19,7 +19,8 @@ shock tube of its default TXYZ5 block) after 20 steps; a sixth, ns10_lbi,
 is NEWEST10's ten-component Navier-Stokes shear tensor (CalcNS); a
 seventh, bjorken, is the reference's Bjorken scenario run to tau = 10; an
 eighth, cgc, the reference's Glasma initialisation (ginit.h) on one rank's
-window.  The CPU tests
+window; a ninth, gubser_is_table, cells of the reference's shipped viscous
+Gubser initial table (NEWEST5/init/tempbin-8.7z).  The CPU tests
 rebuild the same inputs and check the oracle against these numbers.
 """
 from __future__ import annotations
@@ -260,9 +261,85 @@ def make_ns10() -> dict:
             "ns": ns[:, cells], "du": du[:, cells], "ns_sum": ns[:, inner].sum(axis=1)}
 
 
+def make_gubser_is_table() -> dict:
+    """The reference's shipped Gubser initial table, NEWEST5/init/tempbin-8.7z
+    (a 7-zip archive of one LZMA stream holding tempbin-8.dat: 326 x 326 cells
+    x 8 doubles, the layout initGubser reads at NEWEST5/init.h:419-459: T,
+    then pi^{tau tau}, pi^{tau x}, pi^{tau y}, pi^{xx}, pi^{xy}, pi^{yy},
+    tau^2 pi^{eta eta}).  The archive's own headers are parsed here (the
+    signature header, then the uncompressed header: one packed stream, one
+    LZMA coder with its 5 property bytes) and the stream is decoded with the
+    standard library's raw LZMA1 decoder; the CRC32 of the result is checked
+    against the archive's.  Kept: the cells of the positive x axis and of the
+    diagonal from the centre (163, 163), and a seeded sample."""
+    import lzma
+    import struct
+    import zlib
+    from refpath import reference_root
+    path = os.path.join(reference_root(), "NEWEST5", "init", "tempbin-8.7z")
+    with open(path, "rb") as fh:
+        d = fh.read()
+    assert d[:6] == b"7z\xbc\xaf\x27\x1c"
+    next_off, next_size, _ = struct.unpack("<QQI", d[12:32])
+    hdr = d[32 + next_off:32 + next_off + next_size]
+
+    def num(b, k):  # the archive's variable-length integer at offset k
+        first, mask, extra = b[k], 0x80, 0
+        while extra < 8 and first & mask:
+            extra += 1
+            mask >>= 1
+        val = int.from_bytes(b[k + 1:k + 1 + extra], "little")
+        if extra < 8:
+            val |= (first & (mask - 1)) << (8 * extra)
+        return val, k + 1 + extra
+
+    # kHeader, kMainStreamsInfo, kPackInfo: pack position, one stream, its size
+    assert hdr[0:3] == bytes([0x01, 0x04, 0x06])
+    pack_pos, k = num(hdr, 3)
+    nstreams, k = num(hdr, k)
+    assert nstreams == 1 and hdr[k] == 0x09
+    pack_size, k = num(hdr, k + 1)
+    assert hdr[k] == 0x00 and hdr[k + 1] == 0x07 and hdr[k + 2] == 0x0B  # end, kUnpackInfo, kFolder
+    k += 3
+    nfolders, k = num(hdr, k)
+    assert nfolders == 1 and hdr[k] == 0 and hdr[k + 1] == 1  # not external, one coder
+    flags = hdr[k + 2]
+    idlen = flags & 0x0F
+    coder = hdr[k + 3:k + 3 + idlen]
+    assert coder == bytes([0x03, 0x01, 0x01]) and flags & 0x20  # LZMA, with properties
+    k += 3 + idlen
+    nprops, k = num(hdr, k)
+    props = hdr[k:k + nprops]
+    k += nprops
+    assert hdr[k] == 0x0C  # kCodersUnpackSize
+    unpack_size, k = num(hdr, k + 1)
+    # end of the unpack info, then kSubStreamsInfo: kCRC, all defined, CRC32
+    assert hdr[k] == 0x00 and hdr[k + 1] == 0x08 and hdr[k + 2] == 0x0A and hdr[k + 3] == 1
+    crc = struct.unpack("<I", hdr[k + 4:k + 8])[0]
+    lc, rem = props[0] % 9, props[0] // 9
+    lp, pb = rem % 5, rem // 5
+    dict_size = int.from_bytes(props[1:5], "little")
+    dec = lzma.LZMADecompressor(format=lzma.FORMAT_RAW,
+                                filters=[{"id": lzma.FILTER_LZMA1, "dict_size": dict_size, "lc": lc, "lp": lp,
+                                          "pb": pb}])
+    raw = dec.decompress(d[32 + pack_pos:32 + pack_pos + pack_size], max_length=unpack_size)
+    assert len(raw) == unpack_size and zlib.crc32(raw) == crc
+    g = int(round(math.sqrt(len(raw) // 64)))
+    t = np.frombuffer(raw, dtype="<f8").reshape(g, g, 8)  # [j][i][column]
+    c = g // 2
+    ii = list(range(c, g)) + list(range(c, g))
+    jj = [c] * (g - c) + list(range(c, g))
+    rng = np.random.default_rng(5)
+    ii += list(rng.integers(0, g, 64))
+    jj += list(rng.integers(0, g, 64))
+    ii, jj = np.array(ii), np.array(jj)
+    return {"i": ii, "j": jj, "values": t[jj, ii, :].copy(), "dims": np.array([g, g]),
+            "note": np.array("NEWEST5/init/tempbin-8.7z: T, pi^tt, pi^tx, pi^ty, pi^xx, pi^xy, pi^yy, tau^2 pi^ee")}
+
+
 def main():
     special = {"cart_3d_shock": make_shock, "ns10_lbi": make_ns10, "bjorken": make_bjorken, "cgc": make_cgc,
-               "cart_bjorken": make_cart_bjorken}
+               "cart_bjorken": make_cart_bjorken, "gubser_is_table": make_gubser_is_table}
     which = sys.argv[1:] or list(SCENARIOS) + list(special)
     for v in which:
         d = special[v]() if v in special else make(v)

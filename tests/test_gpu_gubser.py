@@ -1,0 +1,129 @@
+"""The boost-invariant Gubser test on the GPU, over its full length.
+
+* c0 as specified (129 x 129 cells of 0.1 fm, ideal Gubser T with T(0,0) =
+  0.6 GeV and Navier-Stokes pi at tau0 = 1 fm/c, eta/s = 0.2, tau_pi = 5
+  eta/(e+P), mirrored ghosts): all 300 steps to tau = 4 fm/c against the
+  oracle at 1e-10 (tests/test_gpu_parity.py holds the first 50).
+* The semi-analytic Israel-Stewart solution (oracle/gubser_is.py, pinned to
+  the reference's shipped table by tests/test_gubser_is_cpu.py): the same
+  cells, time step and physics started from the solution the reference's
+  table holds (T = 1.2 fm^-1 and P = 0 at the centre at tau0 = 1 fm/c), on
+  the table's 16 fm box; on c0's own 12.8 fm box the solution's corners (flow
+  velocity near 1, P near 0.55) fail the root-find at tau = 3.55 fm/c in the
+  oracle.  At tau = 4 fm/c the GPU state equals the oracle's to 1e-10, and T
+  and the shear ratio P = tau^2 pi^{eta eta}/(e + P) follow the ODE: within
+  2 fm of the centre to 1.7e-3 in T and 4e-4 in P (measured with the
+  oracle); in the ring 2-5 fm out, where the flow reaches u^r = 4 and T
+  rises by half across 1 fm, to 8 % in T and 6 % in P, which is the 0.1 fm
+  grid's error: at tau = 2.9 fm/c halving the cells (and the step) brings the
+  worst error within 5 fm from 1.6e-2 to 7.8e-4 in T and from 1.6e-2 to
+  1.2e-3 in P.
+Late: newer than the rest of the GPU suite."""
+import numpy as np
+import pytest
+
+from gubser_is import GubserIS, milne_fields
+from helpers import canonical_state, interior_mask, oracle_config, oracle_from_inputs
+from pyoracle import Oracle
+from test_gpu_parity import RUN_TOL, compare_states
+from viral_b200 import _abi as A
+from viral_b200 import configs as C
+from viral_b200.hydro import profile_gubser_is
+
+pytestmark = [pytest.mark.gpu, pytest.mark.late]
+
+T_TABLE_GEV = 1.2 * 0.19733  # the reference table's centre temperature, 1.2 fm^-1
+
+
+def test_c0_full_length_matches_oracle():
+    cfg = C.gubser_config()
+    inp = C.gubser_inputs(cfg)
+    O = oracle_from_inputs(cfg, inp)
+    with C.make_hydro(cfg, inp) as H:
+        tau = cfg.tau0
+        for k in (100, 200, 300):
+            while round((tau - cfg.tau0) / cfg.dtau) < k:
+                assert O.step(tau, cfg.dtau) == 0
+                tau += cfg.dtau
+            H.step(100)
+            worst = compare_states(H.get_state(), O.get_state(), RUN_TOL, fields=range(18))
+            print(f"c0 step {k}: max group-relative error {worst:.2e}")
+        assert abs(H.tau - 4.0) < 1e-9
+        assert abs(H.max_temperature() - O.max_temp_gev()) <= 1e-12 * O.max_temp_gev()
+
+
+def _is_state(cfg):
+    n = cfg.nx
+    e, ux, uy, pi5, pu = profile_gubser_is(n, n, cfg.dx, cfg.dy, 1.0, cfg.tau0, cfg.dtau, T_TABLE_GEV, 0.0, 0.2,
+                                           cfg.eos_a, cfg.hbarc)
+    inp = dict(tau=cfg.tau0, e=e, ux=ux, uy=uy, ueta=None, prevu=pu, pi_mode=A.PI_GIVEN, pi5=pi5)
+    return inp
+
+
+def _t_and_p(st, cfg):
+    """T (fm^-1) and P = tau^2 pi^{eta eta}/(e + P) (tracelessness and
+    transversality) of a boost-invariant conformal state"""
+    u0, u1, u2 = st[1], st[2], st[3]
+    ptt = (u1 * u1 * st[5] + 2 * u1 * u2 * st[7] + u2 * u2 * st[6]) / (u0 * u0)
+    return (st[0] / cfg.eos_a) ** 0.25, (ptt - st[5] - st[6]) / ((4 / 3) * st[0])
+
+
+def _errors(st, cfg, tau, bands):
+    n = cfg.nx
+    gx = n + 6
+    idx = np.arange(gx * gx)
+    x0 = -(n // 2) * cfg.dx
+    X, Y = x0 + (idx % gx - 3) * cfg.dx, x0 + (idx // gx - 3) * cfg.dx
+    r = np.hypot(X, Y)
+    T, e, u, pi = milne_fields(GubserIS(T_TABLE_GEV / cfg.hbarc, 0.0, 0.2), tau, X, Y, cfg.eos_a)
+    P = pi["ee"] / ((4 / 3) * e)
+    Tn, Pn = _t_and_p(st, cfg)
+    inner = interior_mask(cfg)
+    out = []
+    for rmax in bands:
+        m = inner & (r < rmax)
+        out.append((float(np.max(np.abs(Tn[m] - T[m]) / T[m])), float(np.max(np.abs(Pn[m] - P[m])))))
+    return out
+
+
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_follows_semi_analytic_israel_stewart_gubser(precision):
+    cfg = C.gubser_config(nx=161, ny=161, precision=precision)
+    inp = _is_state(cfg)
+    with C.make_hydro(cfg, inp) as H:
+        H.step(300)
+        st = H.get_state()
+        tau = H.tau
+    assert abs(tau - 4.0) < 1e-9
+    if precision == A.PREC_FP64:
+        f = canonical_state(cfg, inp)
+        f[5:10] = inp["pi5"]
+        O = Oracle(oracle_config(cfg))
+        O.set_state(f)
+        O.fill_tmunu(cfg.tau0)
+        t = cfg.tau0
+        for _ in range(300):
+            assert O.step(t, cfg.dtau) == 0
+            t += cfg.dtau
+        worst = compare_states(st, O.get_state(), RUN_TOL, fields=range(18))
+        print(f"IS Gubser 161x161, 300 steps: GPU vs oracle {worst:.2e}")
+    (t2, p2), (t7, p7) = _errors(st, cfg, tau, (2.0, 7.0))
+    print(f"tau 4: r < 2: T {t2:.2e}, P {p2:.2e}; r < 7: T {t7:.2e}, P {p7:.2e}")
+    assert t2 < 2.5e-3 and p2 < 1e-3
+    assert t7 < 0.1 and p7 < 0.08
+
+
+def test_semi_analytic_error_converges_with_the_grid():
+    """at tau = 2.9 fm/c, within 5 fm: 0.1 fm cells and 0.01 fm/c steps
+    against 0.05 fm and 0.005 fm/c on the same 16 fm box"""
+    res = []
+    for n, dx, dt, steps in ((161, 0.1, 0.01, 190), (321, 0.05, 0.005, 380)):
+        cfg = C.gubser_config(nx=n, ny=n, dx=dx)
+        cfg.dtau = dt
+        with C.make_hydro(cfg, _is_state(cfg)) as H:
+            H.step(steps)
+            assert abs(H.tau - 2.9) < 1e-9
+            res.append(_errors(H.get_state(), cfg, H.tau, (5.0,))[0])
+    print("r < 5 at tau 2.9: dx 0.1: T %.2e P %.2e; dx 0.05: T %.2e P %.2e" % (*res[0], *res[1]))
+    assert res[1][0] < res[0][0] / 5 and res[1][1] < res[0][1] / 5
+    assert res[1][0] < 2e-3 and res[1][1] < 3e-3

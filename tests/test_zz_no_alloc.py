@@ -67,7 +67,8 @@ def _run_pair(cfg, f0, tau0, steps=(3, 2)):
         assert rc == A.OK, A.STATUS_NAMES.get(rc, rc)
         if q == len(steps) - 1:
             free.append(torch.cuda.mem_get_info()[0])
-        tau += n * cfg.dtau
+        for _ in range(n):  # the time advances by repeated addition, as in the library
+            tau += cfg.dtau
         got.append(dev.cpu().numpy().reshape(A.NFIELDS, -1).copy())
     return ref, got, free
 

@@ -110,6 +110,10 @@ SIGNATURES = [
     ("vh_profile_gubser_cold", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                               ctypes.c_double, _dp, _dp, _dp, _dp, _dp]),
+    ("vh_profile_gubser_is", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                            _dp, _dp, _dp, _dp, _dp]),
     ("vh_freezeout_2d", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, _dp, _dp, _dp, _dp, ctypes.c_double, _dp, ctypes.c_longlong,
                                        ctypes.POINTER(ctypes.c_longlong)]),

@@ -1,9 +1,10 @@
 // Seeded host-side input generators (include/vh.h "inputs"): the synthetic
-// tabulated EOS, the ideal Gubser profile and a Monte-Carlo Glauber energy
-// density.  The reference reads its Gubser table from a file it does not
+// tabulated EOS, the ideal, cold-plasma and Israel-Stewart Gubser profiles
+// and a Monte-Carlo Glauber energy density.  The reference reads its Gubser table from a file it does not
 // ship (NEWEST5/init.h:419-459) and builds optical-Glauber/CGC profiles with
 // GSL (NEWEST5/ginit.h); these generators stand in for both so that the GPU
 // path and its tests consume identical inputs.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -166,6 +167,135 @@ extern "C" int vh_profile_gubser_cold(int nx, int ny, double dx, double dy, doub
         pi5[2 * n + c] = sphi * cphi * (prr - pff);              // xy
         pi5[3 * n + c] = 0.0;                                    // x eta
         pi5[4 * n + c] = 0.0;                                    // y eta
+      }
+    }
+  return VH_OK;
+}
+
+namespace {
+
+// The Israel-Stewart Gubser flow (conformal fluid, tau_pi = 5 eta/(e+P),
+// constant eta/s) as functions of the de Sitter time rho, sinh rho =
+// -(1 - q^2 tau^2 + q^2 r^2)/(2 q tau): T^ = tau T and the shear ratio
+// P = tau^2 pi^{eta eta}/(e + P_pressure), both Weyl invariant.  In the
+// fluid's rest frame of de Sitter space (theta^ = 2 tanh rho,
+// sigma^{eta eta} = (2/3) tanh rho in the reference's mostly-minus
+// convention) energy conservation and the relaxation equation
+// tau_pi (D pi + (4/3) pi theta) + pi = 2 eta sigma become
+//   d ln T^/d rho = -(2/3) tanh rho + (1/3) P tanh rho
+//   dP/d rho      = -(4/3) P^2 tanh rho - P T^/(5 eta/s) + (4/15) tanh rho.
+// Integrated by classical RK4 on a uniform rho grid outward from rho0 in
+// both directions; values between nodes by cubic Hermite interpolation with
+// the right-hand side as the derivative.
+struct GubserIS {
+  double etas, rho0, h;
+  std::vector<double> lt, pb;  // node values from rho_lo upward
+  double rho_lo = 0;
+
+  void rhs(double rho, double l, double p, double& dl, double& dp) const {
+    const double th = std::tanh(rho), T = std::exp(l);
+    dl = -(2.0 / 3.0) * th + (1.0 / 3.0) * p * th;
+    dp = -(4.0 / 3.0) * p * p * th - p * T / (5.0 * etas) + (4.0 / 15.0) * th;
+  }
+  // n steps of size hs (signed) from (rho, l, p), appending the nodes
+  void march(double rho, double l, double p, double hs, int n, std::vector<double>& L, std::vector<double>& Pv) const {
+    for (int i = 0; i < n; i++) {
+      double k1l, k1p, k2l, k2p, k3l, k3p, k4l, k4p;
+      rhs(rho, l, p, k1l, k1p);
+      rhs(rho + 0.5 * hs, l + 0.5 * hs * k1l, p + 0.5 * hs * k1p, k2l, k2p);
+      rhs(rho + 0.5 * hs, l + 0.5 * hs * k2l, p + 0.5 * hs * k2p, k3l, k3p);
+      rhs(rho + hs, l + hs * k3l, p + hs * k3p, k4l, k4p);
+      l += hs / 6.0 * (k1l + 2 * k2l + 2 * k3l + k4l);
+      p += hs / 6.0 * (k1p + 2 * k2p + 2 * k3p + k4p);
+      rho += hs;
+      L.push_back(l);
+      Pv.push_back(p);
+    }
+  }
+  bool build(double t_hat0, double p0, double lo, double hi) {
+    if (!(t_hat0 > 0) || !(etas > 0) || lo > rho0 || hi < rho0) return false;
+    const int nd = (int)std::ceil((rho0 - lo) / h) + 2, nu = (int)std::ceil((hi - rho0) / h) + 2;
+    std::vector<double> Ld, Pd, Lu, Pu;
+    march(rho0, std::log(t_hat0), p0, -h, nd, Ld, Pd);
+    march(rho0, std::log(t_hat0), p0, h, nu, Lu, Pu);
+    lt.assign(Ld.rbegin(), Ld.rend());
+    pb.assign(Pd.rbegin(), Pd.rend());
+    lt.push_back(std::log(t_hat0));
+    pb.push_back(p0);
+    lt.insert(lt.end(), Lu.begin(), Lu.end());
+    pb.insert(pb.end(), Pu.begin(), Pu.end());
+    rho_lo = rho0 - nd * h;
+    for (size_t i = 0; i < lt.size(); i++)
+      if (!std::isfinite(lt[i]) || !std::isfinite(pb[i])) return false;
+    return true;
+  }
+  void at(double rho, double& t_hat, double& p) const {
+    const double u = (rho - rho_lo) / h;
+    int i = (int)std::floor(u);
+    i = i < 0 ? 0 : (i > (int)lt.size() - 2 ? (int)lt.size() - 2 : i);
+    const double s = u - i, r0 = rho_lo + i * h;
+    double d0l, d0p, d1l, d1p;
+    rhs(r0, lt[i], pb[i], d0l, d0p);
+    rhs(r0 + h, lt[i + 1], pb[i + 1], d1l, d1p);
+    const double h00 = (1 + 2 * s) * (1 - s) * (1 - s), h10 = s * (1 - s) * (1 - s), h01 = s * s * (3 - 2 * s),
+                 h11 = s * s * (s - 1);
+    const double l = h00 * lt[i] + h10 * h * d0l + h01 * lt[i + 1] + h11 * h * d1l;
+    p = h00 * pb[i] + h10 * h * d0p + h01 * pb[i + 1] + h11 * h * d1p;
+    t_hat = std::exp(l);
+  }
+};
+
+}  // namespace
+
+extern "C" int vh_profile_gubser_is(int nx, int ny, double dx, double dy, double q, double tau0, double dtau,
+                                    double t0_gev, double p0, double etas, double a, double hbarc, double* e,
+                                    double* ux, double* uy, double* pi5, double* prevu4) {
+  if (nx < 1 || ny < 1 || !e || !ux || !uy || !pi5 || !(tau0 > dtau) || !(q > 0) || !(etas > 0) || !(a > 0) ||
+      !(hbarc > 0) || !(t0_gev > 0))
+    return VH_E_ARG;
+  std::vector<double> X, Y;
+  axis_coords(nx, 3, dx, X);
+  axis_coords(ny, 3, dy, Y);
+  const int gx = nx + 6, gy = ny + 6;
+  const long long n = (long long)gx * gy;
+  const double q2 = q * q;
+  auto rho_of = [&](double tau, double r) { return std::asinh(-(1 - q2 * tau * tau + q2 * r * r) / (2 * q * tau)); };
+  // the solution is fixed at the grid centre at tau0: T^ = tau0 T0, P = p0
+  GubserIS G{etas, rho_of(tau0, 0.0), 1e-3, {}, {}};
+  double rmax = 0;
+  for (double x : X)
+    for (double y : Y) rmax = std::max(rmax, std::sqrt(x * x + y * y));
+  if (!G.build(tau0 * t0_gev / hbarc, p0, rho_of(tau0, rmax) - 0.01, G.rho0 + 0.01)) return VH_E_ARG;
+  for (int j = 0; j < gy; j++)
+    for (int i = 0; i < gx; i++) {
+      const long long c = (long long)j * gx + i;
+      const double x = X[i], y = Y[j], r = std::sqrt(x * x + y * y);
+      const double cphi = r > 0 ? x / r : 1.0, sphi = r > 0 ? y / r : 0.0;
+      for (int pass = 0; pass < 2; pass++) {
+        const double tau = pass ? tau0 - dtau : tau0;
+        const double kap = std::atanh(2 * q2 * tau * r / (1 + q2 * tau * tau + q2 * r * r));
+        const double sh = std::sinh(kap), ch = std::cosh(kap);
+        if (pass) {
+          if (prevu4) {
+            prevu4[c] = ch; prevu4[n + c] = sh * cphi; prevu4[2 * n + c] = sh * sphi; prevu4[3 * n + c] = 0.0;
+          }
+          continue;
+        }
+        ux[c] = sh * cphi;
+        uy[c] = sh * sphi;
+        double t_hat, pr;
+        G.at(rho_of(tau, r), t_hat, pr);
+        const double T = t_hat / tau;
+        e[c] = a * T * T * T * T;
+        // rest-frame shear: w P along eta (orthonormal), -w P/2 along phi and
+        // along n = (sinh kap, cosh kap cos phi, cosh kap sin phi), the unit
+        // vector of the (tau, r) plane orthogonal to u
+        const double w = (4.0 / 3.0) * e[c], hp = -0.5 * w * pr;
+        pi5[c] = hp * (sphi * sphi + ch * ch * cphi * cphi);          // xx
+        pi5[n + c] = hp * (cphi * cphi + ch * ch * sphi * sphi);      // yy
+        pi5[2 * n + c] = hp * sphi * cphi * (ch * ch - 1.0);          // xy
+        pi5[3 * n + c] = 0.0;                                         // x eta
+        pi5[4 * n + c] = 0.0;                                         // y eta
       }
     }
   return VH_OK;

@@ -420,6 +420,18 @@ def profile_gubser_cold(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, b=1.21, a=A_
     return e, ux, uy, pi5, pu
 
 
+def profile_gubser_is(nx, ny, dx, dy, q=1.0, tau0=1.0, dtau=0.01, t0_gev=0.6, p0=0.0, etas=0.2, a=A_QGP,
+                      hbarc=HBARC):
+    """the Israel-Stewart Gubser flow at tau0 (T = t0_gev and shear ratio
+    tau^2 pi^{eta eta}/(e+P) = p0 at the grid centre): e, u^x, u^y, pi5 and
+    prevu (at tau0 - dtau) on the 2+1D ghost-inclusive grid"""
+    n = (nx + 6) * (ny + 6)
+    e, ux, uy, pi5, pu = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros((5, n)), np.zeros((4, n))
+    A.check(A.lib().vh_profile_gubser_is(nx, ny, dx, dy, q, tau0, dtau, t0_gev, p0, etas, a, hbarc, A.ptr(e),
+                                         A.ptr(ux), A.ptr(uy), A.ptr(pi5), A.ptr(pu)))
+    return e, ux, uy, pi5, pu
+
+
 def profile_cgc(nx, ny, nz=1, boost_invariant=True, dx=0.1, dy=0.1, dz=0.1, tau=0.1, e_peak=1.0, x_pos=3.0,
                 mass_number=197.0, ws_a=0.546, thickness_scale=12.2546, eta_flat=4.0, delta=100.0) -> np.ndarray:
     """the optical-Glauber CGC T^{mu nu} (10, n) of the reference's Glasma
