@@ -276,6 +276,51 @@ class RefBuild:
         return y, J.reshape(4, 4)
 
 
+class RefWrite:
+    """The reference's snapshot writers (oracle/ref_write.cpp): NEWEST5's
+    write.h (12 doubles per cell) or NEWEST10's (17, and the Navier-Stokes
+    snapshot) in one compile-time block."""
+
+    def __init__(self, variant: str):
+        L = _load(os.path.join(HERE, "_ref", f"libref_{variant}.so"))
+        d = (ctypes.c_int * 9)()
+        c = (ctypes.c_double * 4)()
+        L.refw_init(d, c)
+        L.refw_set_state.argtypes = [_dp, _dp, _dp]
+        L.refw_write_xy.argtypes = [ctypes.c_double]
+        self.n10 = hasattr(L, "refw_write_ns_xy")
+        if self.n10:
+            L.refw_write_ns_xy.argtypes = [ctypes.c_double]
+        else:
+            L.refw_write_full.argtypes = [ctypes.c_double]
+        self.L = L
+        self.gx, self.gy, self.gz, self.nx, self.ny, self.nz, self.freq, self.freqz, lbi = list(d)
+        self.boost_invariant = bool(lbi)
+        self.dx, self.dy, self.dz, self.factor = list(c)
+        self.n = self.gx * self.gy * self.gz
+
+    def set_state(self, f, pi10=None, nspi=None):
+        c = lambda a: None if a is None else _ptr(np.ascontiguousarray(a, dtype=np.float64))
+        self.L.refw_set_state(c(f), c(pi10), c(nspi))
+
+    def write(self, which: str, tau: float, workdir: str) -> bytes:
+        """the file the reference's writer leaves in workdir/res/"""
+        name = ("NStau%2.3ffm.bin" if which == "ns_xy" else "tau%2.3ffm.bin") % tau
+        os.makedirs(os.path.join(workdir, "res"), exist_ok=True)
+        path = os.path.join(workdir, "res", name)
+        if os.path.exists(path):
+            os.remove(path)
+        cwd = os.getcwd()
+        os.chdir(workdir)
+        try:
+            {"xy": lambda: self.L.refw_write_xy(tau), "full": lambda: self.L.refw_write_full(tau),
+             "ns_xy": lambda: self.L.refw_write_ns_xy(tau)}[which]()
+        finally:
+            os.chdir(cwd)
+        with open(path, "rb") as fh:
+            return fh.read()
+
+
 class RefNS10:
     """NEWEST10's CalcNS in its default compile-time block, boost invariant
     (oracle/ref_ns10.cpp)."""

@@ -60,4 +60,48 @@ static inline int MPI_Isend(const void*, int, MPI_Datatype, int, int, MPI_Comm, 
 static inline int MPI_Irecv(void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request*) { abort(); return 0; }
 static inline int MPI_Waitall(int, MPI_Request*, MPI_Status*) { return 0; }
 
+/* MPI-IO on one rank: a file handle is an index into a table of stdio
+ * streams (MPI_File_open with MPI_MODE_CREATE opens for update, creating the
+ * file; seek, read and write move through the stream).  A harness that
+ * defines VH_SHIM_NO_FILES brings its own. */
+#ifndef VH_SHIM_NO_FILES
+#include <stdio.h>
+#define VH_SHIM_MAX_FILES 16
+static FILE* vh_shim_files[VH_SHIM_MAX_FILES];
+static inline int MPI_File_open(MPI_Comm, const char* name, int amode, MPI_Info, MPI_File* fh) {
+  FILE* f = 0;
+  if (amode & MPI_MODE_RDONLY) {
+    f = fopen(name, "rb");
+  } else {
+    f = fopen(name, "r+b");
+    if (!f && (amode & MPI_MODE_CREATE)) f = fopen(name, "w+b");
+  }
+  if (!f) return 1;
+  for (int q = 1; q < VH_SHIM_MAX_FILES; q++)
+    if (!vh_shim_files[q]) { vh_shim_files[q] = f; *fh = q; return 0; }
+  fclose(f);
+  return 1;
+}
+static inline int MPI_File_seek(MPI_File fh, MPI_Offset off, int) {
+  return fseek(vh_shim_files[fh], (long)off, SEEK_SET) == 0 ? 0 : 1;
+}
+static inline int MPI_File_write(MPI_File fh, const void* buf, int n, MPI_Datatype t, MPI_Status*) {
+  const size_t sz = (size_t)vh_shim_type_size(t);
+  return fwrite(buf, sz, (size_t)n, vh_shim_files[fh]) == (size_t)n ? 0 : 1;
+}
+static inline int MPI_File_read(MPI_File fh, void* buf, int n, MPI_Datatype t, MPI_Status*) {
+  const size_t sz = (size_t)vh_shim_type_size(t);
+  return fread(buf, sz, (size_t)n, vh_shim_files[fh]) == (size_t)n ? 0 : 1;
+}
+static inline int MPI_File_close(MPI_File* fh) {
+  if (*fh > 0 && *fh < VH_SHIM_MAX_FILES && vh_shim_files[*fh]) {
+    fclose(vh_shim_files[*fh]);
+    vh_shim_files[*fh] = 0;
+  }
+  *fh = 0;
+  return 0;
+}
+static inline int MPI_Finalize(void) { return 0; }
+#endif
+
 #endif

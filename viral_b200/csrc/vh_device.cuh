@@ -581,8 +581,16 @@ VH_HD inline bool solve4(double A[4][4], double b[4]) {
 // |dx_i| <= qtol |x_i| (or dx_i = 0): in the quadratic regime the error left
 // after such a step is of order |dx|^2, so qtol = 1e-8 leaves ~1e-16 and
 // saves the confirming iteration whose step would fall below rtol.
+// With qskip > 0 a Newton step whose every component is already below
+// qskip |x_i + st_i| (or zero) is taken without evaluating the residual at
+// its end: that evaluation would only confirm, through the step control, a
+// step of a size that the quadratic regime always accepts, so the iterate
+// is the one the loop above would reach (one evaluation fewer per cell,
+// the last of three or four).  The root test then applies to the residual
+// before that step, against fskip |T^{tau mu}|: a Newton step of relative
+// size qskip leaves a residual of about qskip |J x|.
 VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, double tau, double* x,
-                               double rtol = 1e-16, double qtol = 0.0) {
+                               double rtol = 1e-16, double qtol = 0.0, double qskip = 0.0, double fskip = 0.0) {
   const double t2 = C.cart ? 1.0 : tau * tau;
   double y[4], J[4][4];
   c2p_fj(C, Tt, p, t2, x, y, J, true);
@@ -594,6 +602,18 @@ VH_HD inline int con2prim(const DevCfg& C, const double* Tt, const double* p, do
     it++;
     double st[4] = {-y[0], -y[1], -y[2], -y[3]};
     if (!solve4(J, st)) return -1;
+    if (qskip > 0.0) {
+      bool small = true;
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (!(fabs(st[i]) <= qskip * fabs(x[i] + st[i]) || st[i] == 0.0)) small = false;
+      if (small) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) x[i] += st[i];
+        const double sc = fskip * (fabs(Tt[0]) + fabs(Tt[1]) + fabs(Tt[2]) + fabs(Tt[3]));
+        return phi <= sc * sc ? it : -1;
+      }
+    }
     double t = 1.0, xt[4], phi1 = 0;
     bool ok = false;
     for (int tries = 0; tries < 64; tries++) {

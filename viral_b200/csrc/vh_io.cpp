@@ -56,11 +56,14 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
   const long long n = (long long)gx * gy * gz;
   std::vector<double> f(18 * (size_t)n);
   if ((r = vh_get_state(h, f.data()))) return r;
-  // the 17-variable records take T, P and the full pi^{mu nu} from the device
-  std::vector<double> pT, pP, pi10;
+  // the 17-variable records take the full pi^{mu nu} from the device (the
+  // closure of the five stored components); T and P, as in every record,
+  // come from the EOS at e on the host, as the reference's FT and EOS give
+  // them (NEWEST5/multiroot.h:428-429)
+  std::vector<double> pi10;
   if (v17) {
-    pT.resize(n); pP.resize(n); pi10.resize(10 * (size_t)n);
-    if ((r = vh_get_primitive(h, nullptr, pP.data(), pT.data(), nullptr, pi10.data()))) return r;
+    pi10.resize(10 * (size_t)n);
+    if ((r = vh_get_primitive(h, nullptr, nullptr, nullptr, nullptr, pi10.data()))) return r;
   }
   // NEWEST10/write.h:123-170 (WriteNSXY): the ten Navier-Stokes pi^{mu nu}
   // and the (zero) bulk part per cell
@@ -96,8 +99,6 @@ extern "C" int vh_write(vh_handle* h, const char* path, int layout, int every) {
     o[4] = f[3 * n + c] / u0;
     o[5] = f[4 * n + c] / u0;
     if (v17) {
-      o[1] = pT[c];
-      o[2] = pP[c];
       for (int l = 0; l < 10; l++) o[6 + l] = pi10[(size_t)l * n + c];
       o[16] = 0.0;  // bulk pressure is not evolved
       return;

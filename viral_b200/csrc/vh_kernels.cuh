@@ -35,9 +35,21 @@ struct DirSmem {
   static constexpr int NA = Tile<DIR, R>::NA, NC = NC_;
   static constexpr int TL = NA - 6;
   static constexpr int LD = NA + 1;  // padded line length (bank spread)
-  R q[19][NC * LD];  // 0..8 F^DIR, 9..17 Var, 18 signal speed
-  R u[4][NC * LD];   // u^mu for the velocity derivative
+  // F^l and Var^l of a cell side by side, and the velocity as the pairs
+  // (u^tau, u^x), (u^y, u^eta): the reconstruction takes both members of a
+  // pair with one shared-memory load (8 bytes in FP32, 16 in FP64)
+  alignas(16) R fv[9][NC * LD][2];
+  R spd[NC * LD];                   // signal speed
+  alignas(16) R up[2][NC * LD][2];  // u^mu for the velocity derivative
 };
+
+// both members of a pair at line position s
+__device__ __forceinline__ unsigned long long ld_pair(const float (*a)[2], int s) {
+  return *reinterpret_cast<const unsigned long long*>(a[s]);
+}
+__device__ __forceinline__ double2 ld_pair(const double (*a)[2], int s) {
+  return *reinterpret_cast<const double2*>(a[s]);
+}
 
 // Centre flux along DIR, Var and signal speed of one cell
 // (NEWEST5/hydroKT.h:16-83, 161-245, 349-367).
@@ -85,14 +97,15 @@ __device__ inline void cell_terms(const DevCfg& C, R tau, R e, const R* u, const
 }
 
 // Both face states of the stencil centred on the lane's cell: L at the
-// right face, R at the left face (WENO5, or generalized minmod).
-template <class R>
+// right face, R at the left face (WENO5, or generalized minmod).  Line
+// position k of the quantity is q[k * ST].
+template <class R, int ST = 1>
 __device__ inline void recon_lr(const DevCfg& C, const R* q, int s, R& L, R& Rr) {
   if (C.recon == 0) {
-    weno_lr<R>(q[s - 2], q[s - 1], q[s], q[s + 1], q[s + 2], L, Rr);
+    weno_lr<R>(q[(s - 2) * ST], q[(s - 1) * ST], q[s * ST], q[(s + 1) * ST], q[(s + 2) * ST], L, Rr);
   } else {
-    L = mm_left<R>((R)C.mm_theta, q[s - 1], q[s], q[s + 1]);
-    Rr = mm_right<R>((R)C.mm_theta, q[s - 1], q[s], q[s + 1]);
+    L = mm_left<R>((R)C.mm_theta, q[(s - 1) * ST], q[s * ST], q[(s + 1) * ST]);
+    Rr = mm_right<R>((R)C.mm_theta, q[(s - 1) * ST], q[s * ST], q[(s + 1) * ST]);
   }
 }
 
@@ -225,10 +238,10 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
       for (int l = 0; l < 9; l++) { F[l] = 0; V[l] = 0; }
     }
 #pragma unroll
-    for (int l = 0; l < 9; l++) { sm.q[l][s] = F[l]; sm.q[9 + l][s] = V[l]; }
-    sm.q[18][s] = spd;
+    for (int l = 0; l < 9; l++) { sm.fv[l][s][0] = F[l]; sm.fv[l][s][1] = V[l]; }
+    sm.spd[s] = spd;
 #pragma unroll
-    for (int l = 0; l < 4; l++) sm.u[l][s] = uu[l];
+    for (int l = 0; l < 4; l++) sm.up[l >> 1][s][l & 1] = uu[l];
   }
   __syncthreads();
 
@@ -246,7 +259,7 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   R amax = 0;
   {
     R L = 0, Rr = 0;
-    if (stencil) recon_lr<R>(C, sm.q[18], s, L, Rr);
+    if (stencil) recon_lr<R>(C, sm.spd, s, L, Rr);
     const R Rn = shfl_dn<R>(Rr, 1);
     // the face left of the first interior cell takes no dissipation: its
     // max speed sits in a ghost cell the reference never fills
@@ -267,31 +280,36 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
       if constexpr (sizeof(R) == 4) {
         if (C.recon == 0) {
           // F^l and V^l of the stencil reconstructed as one pair
-          const float* qa = reinterpret_cast<const float*>(sm.q[l]);
-          const float* qb = reinterpret_cast<const float*>(sm.q[9 + l]);
-          F2 L2, R2;
-          weno_lr2(f2(qa[s - 2], qb[s - 2]), f2(qa[s - 1], qb[s - 1]), f2(qa[s], qb[s]), f2(qa[s + 1], qb[s + 1]),
-                   f2(qa[s + 2], qb[s + 2]), L2, R2);
+          const float(*q)[2] = reinterpret_cast<const float(*)[2]>(sm.fv[l]);
+          F2 L2, R2, x0, x1, x2, x3, x4;
+          x0.v = ld_pair(q, s - 2); x1.v = ld_pair(q, s - 1); x2.v = ld_pair(q, s);
+          x3.v = ld_pair(q, s + 1); x4.v = ld_pair(q, s + 2);
+          weno_lr2(x0, x1, x2, x3, x4, L2, R2);
           float a, b;
           f2u(L2, a, b);
           fl = a; vl = b;
           f2u(R2, a, b);
           fr = a; vr = b;
         } else {
-          recon_lr<R>(C, sm.q[l], s, fl, fr);
-          recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
+          recon_lr<R, 2>(C, &sm.fv[l][0][0], s, fl, fr);
+          recon_lr<R, 2>(C, &sm.fv[l][0][1], s, vl, vr);
         }
       } else if (C.recon == 0) {
         // F^l and V^l with one reciprocal between them
-        const double* qa = reinterpret_cast<const double*>(sm.q[l]) + s - 2;
-        const double* qb = reinterpret_cast<const double*>(sm.q[9 + l]) + s - 2;
-        double a_[5] = {qa[0], qa[1], qa[2], qa[3], qa[4]}, b_[5] = {qb[0], qb[1], qb[2], qb[3], qb[4]};
+        const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.fv[l]);
+        double a_[5], b_[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+          const double2 v = ld_pair(q, s - 2 + k);
+          a_[k] = v.x;
+          b_[k] = v.y;
+        }
         double flx, frx, vlx, vrx;
         weno_lr_pair(a_, b_, flx, frx, vlx, vrx);
         fl = flx; fr = frx; vl = vlx; vr = vrx;
       } else {
-        recon_lr<R>(C, sm.q[l], s, fl, fr);
-        recon_lr<R>(C, sm.q[9 + l], s, vl, vr);
+        recon_lr<R, 2>(C, &sm.fv[l][0][0], s, fl, fr);
+        recon_lr<R, 2>(C, &sm.fv[l][0][1], s, vl, vr);
       }
     }
     fr = shfl_dn<R>(fr, 1);
@@ -307,16 +325,24 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   if (out) {
 #pragma unroll
     for (int l = 0; l < 4; l += 2) {
-      const R* qa = sm.u[l] + s - 2;
-      const R* qb = sm.u[l + 1] + s - 2;
       R La, Ra, Lb, Rb;
       if constexpr (sizeof(R) == 4) {
-        F2 L2, R2;
-        weno_lr2(f2(qa[0], qb[0]), f2(qa[1], qb[1]), f2(qa[2], qb[2]), f2(qa[3], qb[3]), f2(qa[4], qb[4]), L2, R2);
+        const float(*q)[2] = reinterpret_cast<const float(*)[2]>(sm.up[l >> 1]);
+        F2 L2, R2, x0, x1, x2, x3, x4;
+        x0.v = ld_pair(q, s - 2); x1.v = ld_pair(q, s - 1); x2.v = ld_pair(q, s);
+        x3.v = ld_pair(q, s + 1); x4.v = ld_pair(q, s + 2);
+        weno_lr2(x0, x1, x2, x3, x4, L2, R2);
         f2u(L2, La, Lb);
         f2u(R2, Ra, Rb);
       } else {
-        const double a_[5] = {qa[0], qa[1], qa[2], qa[3], qa[4]}, b_[5] = {qb[0], qb[1], qb[2], qb[3], qb[4]};
+        const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.up[l >> 1]);
+        double a_[5], b_[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+          const double2 v = ld_pair(q, s - 2 + k);
+          a_[k] = v.x;
+          b_[k] = v.y;
+        }
         weno_lr_pair(a_, b_, La, Ra, Lb, Rb);
       }
       P.du(l * 3 + DIR)[cell] = (La - Ra) * inv_h;
@@ -486,7 +512,11 @@ __device__ __forceinline__ unsigned root_cell(const DevCfg& C, const DevPtrs<R>&
     for (int l = 0; l < 4; l++) Tt[l] = (double)q9[l];
 #pragma unroll
     for (int l = 0; l < 5; l++) pd[l] = (double)q9[4 + l];
+    // stopping (con2prim): FP64 steps below 1e-13, or an undamped one below
+    // 1e-8, taken without the confirming evaluation; the mixed mode stores
+    // the result in FP32, so a step below 1e-5 (error ~1e-10) ends it
     const double rtol = sizeof(R) == 4 ? 1e-10 : 1e-13, qtol = sizeof(R) == 4 ? 1e-6 : 1e-8;
+    const double qskip = sizeof(R) == 4 ? 1e-5 : 1e-8, fskip = sizeof(R) == 4 ? 1e-4 : 1e-6;
     int it = -1;
     // a second attempt starts from the stage's primitives, still in memory
     // (near-vacuum cells, where the extrapolated start can lead Newton
@@ -498,7 +528,7 @@ __device__ __forceinline__ unsigned root_cell(const DevCfg& C, const DevPtrs<R>&
 #pragma unroll
         for (int l = 1; l < 4; l++) x[l] = (double)P.u(l)[c];
       }
-      it = con2prim(C, Tt, pd, tau1, x, rtol, qtol);
+      it = con2prim(C, Tt, pd, tau1, x, rtol, qtol, qskip, fskip);
     }
     if (it < 0) {
       atomicOr(P.status, ST_ROOT);
