@@ -364,8 +364,10 @@ int vh_eps_p(vh_handle* h, double* eps_p);
  *               T^{tau mu} = (e + P) u^tau u^mu - P g^{tau mu} + pi^{tau mu}
  *               re-derived from e at fixed u and pi (ghost cells included);
  *   grad_etas   2 doubles: d eps_p / d (etas0, etas1) of vh_config.
- * The handle is left at the final state.  In the mixed mode the adjoint runs
- * in FP32 with the implicit-function solve in FP64. */
+ * The handle is left at the final state.  In the mixed mode the forward and
+ * its recomputations run the FP32 step, and the reverse sweep runs in FP64
+ * on the recorded FP32 trajectory (the records promoted to FP64 segment by
+ * segment). */
 int vh_adjoint_eps_p(vh_handle* h, int nsteps, int checkpoint_every, double* eps_p, double* grad_state,
                      double* grad_e, double* grad_etas);
 /* Device milliseconds of the last vh_adjoint_eps_p on this handle: [0] the
