@@ -68,7 +68,15 @@ typedef struct {
   int coords;           /* VH_COORD_* (NEWEST5 Milne, TXYZ5 Cartesian) */
   int precision;        /* VH_PREC_FP64, or VH_PREC_MIXED: FP32 state, fluxes,
                            reconstruction and sources; FP64 root-find, EOS
-                           inversion and compensated conservation sums */
+                           inversion and compensated conservation sums.
+                           Range of the mixed mode: its WENO5 weights take
+                           one FP32 division per face pair, whose divisor
+                           grows as the eighth power of the stencil's
+                           differences; differences of a reconstructed
+                           quantity (tau T^{tau mu}, pi^{mu nu}, the fluxes,
+                           u^mu) above about 1e4 in fm units (e.g. energy-
+                           density spikes above about 2000 GeV/fm^3 across a
+                           cell) overflow it.  Run such states in FP64. */
   int recon;            /* VH_RECON_* */
   int nx, ny, nz;       /* interior cells (nz = 1 when boost_invariant) */
   int boost_invariant;  /* 1: no eta direction, no eta ghosts (reference LBI) */

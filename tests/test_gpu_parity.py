@@ -367,3 +367,32 @@ def test_smallest_grids_match_oracle(cfgkw):
         H.set_state(f, cfg.tau0)
         H.step(3)
         compare_states(H.get_state(), O.get_state(), 1e-11, fields=range(18))
+
+
+@pytest.mark.late
+def test_mixed_precision_near_its_weno_range():
+    """The mixed mode's FP32 WENO weights divide once per face pair by a
+    number of order (stencil difference)^8, which overflows FP32 above
+    differences of about 1e4 (include/vh.h).  A hot spot of 5000 fm^-4
+    (about 1000 GeV/fm^3) and 0.3 fm width at tau = 0.6 fm/c, differences of
+    a few thousand per cell, stays finite and tracks the FP64 step to FP32
+    rounding over 10 steps (late: newer than the rest of this file)."""
+    cfg64 = C.glauber_config(nx=48, ny=48, boost_invariant=True)
+    gx, gy, _ = cfg64.gdims()
+    idx = np.arange(gx * gy)
+    x = (idx % gx - 3 - 24) * cfg64.dx
+    y = (idx // gx - 3 - 24) * cfg64.dy
+    e = 1.0 + 5000.0 * np.exp(-(x * x + y * y) / (2 * 0.3 ** 2))
+    z = np.zeros_like(e)
+    inp = dict(tau=cfg64.tau0, e=e, ux=z, uy=z, ueta=None, prevu=None, pi_mode=A.PI_ZERO)
+    out = []
+    for prec in (A.PREC_FP64, A.PREC_MIXED):
+        cfg = C.glauber_config(nx=48, ny=48, boost_invariant=True, precision=prec)
+        with C.make_hydro(cfg, inp) as H:
+            H.step(10)
+            out.append(H.get_state())
+    m = interior_mask(cfg64)
+    assert np.all(np.isfinite(out[1]))
+    assert rel_err(out[1][0][m], out[0][0][m]) < 1e-4
+    for q in (1, 2, 3):
+        assert rel_err(out[1][q][m], out[0][q][m]) < 1e-3

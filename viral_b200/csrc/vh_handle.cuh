@@ -73,6 +73,25 @@ static constexpr int kStateArrays = 52;
 
 static inline unsigned grid1(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
+// A step kernel launched with programmatic stream serialization: it may begin
+// while the kernel before it in the stream finishes its last blocks; the
+// kernel itself waits for that kernel's completion before reading anything
+// (pdl_wait_then_release), so the overlap covers launch and block set-up.
+template <class K, class... Args>
+static cudaError_t launch_step_kernel(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, kernel, args...);
+}
+
 template <class R>
 static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, double tau, int first) {
   const DevCfg& C = h->C;
@@ -86,19 +105,19 @@ static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, dou
     block = dim3(T::NA * T::NC);
     grid = dim3((C.nx + T::NA - 7) / (T::NA - 6), (C.ny + T::NC - 1) / T::NC, nzi);
     sm = sizeof(DirSmem<R, 0>);
-    k_dir<R, 0><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
+    VH_CUDA(h, launch_step_kernel(k_dir<R, 0>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr, first));
   } else if (dir == 1) {
     using T = Tile<1, R>;
     block = dim3(T::NA * T::NC);
     grid = dim3((C.ny + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, nzi);
     sm = sizeof(DirSmem<R, 1>);
-    k_dir<R, 1><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
+    VH_CUDA(h, launch_step_kernel(k_dir<R, 1>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr, first));
   } else {
     using T = Tile<2, R>;
     block = dim3(T::NA * T::NC);
     grid = dim3((C.nz + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, C.ny);
     sm = sizeof(DirSmem<R, 2>);
-    k_dir<R, 2><<<grid, block, sm, h->stream>>>(C, P, use_b, (R)tau, inv_h, hr, first);
+    VH_CUDA(h, launch_step_kernel(k_dir<R, 2>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr, first));
   }
   VH_CUDA(h, cudaGetLastError());
   return VH_OK;
@@ -128,8 +147,7 @@ template <class R, int STAGE>
 static int stage_update(vh_handle* h, const DevPtrs<R>& P, double tau, double ts) {
   const DevCfg& C = h->C;
   const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
-  k_update<R, STAGE><<<grid1(nint, 128), 128, 0, h->stream>>>(C, P, tau, ts);
-  VH_CUDA(h, cudaGetLastError());
+  VH_CUDA(h, launch_step_kernel(k_update<R, STAGE>, dim3(grid1(nint, 128)), dim3(128), 0, h->stream, C, P, tau, ts));
   return VH_OK;
 }
 
