@@ -96,38 +96,33 @@ template <class R>
 static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, double tau, int first) {
   const DevCfg& C = h->C;
   const int nzi = C.kr - C.kl;
-  dim3 grid, block;
-  size_t sm;
   const double hh = dir == 0 ? C.dx : (dir == 1 ? C.dy : C.dz);
-  const R inv_h = (R)(1.0 / hh), hr = (R)hh;
+  const R inv_h = (R)(1.0 / hh);
+  // two cells per lane (k_dir2): a line of 64 cells, 58 outputs, per warp
   if (dir == 0) {
-    using T = Tile<0, R>;
-    block = dim3(T::NA * T::NC);
-    grid = dim3((C.nx + T::NA - 7) / (T::NA - 6), (C.ny + T::NC - 1) / T::NC, nzi);
-    sm = sizeof(DirSmem<R, 0>);
-    VH_CUDA(h, launch_step_kernel(k_dir<R, 0>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr, first));
+    using S = DirSmem2<R, 0>;
+    const dim3 grid((C.nx + S::TL - 1) / S::TL, (C.ny + S::NC - 1) / S::NC, nzi);
+    VH_CUDA(h, launch_step_kernel(k_dir2<R, 0>, grid, dim3(32 * S::NC), sizeof(S), h->stream, C, P, use_b, (R)tau,
+                                  inv_h, first));
   } else if (dir == 1) {
-    using T = Tile<1, R>;
-    block = dim3(T::NA * T::NC);
-    grid = dim3((C.ny + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, nzi);
-    sm = sizeof(DirSmem<R, 1>);
-    VH_CUDA(h, launch_step_kernel(k_dir<R, 1>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr, first));
+    using S = DirSmem2<R, 1>;
+    const dim3 grid((C.ny + S::TL - 1) / S::TL, (C.nx + S::NC - 1) / S::NC, nzi);
+    VH_CUDA(h, launch_step_kernel(k_dir2<R, 1>, grid, dim3(32 * S::NC), sizeof(S), h->stream, C, P, use_b, (R)tau,
+                                  inv_h, first));
   } else {
-    using T = Tile<2, R>;
-    block = dim3(T::NA * T::NC);
-    grid = dim3((C.nz + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, C.ny);
-    sm = sizeof(DirSmem<R, 2>);
-    VH_CUDA(h, launch_step_kernel(k_dir<R, 2>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr, first));
+    using S = DirSmem2<R, 2>;
+    const dim3 grid((C.nz + S::TL - 1) / S::TL, (C.nx + S::NC - 1) / S::NC, C.ny);
+    VH_CUDA(h, launch_step_kernel(k_dir2<R, 2>, grid, dim3(32 * S::NC), sizeof(S), h->stream, C, P, use_b, (R)tau,
+                                  inv_h, first));
   }
-  VH_CUDA(h, cudaGetLastError());
   return VH_OK;
 }
 
 template <class R>
 static int set_smem_attrs(vh_handle* h) {
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 0>)));
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 1>)));
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 2>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir2<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem2<R, 0>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir2<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem2<R, 1>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir2<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem2<R, 2>)));
   return VH_OK;
 }
 
