@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 #include <string>
@@ -69,6 +70,7 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
   C.cold = cfg->cold_plasma != 0;
   C.mm_theta = cfg->minmod_theta;
   h->tau = cfg->tau0;
+  if (const char* v = std::getenv("VH_PDL")) h->pdl = std::strcmp(v, "0") != 0;
 
   auto bail = [&](cudaError_t e, const char* what) {
     g_create_err = std::string("vh_create: ") + what + ": " + cudaGetErrorString(e);

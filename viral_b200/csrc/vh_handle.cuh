@@ -34,6 +34,10 @@ struct vh_handle {
   std::vector<double> eos_host;  // 4 x eos_n
   double tau = 0;
   bool have_state = false;
+  // step kernels launched with programmatic dependent launch (VH_PDL=0 in
+  // the environment at vh_create turns it off, e.g. under a profiler that
+  // replays kernels one by one)
+  bool pdl = true;
   // discrete-adjoint workspace (kept between calls) and the device
   // milliseconds of the last call's phases
   void* adj_buf = nullptr;
@@ -73,12 +77,14 @@ static constexpr int kStateArrays = 52;
 
 static inline unsigned grid1(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
-// A step kernel launched with programmatic stream serialization: it may begin
-// while the kernel before it in the stream finishes its last blocks; the
-// kernel itself waits for that kernel's completion before reading anything
-// (pdl_wait_then_release), so the overlap covers launch and block set-up.
+// A step kernel launched with programmatic stream serialization (when pdl):
+// it may begin while the kernel before it in the stream finishes its last
+// blocks; the kernel itself waits for that kernel's completion before
+// reading anything (pdl_wait_then_release), so the overlap covers launch and
+// block set-up.
 template <class K, class... Args>
-static cudaError_t launch_step_kernel(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+static cudaError_t launch_step_kernel(bool pdl, K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                      Args... args) {
   cudaLaunchConfig_t lc = {};
   lc.gridDim = grid;
   lc.blockDim = block;
@@ -88,7 +94,7 @@ static cudaError_t launch_step_kernel(K kernel, dim3 grid, dim3 block, size_t sm
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   lc.attrs = at;
-  lc.numAttrs = 1;
+  lc.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&lc, kernel, args...);
 }
 
@@ -96,33 +102,40 @@ template <class R>
 static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, double tau, int first) {
   const DevCfg& C = h->C;
   const int nzi = C.kr - C.kl;
+  dim3 grid, block;
+  size_t sm;
   const double hh = dir == 0 ? C.dx : (dir == 1 ? C.dy : C.dz);
-  const R inv_h = (R)(1.0 / hh);
-  // two cells per lane (k_dir2): a line of 64 cells, 58 outputs, per warp
+  const R inv_h = (R)(1.0 / hh), hr = (R)hh;
   if (dir == 0) {
-    using S = DirSmem2<R, 0>;
-    const dim3 grid((C.nx + S::TL - 1) / S::TL, (C.ny + S::NC - 1) / S::NC, nzi);
-    VH_CUDA(h, launch_step_kernel(k_dir2<R, 0>, grid, dim3(32 * S::NC), sizeof(S), h->stream, C, P, use_b, (R)tau,
-                                  inv_h, first));
+    using T = Tile<0, R>;
+    block = dim3(T::NA * T::NC);
+    grid = dim3((C.nx + T::NA - 7) / (T::NA - 6), (C.ny + T::NC - 1) / T::NC, nzi);
+    sm = sizeof(DirSmem<R, 0>);
+    VH_CUDA(h, launch_step_kernel(h->pdl, k_dir<R, 0>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr,
+                                  first));
   } else if (dir == 1) {
-    using S = DirSmem2<R, 1>;
-    const dim3 grid((C.ny + S::TL - 1) / S::TL, (C.nx + S::NC - 1) / S::NC, nzi);
-    VH_CUDA(h, launch_step_kernel(k_dir2<R, 1>, grid, dim3(32 * S::NC), sizeof(S), h->stream, C, P, use_b, (R)tau,
-                                  inv_h, first));
+    using T = Tile<1, R>;
+    block = dim3(T::NA * T::NC);
+    grid = dim3((C.ny + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, nzi);
+    sm = sizeof(DirSmem<R, 1>);
+    VH_CUDA(h, launch_step_kernel(h->pdl, k_dir<R, 1>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr,
+                                  first));
   } else {
-    using S = DirSmem2<R, 2>;
-    const dim3 grid((C.nz + S::TL - 1) / S::TL, (C.nx + S::NC - 1) / S::NC, C.ny);
-    VH_CUDA(h, launch_step_kernel(k_dir2<R, 2>, grid, dim3(32 * S::NC), sizeof(S), h->stream, C, P, use_b, (R)tau,
-                                  inv_h, first));
+    using T = Tile<2, R>;
+    block = dim3(T::NA * T::NC);
+    grid = dim3((C.nz + T::NA - 7) / (T::NA - 6), (C.nx + T::NC - 1) / T::NC, C.ny);
+    sm = sizeof(DirSmem<R, 2>);
+    VH_CUDA(h, launch_step_kernel(h->pdl, k_dir<R, 2>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h, hr,
+                                  first));
   }
   return VH_OK;
 }
 
 template <class R>
 static int set_smem_attrs(vh_handle* h) {
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir2<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem2<R, 0>)));
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir2<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem2<R, 1>)));
-  VH_CUDA(h, cudaFuncSetAttribute(k_dir2<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem2<R, 2>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 0>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 1>)));
+  VH_CUDA(h, cudaFuncSetAttribute(k_dir<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirSmem<R, 2>)));
   return VH_OK;
 }
 
@@ -142,7 +155,8 @@ template <class R, int STAGE>
 static int stage_update(vh_handle* h, const DevPtrs<R>& P, double tau, double ts) {
   const DevCfg& C = h->C;
   const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
-  VH_CUDA(h, launch_step_kernel(k_update<R, STAGE>, dim3(grid1(nint, 128)), dim3(128), 0, h->stream, C, P, tau, ts));
+  VH_CUDA(h, launch_step_kernel(h->pdl, k_update<R, STAGE>, dim3(grid1(nint, 128)), dim3(128), 0, h->stream, C, P,
+                                tau, ts));
   return VH_OK;
 }
 

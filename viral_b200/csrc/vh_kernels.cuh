@@ -361,230 +361,6 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   }
 }
 
-// ---------------------------------------------------------------------------
-// The sweep with two cells per lane: a line of NA2 = 64 cells (58 outputs and
-// the 3-cell halo on each side) per warp, lane a owning the adjacent cells
-// 2a and 2a + 1.  Against one cell per lane (dir_tile) the halo is loaded
-// and its per-cell terms formed for 64 cells per 58 outputs instead of 32
-// per 26, the stencils of a lane's two cells (positions 2a-2 .. 2a+3) come
-// from shared memory as three 16-byte loads per quantity pair, and the face
-// between the two cells needs no shuffle.  The arithmetic per face is
-// dir_tile's.
-template <class R, int DIR>
-struct Tile2 { static constexpr int NC = (DIR == 0 || sizeof(R) == 8) ? 4 : 8; };
-
-template <class R, int DIR, int NC_ = Tile2<R, DIR>::NC>
-struct DirSmem2 {
-  static constexpr int NA = 64, NC = NC_;
-  static constexpr int TL = NA - 6;
-  // even, so that a lane's 16-byte loads stay aligned, and 2 cells more than
-  // the line so that the strided stores of the load phase spread over banks
-  static constexpr int LD = NA + 2;
-  alignas(16) R fv[9][NC * LD][2];  // F^l and Var^l side by side
-  alignas(16) R up[2][NC * LD][2];  // (u^tau, u^x), (u^y, u^eta)
-  alignas(16) R spd[NC * LD];       // signal speed
-};
-
-// the six pairs at positions s0 .. s0+5 of a pair array (s0 even)
-template <class R>
-__device__ __forceinline__ void ld_pairs6(const R (*a)[2], int s0, R* x, R* y) {
-  if constexpr (sizeof(R) == 4) {
-#pragma unroll
-    for (int k = 0; k < 6; k += 2) {
-      const float4 v = *reinterpret_cast<const float4*>(a[s0 + k]);
-      x[k] = v.x; y[k] = v.y; x[k + 1] = v.z; y[k + 1] = v.w;
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-      const double2 v = *reinterpret_cast<const double2*>(a[s0 + k]);
-      x[k] = v.x; y[k] = v.y;
-    }
-  }
-}
-
-// L and R face states of two quantities a, b at the two stencils centred on
-// positions 2 and 3 of the six values (the lane's two cells)
-template <class R>
-__device__ __forceinline__ void recon2_pair(const DevCfg& C, const R* a, const R* b, R* La, R* Ra, R* Lb, R* Rb) {
-  if (C.recon == 0) {
-    if constexpr (sizeof(R) == 4) {
-#pragma unroll
-      for (int p = 0; p < 2; p++) {
-        F2 L2, R2;
-        weno_lr2(f2(a[p], b[p]), f2(a[p + 1], b[p + 1]), f2(a[p + 2], b[p + 2]), f2(a[p + 3], b[p + 3]),
-                 f2(a[p + 4], b[p + 4]), L2, R2);
-        f2u(L2, La[p], Lb[p]);
-        f2u(R2, Ra[p], Rb[p]);
-      }
-    } else {
-#pragma unroll
-      for (int p = 0; p < 2; p++) weno_lr_pair(a + p, b + p, La[p], Ra[p], Lb[p], Rb[p]);
-    }
-  } else {
-#pragma unroll
-    for (int p = 0; p < 2; p++) {
-      recon_lr<R>(C, a, p + 2, La[p], Ra[p]);
-      recon_lr<R>(C, b, p + 2, Lb[p], Rb[p]);
-    }
-  }
-}
-
-template <class R, int DIR, int NC>
-__device__ __forceinline__ void dir_tile2(const DevCfg& C, const DevPtrs<R>& P, int use_b, R tau, R inv_h,
-                                          int first, int bx, int by, int bz, DirSmem2<R, DIR, NC>& sm) {
-  using S = DirSmem2<R, DIR, NC>;
-  constexpr int NA = S::NA, TL = S::TL, LD = S::LD;
-  const int tid = threadIdx.x;
-  int lo, hi, galong;
-  if (DIR == 0) { lo = C.il; hi = C.ir; galong = C.gx; }
-  else if (DIR == 1) { lo = C.jl; hi = C.jr; galong = C.gy; }
-  else { lo = C.kl; hi = C.kr; galong = C.gz; }
-  const int a0 = lo - NG + bx * TL;  // global along index of local 0
-  const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)C.gx : (long long)C.gx * C.gy);
-  auto cross_base = [&](int c, bool& ok) -> long long {
-    int i, j, k;
-    if (DIR == 0) { i = 0; j = C.jl + by * NC + c; k = C.kl + bz; ok = j < C.jr; }
-    else if (DIR == 1) { i = C.il + by * NC + c; j = 0; k = C.kl + bz; ok = i < C.ir; }
-    else { i = C.il + by * NC + c; j = C.jl + bz; k = 0; ok = i < C.ir; }
-    return cix(C, i, j, k);
-  };
-
-  // ---- load and per-cell terms, two cells per thread (x-fastest order)
-#pragma unroll
-  for (int half = 0; half < 2; half++) {
-    const int q = tid + half * 32 * NC;
-    const int ta = DIR == 0 ? q % NA : q / NC;
-    const int tc = DIR == 0 ? q / NA : q % NC;
-    bool ok;
-    const long long cb = cross_base(tc, ok);
-    const int g = a0 + ta;
-    const int s = tc * LD + ta;
-    R F[9], V[9], spd = 0, uu[4] = {0, 0, 0, 0};
-    if (ok && g >= 0 && g < galong) {
-      const long long c = cb + (long long)g * stride;
-      R p[5], T[4];
-      const R e = P.e()[c];
-#pragma unroll
-      for (int l = 0; l < 4; l++) uu[l] = P.u(l)[c];
-#pragma unroll
-      for (int l = 0; l < 4; l++) T[l] = P.S(use_b, l)[c];
-#pragma unroll
-      for (int l = 0; l < 5; l++) p[l] = P.S(use_b, 4 + l)[c];
-      cell_terms<R, DIR>(C, tau, e, uu, p, T, g >= lo && g < hi, F, V, spd);
-    } else {
-#pragma unroll
-      for (int l = 0; l < 9; l++) { F[l] = 0; V[l] = 0; }
-    }
-#pragma unroll
-    for (int l = 0; l < 9; l++) { sm.fv[l][s][0] = F[l]; sm.fv[l][s][1] = V[l]; }
-    sm.spd[s] = spd;
-#pragma unroll
-    for (int l = 0; l < 4; l++) sm.up[l >> 1][s][l & 1] = uu[l];
-  }
-  __syncthreads();
-
-  // ---- one warp per line; lane a: cells t0 = 2a, t1 = 2a + 1
-  const int a = tid & 31, c = tid >> 5;
-  bool ok;
-  const long long cb = cross_base(c, ok);
-  if (!ok) return;  // whole warp (no barrier follows)
-  const int t0 = 2 * a;
-  const int row = c * LD;
-  const bool stencil = a >= 1 && a <= 30;  // positions 2a-2 .. 2a+3 inside the line
-  const int sb = row + (stencil ? t0 - 2 : 0);  // first stencil position (even)
-  const int g0 = a0 + t0;
-  // faces: m between t0 and t1 (position t0 + 1/2), r between t1 and the next
-  // lane's t0 (t0 + 3/2)
-  R am = 0, ar = 0;
-  {
-    R sp[6];
-#pragma unroll
-    for (int k = 0; k < 6; k++) sp[k] = sm.spd[sb + k];
-    R L[2] = {0, 0}, Rr[2] = {0, 0};
-    if (stencil) {
-#pragma unroll
-      for (int p = 0; p < 2; p++) recon_lr<R>(C, sp, p + 2, L[p], Rr[p]);
-    }
-    const R Rn = shfl_dn<R>(Rr[0], 1);
-    // the face left of the first interior cell takes no dissipation
-    // (NEWEST5/hydroKT.h:265-314 vs 435-440)
-    am = (g0 + 1 == lo) ? (R)0 : fmax(fabs(L[0]), fabs(Rr[1]));
-    ar = (g0 + 2 == lo) ? (R)0 : fmax(fabs(L[1]), fabs(Rn));
-  }
-  const bool out0 = t0 >= 3 && t0 < 3 + TL && g0 < hi;
-  const bool out1 = t0 + 1 >= 3 && t0 + 1 < 3 + TL && g0 + 1 < hi;
-  const long long cell0 = cb + (long long)g0 * stride, cell1 = cell0 + stride;
-  R racc0[9], racc1[9];
-#pragma unroll
-  for (int l = 0; l < 9; l++) {
-    racc0[l] = (!first && out0) ? P.res(l)[cell0] : (R)0;
-    racc1[l] = (!first && out1) ? P.res(l)[cell1] : (R)0;
-  }
-#pragma unroll 1
-  for (int l = 0; l < 9; l++) {
-    R fl[2] = {0, 0}, fr[2] = {0, 0}, vl[2] = {0, 0}, vr[2] = {0, 0};
-    if (stencil) {
-      R qa[6], qb[6];
-      ld_pairs6<R>(reinterpret_cast<const R(*)[2]>(sm.fv[l]), sb, qa, qb);
-      recon2_pair<R>(C, qa, qb, fl, fr, vl, vr);
-    }
-    const R frn = shfl_dn<R>(fr[0], 1), vrn = shfl_dn<R>(vr[0], 1);
-    const R Hm = (R)0.5 * (fl[0] + fr[1]) - (R)0.5 * am * (vr[1] - vl[0]);  // face t0 + 1/2
-    const R Hr = (R)0.5 * (fl[1] + frn) - (R)0.5 * ar * (vrn - vl[1]);     // face t0 + 3/2
-    const R Hl = shfl_up<R>(Hr, 1);                                          // face t0 - 1/2
-    if (out0) {
-      const R r = -inv_h * (Hm - Hl);
-      P.res(l)[cell0] = first ? r : racc0[l] + r;
-    }
-    if (out1) {
-      const R r = -inv_h * (Hr - Hm);
-      P.res(l)[cell1] = first ? r : racc1[l] + r;
-    }
-  }
-  // velocity derivatives along DIR: (L - R)/h of the same stencils
-  if (out0 || out1) {
-#pragma unroll
-    for (int l = 0; l < 4; l += 2) {
-      R qa[6], qb[6], La[2], Ra[2], Lb[2], Rb[2];
-      ld_pairs6<R>(reinterpret_cast<const R(*)[2]>(sm.up[l >> 1]), sb, qa, qb);
-      // the derivative is WENO in every reconstruction mode (genWENOder)
-      if constexpr (sizeof(R) == 4) {
-#pragma unroll
-        for (int p = 0; p < 2; p++) {
-          F2 L2, R2;
-          weno_lr2(f2(qa[p], qb[p]), f2(qa[p + 1], qb[p + 1]), f2(qa[p + 2], qb[p + 2]), f2(qa[p + 3], qb[p + 3]),
-                   f2(qa[p + 4], qb[p + 4]), L2, R2);
-          f2u(L2, La[p], Lb[p]);
-          f2u(R2, Ra[p], Rb[p]);
-        }
-      } else {
-#pragma unroll
-        for (int p = 0; p < 2; p++) weno_lr_pair(qa + p, qb + p, La[p], Ra[p], Lb[p], Rb[p]);
-      }
-      if (out0) {
-        P.du(l * 3 + DIR)[cell0] = (La[0] - Ra[0]) * inv_h;
-        P.du((l + 1) * 3 + DIR)[cell0] = (Lb[0] - Rb[0]) * inv_h;
-      }
-      if (out1) {
-        P.du(l * 3 + DIR)[cell1] = (La[1] - Ra[1]) * inv_h;
-        P.du((l + 1) * 3 + DIR)[cell1] = (Lb[1] - Rb[1]) * inv_h;
-      }
-    }
-  }
-}
-
-template <class R, int DIR>
-__global__ void __launch_bounds__(32 * Tile2<R, DIR>::NC)
-    k_dir2(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, int first) {
-  using S = DirSmem2<R, DIR>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  pdl_wait_then_release();
-  if (*P.status) return;
-  dir_tile2<R, DIR, S::NC>(C, P, use_b, tau, inv_h, first, blockIdx.x, blockIdx.y, blockIdx.z,
-                           *reinterpret_cast<S*>(smem_raw));
-}
-
 template <class R, int DIR>
 __global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
     k_dir(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, R h, int first) {
