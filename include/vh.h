@@ -265,6 +265,13 @@ int vh_time_kernels(vh_handle* h, int nsteps, double* ms_out);
 /* Newton iterations of the last step, summed over cells (diagnostic). */
 int vh_last_iterations(vh_handle* h, long long* iters);
 
+/* How the flux sweeps read their tiles (diagnostic): *tma = 1 when each
+ * tile is staged in shared memory by tensor-memory-accelerator box copies
+ * (cp.async.bulk.tensor from tensor maps over the state), 0 when the
+ * threads load it through the cache.  TMA is the default; VH_TMA=0 in the
+ * environment at vh_create selects the cached loads (same arithmetic). */
+int vh_sweep_uses_tma(const vh_handle* h, int* tma);
+
 /* Step without allocating: the FP64 step of vh_step on device memory the
  * caller owns, for callers that must not call cudaMalloc where they step the
  * fluid (a device memory pool owned by another framework, whose budget a
@@ -372,10 +379,8 @@ int vh_eps_p(vh_handle* h, double* eps_p);
  *               T^{tau mu} = (e + P) u^tau u^mu - P g^{tau mu} + pi^{tau mu}
  *               re-derived from e at fixed u and pi (ghost cells included);
  *   grad_etas   2 doubles: d eps_p / d (etas0, etas1) of vh_config.
- * The handle is left at the final state.  In the mixed mode the forward and
- * its recomputations run the FP32 step, and the reverse sweep runs in FP64
- * on the recorded FP32 trajectory (the records promoted to FP64 segment by
- * segment). */
+ * The handle is left at the final state.  In the mixed mode the adjoint runs
+ * in FP32 with the implicit-function solve in FP64. */
 int vh_adjoint_eps_p(vh_handle* h, int nsteps, int checkpoint_every, double* eps_p, double* grad_state,
                      double* grad_e, double* grad_etas);
 /* Device milliseconds of the last vh_adjoint_eps_p on this handle: [0] the

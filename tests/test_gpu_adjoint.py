@@ -196,9 +196,10 @@ def test_glauber_128_fp64_to_tau_7_2():
 
 
 def test_glauber_128_mixed_against_fp64():
-    """the mixed adjoint (FP32 forward, FP64 reverse on the recorded FP32
-    trajectory) against the FP64 adjoint and the FP64 forward's finite
-    differences, 100 steps"""
+    """the mixed adjoint (FP32, implicit-function solve in FP64) against the
+    FP64 adjoint and the FP64 forward's finite differences, 100 steps; the
+    agreement is bounded by the FP32 trajectory, which the FP64 gradient is
+    sensitive to (a 1e-7 perturbation of e0 moves its field by 1e-3)"""
     ev = Event(side=128, nsteps=100)
     eps64, _, ge64, gc64 = ev.adjoint(every=25)
     eps32, _, ge32, gc32 = ev.adjoint(every=25, precision=A.PREC_MIXED)

@@ -72,6 +72,7 @@ SIGNATURES = [
     ("vh_debug_stage_terms", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp]),
     ("vh_time_kernels", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     ("vh_last_iterations", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    ("vh_sweep_uses_tma", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("vh_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("vh_step_static", ctypes.c_int, [ctypes.POINTER(VhConfig), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                       ctypes.c_int, ctypes.c_void_p]),

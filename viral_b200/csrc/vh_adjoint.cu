@@ -23,7 +23,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <type_traits>
 #include <vector>
 
 #include "vh.h"
@@ -64,7 +63,7 @@ template <class R>
 __device__ __forceinline__ void du_space(const DevCfg& C, const R* U, long long n, long long c, R* du9) {
 #pragma unroll
   for (int d = 0; d < 2; d++) {
-    const long long s = d == 0 ? 1 : C.gx;
+    const long long s = d == 0 ? 1 : C.px;
     const R h = (R)(d == 0 ? C.dx : C.dy);
 #pragma unroll
     for (int l = 0; l < 3; l++) {
@@ -316,7 +315,7 @@ __device__ __forceinline__ void adj_line(const DirArgs<R>& a, int line, R* sm) {
   const long long n = a.n;
   const int G = DIR == 0 ? C.gx : C.gy;
   const int lo = DIR == 0 ? C.il : C.jl, hi = DIR == 0 ? C.ir : C.jr;
-  const long long stride = DIR == 0 ? 1 : C.gx;
+  const long long stride = DIR == 0 ? 1 : C.px;
   const long long base = DIR == 0 ? cix(C, 0, C.jl + line, 0) : cix(C, C.il + line, 0, 0);
   const double hh = DIR == 0 ? C.dx : C.dy;
   const R h = (R)hh, inv_h = (R)(1.0 / hh);
@@ -437,7 +436,7 @@ __device__ __forceinline__ void adj_line(const DirArgs<R>& a, int line, R* sm) {
 // blockIdx.y = direction, blockIdx.x = line
 template <class R>
 __global__ void __launch_bounds__(DirShape<R>::threads, 2) k_adj_dir(DirArgs<R> a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
   if (blockIdx.y == 0) {
     if ((int)blockIdx.x < a.C.ny) adj_line<R, 0>(a, blockIdx.x, sm);
@@ -486,14 +485,14 @@ __global__ void k_obs_final(const double* part, int nb, double* out) {
 }
 
 // adjoint seed: d eps_p / d (e, u^x, u^y, pi^xx, pi^yy) of the final state
-template <class R, class A>
-__global__ void k_obs_seed(DevCfg C, const R* S, long long n, const double* nd, A* xo) {
+template <class R>
+__global__ void k_obs_seed(DevCfg C, const R* S, long long n, const double* nd, R* xo) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)C.nx * C.ny) return;
   const int i = C.il + (int)(t % C.nx), j = C.jl + (int)(t / C.nx);
   const long long c = cix(C, i, j, 0);
-  A eb, u1b, u2b, p1b, p2b;
-  obs_cell_vjp<A>(C, (A)S[c], (A)S[2 * n + c], (A)S[3 * n + c], nd[0], nd[1], eb, u1b, u2b, p1b, p2b);
+  R eb, u1b, u2b, p1b, p2b;
+  obs_cell_vjp<R>(C, S[c], S[2 * n + c], S[3 * n + c], nd[0], nd[1], eb, u1b, u2b, p1b, p2b);
   xo[XE * n + c] = eb;
   xo[(XU0 + 1) * n + c] = u1b;
   xo[(XU0 + 2) * n + c] = u2b;
@@ -504,8 +503,8 @@ __global__ void k_obs_seed(DevCfg C, const R* S, long long n, const double* nd, 
 // gradients of the initial state: the 18 canonical fields (every field an
 // independent variable) and the energy density of vh_init_profile (T^{tau mu}
 // re-derived from e at fixed u and pi)
-template <class R, class A>
-__global__ void k_adj_final(DevCfg C, const R* X0, long long n, const A* xo, const A* xd, double* gs, double* ge) {
+template <class R>
+__global__ void k_adj_final(DevCfg C, const R* X0, long long n, const R* xo, const R* xd, double* gs, double* ge) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   double v[NX];
@@ -527,13 +526,6 @@ __global__ void k_adj_final(DevCfg C, const R* X0, long long n, const A* xo, con
     ge[c] = v[XE] + v[XT0] * ((1 + dP) * u0 * u0 - dP) + v[XT0 + 1] * (1 + dP) * u0 * u1 +
             v[XT0 + 2] * (1 + dP) * u0 * u2;
   }
-}
-
-// the recorded FP32 trajectory promoted to FP64 for the reverse sweep
-__global__ void k_promote(const float* src, double* dst, long long count) {
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
-       t += (long long)gridDim.x * blockDim.x)
-    dst[t] = (double)src[t];
 }
 
 __global__ void k_sum_cells(const double* cacc, long long n, double* out2) {
@@ -624,19 +616,12 @@ struct PhaseClock {
   }
 };
 
-// R: the forward's precision (the trajectory and its records); A: the
-// reverse sweep's.  The mixed mode runs its FP32 step forward and the
-// reverse in FP64 on the recorded trajectory promoted to FP64 (A = double):
-// the adjoint of the FP64 step linearised along the FP32 trajectory, whose
-// reverse sums then carry no FP32 rounding.
-template <class R, class A = R>
+template <class R>
 int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double* eps_p, double* grad_state,
                 double* grad_e, double* grad_etas) {
   const DevCfg& C = h->C;
   const long long n = C.n;
   const size_t nb = (size_t)n * sizeof(R);
-  const size_t na = (size_t)n * sizeof(A);
-  constexpr bool promote = !std::is_same<R, A>::value;
   cudaStream_t st = h->stream;
   const int nseg = (nsteps + every - 1) / every;
   const int seg_len = std::min(every, nsteps);
@@ -648,23 +633,20 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
 
   // ---- workspace
   Carve cv;
-  auto layout = [&](Carve& c, R** ck, R** fin, R** Xr, R** Yr, A** XrA, A** YrA, A** xo, A** xd, A** yo, A** yd,
-                    A** resb, A** dub, A** v1tb, double** cacc, double** part, double** nd, double** sums,
-                    unsigned** ast, double** gs, double** ge) {
+  auto layout = [&](Carve& c, R** ck, R** fin, R** Xr, R** Yr, R** xo, R** xd, R** yo, R** yd, R** resb, R** dub,
+                    R** v1tb, double** cacc, double** part, double** nd, double** sums, unsigned** ast, double** gs,
+                    double** ge) {
     *ck = c.take<R>((size_t)nseg * 18 * n);
     *fin = c.take<R>((size_t)18 * n);
     *Xr = c.take<R>((size_t)(seg_len + 1) * 18 * n);
     *Yr = c.take<R>((size_t)seg_len * kRecY * n);
-    // the records in the reverse's precision (the same buffers when A = R)
-    *XrA = promote ? c.take<A>((size_t)(seg_len + 1) * 18 * n) : reinterpret_cast<A*>(*Xr);
-    *YrA = promote ? c.take<A>((size_t)seg_len * kRecY * n) : reinterpret_cast<A*>(*Yr);
-    *xo = c.take<A>((size_t)NXO * n);
-    *xd = c.take<A>((size_t)2 * NX * n);
-    *yo = c.take<A>((size_t)NX * n);
-    *yd = c.take<A>((size_t)2 * NX * n);
-    *resb = c.take<A>((size_t)6 * n);
-    *dub = c.take<A>((size_t)6 * n);
-    *v1tb = c.take<A>((size_t)3 * n);
+    *xo = c.take<R>((size_t)NXO * n);
+    *xd = c.take<R>((size_t)2 * NX * n);
+    *yo = c.take<R>((size_t)NX * n);
+    *yd = c.take<R>((size_t)2 * NX * n);
+    *resb = c.take<R>((size_t)6 * n);
+    *dub = c.take<R>((size_t)6 * n);
+    *v1tb = c.take<R>((size_t)3 * n);
     *cacc = c.take<double>((size_t)2 * n);
     *part = c.take<double>((size_t)2 * kObsBlocks);
     *nd = c.take<double>(2);
@@ -673,12 +655,11 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
     *gs = c.take<double>((size_t)18 * n);
     *ge = c.take<double>((size_t)n);
   };
-  R *ck, *fin, *Xr, *Yr;
-  A *XrA, *YrA, *xo, *xd, *yo, *yd, *resb, *dub, *v1tb;
+  R *ck, *fin, *Xr, *Yr, *xo, *xd, *yo, *yd, *resb, *dub, *v1tb;
   double *cacc, *part, *nd, *sums, *gs_dev, *ge_dev;
   unsigned* ast;
-  layout(cv, &ck, &fin, &Xr, &Yr, &XrA, &YrA, &xo, &xd, &yo, &yd, &resb, &dub, &v1tb, &cacc, &part, &nd, &sums, &ast,
-         &gs_dev, &ge_dev);
+  layout(cv, &ck, &fin, &Xr, &Yr, &xo, &xd, &yo, &yd, &resb, &dub, &v1tb, &cacc, &part, &nd, &sums, &ast, &gs_dev,
+         &ge_dev);
   if (cv.off > h->adj_bytes) {
     VH_CUDA(h, cudaStreamSynchronize(st));
     cudaFree(h->adj_buf);
@@ -694,21 +675,10 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
   }
   Carve cw;
   cw.base = static_cast<char*>(h->adj_buf);
-  layout(cw, &ck, &fin, &Xr, &Yr, &XrA, &YrA, &xo, &xd, &yo, &yd, &resb, &dub, &v1tb, &cacc, &part, &nd, &sums, &ast,
-         &gs_dev, &ge_dev);
-  const size_t smem = dir_smem<A>(C);
-  VH_CUDA(h, cudaFuncSetAttribute(k_adj_dir<A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  // copy the segment's records into the reverse's precision
-  auto promote_records = [&](int m) -> int {
-    if constexpr (promote) {
-      const long long cx = (long long)(m + 1) * 18 * n, cy = (long long)m * kRecY * n;
-      k_promote<<<1184, 256, 0, st>>>(Xr, XrA, cx);
-      k_promote<<<1184, 256, 0, st>>>(Yr, YrA, cy);
-      VH_CUDA(h, cudaGetLastError());
-    }
-    (void)m;
-    return VH_OK;
-  };
+  layout(cw, &ck, &fin, &Xr, &Yr, &xo, &xd, &yo, &yd, &resb, &dub, &v1tb, &cacc, &part, &nd, &sums, &ast, &gs_dev,
+         &ge_dev);
+  const size_t smem = dir_smem<R>(C);
+  VH_CUDA(h, cudaFuncSetAttribute(k_adj_dir<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   PhaseClock clk;
   int t_start, t_fwd, t_end;
   VH_CUDA(h, clk.mark(st, &t_start));
@@ -739,26 +709,26 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
   double ndh[2];
   if ((r = eps_p_device<R>(h, state, part, nd, ndh))) return r;
   if (eps_p) *eps_p = ndh[0] / ndh[1];
-  VH_CUDA(h, cudaMemsetAsync(xo, 0, NXO * na, st));
-  VH_CUDA(h, cudaMemsetAsync(xd, 0, 2 * NX * na, st));
-  VH_CUDA(h, cudaMemsetAsync(yo, 0, NX * na, st));
-  VH_CUDA(h, cudaMemsetAsync(yd, 0, 2 * NX * na, st));
-  VH_CUDA(h, cudaMemsetAsync(resb, 0, 6 * na, st));
-  VH_CUDA(h, cudaMemsetAsync(dub, 0, 6 * na, st));
-  VH_CUDA(h, cudaMemsetAsync(v1tb, 0, 3 * na, st));
+  VH_CUDA(h, cudaMemsetAsync(xo, 0, NXO * nb, st));
+  VH_CUDA(h, cudaMemsetAsync(xd, 0, 2 * NX * nb, st));
+  VH_CUDA(h, cudaMemsetAsync(yo, 0, NX * nb, st));
+  VH_CUDA(h, cudaMemsetAsync(yd, 0, 2 * NX * nb, st));
+  VH_CUDA(h, cudaMemsetAsync(resb, 0, 6 * nb, st));
+  VH_CUDA(h, cudaMemsetAsync(dub, 0, 6 * nb, st));
+  VH_CUDA(h, cudaMemsetAsync(v1tb, 0, 3 * nb, st));
   VH_CUDA(h, cudaMemsetAsync(cacc, 0, 2 * n * sizeof(double), st));
   VH_CUDA(h, cudaMemsetAsync(ast, 0, sizeof(unsigned), st));
   const long long nint = (long long)C.nx * C.ny;
-  k_obs_seed<R, A><<<grid1(nint, 128), 128, 0, st>>>(C, state, n, nd, xo);
+  k_obs_seed<R><<<grid1(nint, 128), 128, 0, st>>>(C, state, n, nd, xo);
   VH_CUDA(h, cudaGetLastError());
 
-  AdjArgs<A> a{};
+  AdjArgs<R> a{};
   a.C = C; a.n = n; a.xo = xo; a.xd = xd; a.yo = yo; a.yd = yd; a.resb = resb; a.dub = dub; a.v1tb = v1tb;
   a.cacc = cacc; a.status = ast; a.ts = ts;
-  DirArgs<A> d{};
+  DirArgs<R> d{};
   d.C = C; d.n = n; d.resb = resb; d.dub = dub;
   const int G = std::max(C.gx, C.gy);
-  const int dthreads = DirShape<A>::threads;
+  const int dthreads = DirShape<R>::threads;
   const dim3 dgrid(std::max(C.nx, C.ny), 2);
 
   // ---- reverse, one segment at a time
@@ -775,20 +745,19 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
       }
       VH_CUDA(h, cudaMemcpyAsync(Xr + (size_t)m * 18 * n, state, 18 * nb, cudaMemcpyDeviceToDevice, st));
     }
-    if ((r = promote_records(m))) return r;
     VH_CUDA(h, clk.mark(st, &t1));
     for (int q = m - 1; q >= 0; q--) {
       const double tau = taus[s0 + q];
-      a.X = XrA + (size_t)q * 18 * n;
-      a.Y = YrA + (size_t)q * kRecY * n;
-      a.X1 = XrA + (size_t)(q + 1) * 18 * n;
+      a.X = Xr + (size_t)q * 18 * n;
+      a.Y = Yr + (size_t)q * kRecY * n;
+      a.X1 = Xr + (size_t)(q + 1) * 18 * n;
       a.tau_n = tau;
-      k_adj_stage2<A><<<grid1(nint, 128), 128, 0, st>>>(a);
-      d.rec = a.Y; d.kind = REC_Y; d.tau_s = (A)(tau + ts); d.out = yd;
-      k_adj_dir<A><<<dgrid, dthreads, smem, st>>>(d);
-      k_adj_stage1<A><<<grid1(nint, 128), 128, 0, st>>>(a);
-      d.rec = a.X; d.kind = REC_X; d.tau_s = (A)tau; d.out = xd;
-      k_adj_dir<A><<<dgrid, dthreads, smem, st>>>(d);
+      k_adj_stage2<R><<<grid1(nint, 128), 128, 0, st>>>(a);
+      d.rec = a.Y; d.kind = REC_Y; d.tau_s = (R)(tau + ts); d.out = yd;
+      k_adj_dir<R><<<dgrid, dthreads, smem, st>>>(d);
+      k_adj_stage1<R><<<grid1(nint, 128), 128, 0, st>>>(a);
+      d.rec = a.X; d.kind = REC_X; d.tau_s = (R)tau; d.out = xd;
+      k_adj_dir<R><<<dgrid, dthreads, smem, st>>>(d);
       VH_CUDA(h, cudaGetLastError());
     }
     VH_CUDA(h, clk.mark(st, &t2));
@@ -799,16 +768,16 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
   if ((r = read_status(h))) return r;
 
   // ---- gradients of the initial state and of (etas0, etas1)
-  k_adj_final<R, A><<<grid1(n, 256), 256, 0, st>>>(C, ck, n, xo, xd, grad_state ? gs_dev : nullptr,
-                                                     grad_e ? ge_dev : nullptr);
+  k_adj_final<R><<<grid1(n, 256), 256, 0, st>>>(C, ck, n, xo, xd, grad_state ? gs_dev : nullptr,
+                                                  grad_e ? ge_dev : nullptr);
   k_sum_cells<<<1, 256, 0, st>>>(cacc, n, sums);
   VH_CUDA(h, cudaGetLastError());
   double cs[2];
   unsigned astat = 0;
   VH_CUDA(h, cudaMemcpyAsync(cs, sums, sizeof(cs), cudaMemcpyDeviceToHost, st));
   VH_CUDA(h, cudaMemcpyAsync(&astat, ast, sizeof(astat), cudaMemcpyDeviceToHost, st));
-  if (grad_state) VH_CUDA(h, cudaMemcpyAsync(grad_state, gs_dev, 18 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
-  if (grad_e) VH_CUDA(h, cudaMemcpyAsync(grad_e, ge_dev, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (grad_state && (r = pitched_out(h, grad_state, gs_dev, 18))) return r;
+  if (grad_e && (r = pitched_out(h, grad_e, ge_dev, 1))) return r;
   // leave the handle at the final state
   VH_CUDA(h, cudaMemcpyAsync(state, fin, 18 * nb, cudaMemcpyDeviceToDevice, st));
   VH_CUDA(h, clk.mark(st, &t_end));
@@ -860,10 +829,9 @@ extern "C" int vh_adjoint_eps_p(vh_handle* h, int nsteps, int checkpoint_every, 
   if (C.cart || !C.bi || C.mirror || C.recon != VH_RECON_WENO5 || C.cold)
     return fail(h, VH_E_UNSUPPORTED,
                 "vh_adjoint_eps_p: boost-invariant Milne grids with WENO reconstruction and copy boundaries only");
-  const size_t smem = dir_smem<double>(C);
+  const size_t smem = h->mixed ? dir_smem<float>(C) : dir_smem<double>(C);
   if (smem > 227 * 1024)
     return fail(h, VH_E_UNSUPPORTED, "vh_adjoint_eps_p: grid line too long for the line kernel");
-  return h->mixed ? adjoint_run<float, double>(h, h->pf, nsteps, checkpoint_every, eps_p, grad_state, grad_e,
-                                               grad_etas)
+  return h->mixed ? adjoint_run<float>(h, h->pf, nsteps, checkpoint_every, eps_p, grad_state, grad_e, grad_etas)
                   : adjoint_run<double>(h, h->pd, nsteps, checkpoint_every, eps_p, grad_state, grad_e, grad_etas);
 }

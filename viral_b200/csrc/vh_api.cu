@@ -55,9 +55,16 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
   DevCfg& C = h->C;
   C.nx = cfg->nx; C.ny = cfg->ny; C.nz = cfg->boost_invariant ? 1 : cfg->nz;
   C.gx = cfg->nx + 2 * NG; C.gy = cfg->ny + 2 * NG; C.gz = cfg->boost_invariant ? 1 : cfg->nz + 2 * NG;
+  // rows padded to a multiple of 8 cells (32 bytes in FP32, 64 in FP64), so
+  // that every row of every array starts on a 32-byte sector: the y and eta
+  // sweeps' tiles (8 lines across x, starting at multiples of 8 cells) then
+  // read and write whole sectors, and the TMA tiles' strides are multiples
+  // of 16 bytes as the tensor maps require.  The padding cells are never
+  // read; the C ABI's arrays keep the canonical unpadded layout.
+  C.px = (C.gx + 7) / 8 * 8;
   C.il = NG; C.ir = NG + cfg->nx; C.jl = NG; C.jr = NG + cfg->ny;
   C.kl = cfg->boost_invariant ? 0 : NG; C.kr = cfg->boost_invariant ? 1 : NG + cfg->nz;
-  C.n = (long long)C.gx * C.gy * C.gz;
+  C.n = (long long)C.px * C.gy * C.gz;
   C.cart = cfg->coords == VH_COORD_CARTESIAN;
   C.bi = cfg->boost_invariant != 0;
   C.recon = cfg->recon;
@@ -71,6 +78,7 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
   C.mm_theta = cfg->minmod_theta;
   h->tau = cfg->tau0;
   if (const char* v = std::getenv("VH_PDL")) h->pdl = std::strcmp(v, "0") != 0;
+  if (const char* v = std::getenv("VH_TMA")) h->tma_wanted = std::strcmp(v, "0") != 0;
 
   auto bail = [&](cudaError_t e, const char* what) {
     g_create_err = std::string("vh_create: ") + what + ": " + cudaGetErrorString(e);
@@ -125,7 +133,7 @@ extern "C" int vh_destroy(vh_handle* h) {
   if (!h) return VH_OK;
   cudaFree(h->state); cudaFree(h->stage); cudaFree(h->eos_d); cudaFree(h->eos_f);
   cudaFree(h->status); cudaFree(h->iters); cudaFree(h->red); cudaFree(h->part);
-  cudaFree(h->adj_buf); cudaFree(h->fo_prev);
+  cudaFree(h->adj_buf); cudaFree(h->fo_prev); cudaFree(h->xfer);
   delete h;
   return VH_OK;
 }
@@ -143,58 +151,54 @@ extern "C" int vh_dims(const vh_handle* h, int* gx, int* gy, int* gz) {
 }
 
 
-// device canonical doubles (18*n) -> state
-static int import_device(vh_handle* h, const double* dev) {
+// canonical doubles (18 fields; host or device) -> state
+static int import_state(vh_handle* h, const double* canon) {
   const long long n18 = 18 * h->C.n;
   if (h->mixed) {
-    k_d2f<<<grid1(n18, 256), 256, 0, h->stream>>>(dev, static_cast<float*>(h->state), n18);
-  } else if (dev != h->state) {
-    VH_CUDA(h, cudaMemcpyAsync(h->state, dev, sizeof(double) * n18, cudaMemcpyDeviceToDevice, h->stream));
+    if (int r = pitched_in(h, h->stage, canon, 18)) return r;
+    k_d2f<<<grid1(n18, 256), 256, 0, h->stream>>>(h->stage, static_cast<float*>(h->state), n18);
+  } else if (canon != h->state) {
+    if (int r = pitched_in(h, static_cast<double*>(h->state), canon, 18)) return r;
   }
   VH_CUDA(h, cudaGetLastError());
   return VH_OK;
 }
-static int export_device(vh_handle* h, double* dev) {
+static int export_state(vh_handle* h, double* canon) {
   const long long n18 = 18 * h->C.n;
-  if (h->mixed) k_f2d<<<grid1(n18, 256), 256, 0, h->stream>>>(static_cast<const float*>(h->state), dev, n18);
-  else VH_CUDA(h, cudaMemcpyAsync(dev, h->state, sizeof(double) * n18, cudaMemcpyDeviceToDevice, h->stream));
-  VH_CUDA(h, cudaGetLastError());
-  return VH_OK;
+  if (h->mixed) {
+    k_f2d<<<grid1(n18, 256), 256, 0, h->stream>>>(static_cast<const float*>(h->state), h->stage, n18);
+    VH_CUDA(h, cudaGetLastError());
+    return pitched_out(h, canon, h->stage, 18);
+  }
+  return pitched_out(h, canon, static_cast<const double*>(h->state), 18);
 }
 
-extern "C" int vh_set_state_device(vh_handle* h, const double* dev, double tau) {
-  if (!h || !dev) return VH_E_ARG;
-  int r = import_device(h, dev);
-  if (r) return r;
+static int state_was_set(vh_handle* h, double tau) {
   h->tau = tau;
   h->have_state = true;
   h->fo_have = false;
   VH_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(unsigned int), h->stream));
   return VH_OK;
 }
+extern "C" int vh_set_state_device(vh_handle* h, const double* dev, double tau) {
+  if (!h || !dev) return VH_E_ARG;
+  if (int r = import_state(h, dev)) return r;
+  return state_was_set(h, tau);
+}
 extern "C" int vh_get_state_device(vh_handle* h, double* dev) {
   if (!h || !dev) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
-  return export_device(h, dev);
+  return export_state(h, dev);
 }
 extern "C" int vh_set_state(vh_handle* h, const double* host, double tau) {
   if (!h || !host) return VH_E_ARG;
-  const long long n18 = 18 * h->C.n;
-  double* dst = h->mixed ? h->stage : static_cast<double*>(h->state);
-  VH_CUDA(h, cudaMemcpyAsync(dst, host, sizeof(double) * n18, cudaMemcpyHostToDevice, h->stream));
-  return vh_set_state_device(h, dst, tau);
+  if (int r = import_state(h, host)) return r;
+  return state_was_set(h, tau);
 }
 extern "C" int vh_get_state(vh_handle* h, double* host) {
   if (!h || !host) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
-  const long long n18 = 18 * h->C.n;
-  if (h->mixed) {
-    int r = export_device(h, h->stage);
-    if (r) return r;
-    VH_CUDA(h, cudaMemcpyAsync(host, h->stage, sizeof(double) * n18, cudaMemcpyDeviceToHost, h->stream));
-  } else {
-    VH_CUDA(h, cudaMemcpyAsync(host, h->state, sizeof(double) * n18, cudaMemcpyDeviceToHost, h->stream));
-  }
+  if (int r = export_state(h, host)) return r;
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
   return VH_OK;
 }
@@ -265,6 +269,12 @@ extern "C" int vh_get_time(const vh_handle* h, double* tau) {
   return VH_OK;
 }
 
+extern "C" int vh_sweep_uses_tma(const vh_handle* h, int* tma) {
+  if (!h || !tma) return VH_E_ARG;
+  *tma = h->tma ? 1 : 0;
+  return VH_OK;
+}
+
 extern "C" int vh_last_iterations(vh_handle* h, long long* iters) {
   if (!h || !iters) return VH_E_ARG;
   unsigned long long v = 0;
@@ -292,7 +302,7 @@ extern "C" int vh_init_profile(vh_handle* h, double tau, const double* e, const 
   if (!h || !e || !ux || !uy) return VH_E_ARG;
   if (pi_mode != VH_PI_GIVEN && pi_mode != VH_PI_ZERO && pi_mode != VH_PI_NS) return fail(h, VH_E_ARG, "pi_mode");
   if (pi_mode == VH_PI_GIVEN && !pi5) return fail(h, VH_E_ARG, "pi5 is required with VH_PI_GIVEN");
-  const long long n = h->C.n;
+  const long long n = canon_cells(h->C);
   const double t2 = h->C.cart ? 1.0 : tau * tau;
   std::vector<double> f(18 * (size_t)n, 0.0);
   for (long long c = 0; c < n; c++) {
@@ -321,12 +331,13 @@ extern "C" int vh_get_primitive(vh_handle* h, double* e, double* P, double* T, d
   if (h->mixed) k_primitive<float><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pf, h->tau, buf);
   else k_primitive<double><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pd, h->tau, buf);
   VH_CUDA(h, cudaGetLastError());
-  const size_t nb = sizeof(double) * (size_t)n;
-  if (e) VH_CUDA(h, cudaMemcpyAsync(e, buf, nb, cudaMemcpyDeviceToHost, h->stream));
-  if (P) VH_CUDA(h, cudaMemcpyAsync(P, buf + n, nb, cudaMemcpyDeviceToHost, h->stream));
-  if (T) VH_CUDA(h, cudaMemcpyAsync(T, buf + 2 * n, nb, cudaMemcpyDeviceToHost, h->stream));
-  if (u4) VH_CUDA(h, cudaMemcpyAsync(u4, buf + 3 * n, 4 * nb, cudaMemcpyDeviceToHost, h->stream));
-  if (pi10) VH_CUDA(h, cudaMemcpyAsync(pi10, buf + 7 * n, 10 * nb, cudaMemcpyDeviceToHost, h->stream));
+  int r = VH_OK;
+  if (e && !r) r = pitched_out(h, e, buf, 1);
+  if (P && !r) r = pitched_out(h, P, buf + n, 1);
+  if (T && !r) r = pitched_out(h, T, buf + 2 * n, 1);
+  if (u4 && !r) r = pitched_out(h, u4, buf + 3 * n, 4);
+  if (pi10 && !r) r = pitched_out(h, pi10, buf + 7 * n, 10);
+  if (r) return r;
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
   return VH_OK;
 }
@@ -338,25 +349,28 @@ extern "C" int vh_freezeout_step(vh_handle* h, double t_fo, double* out, long lo
   if (h->C.cart) return fail(h, VH_E_UNSUPPORTED, "freeze-out surfaces are built on Milne grids");
   if (c.nx < 2 || c.ny < 2 || (!c.boost_invariant && c.nz < 2))
     return fail(h, VH_E_ARG, "a freeze-out surface needs two cells along every axis");
-  const long long n = h->C.n;
-  const size_t nb = sizeof(double) * (size_t)n;
-  if (!h->fo_prev) VH_CUDA(h, cudaMalloc(&h->fo_prev, 5 * nb));
+  const long long n = h->C.n, nc = canon_cells(h->C);
+  const size_t nb = sizeof(double) * (size_t)nc;
+  // two canonical slices (5 fields each): the kept one and the current one
+  if (!h->fo_prev) VH_CUDA(h, cudaMalloc(&h->fo_prev, 10 * nb));
   // T and u^mu of the current state: rows 2 (T) and 3..6 (u^mu) of the
-  // primitive fields, contiguous
+  // primitive fields, contiguous, in the canonical layout the surface
+  // kernels read
   double* buf = h->stage;
   if (h->mixed) k_primitive<float><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pf, h->tau, buf);
   else k_primitive<double><<<grid1(n, 256), 256, 0, h->stream>>>(h->C, h->pd, h->tau, buf);
   VH_CUDA(h, cudaGetLastError());
-  const double* cur = buf + 2 * n;
+  double* cur = h->fo_prev + 5 * nc;
+  if (int r = pitched_out(h, cur, buf + 2 * n, 5)) return r;
   *count = 0;
   if (h->fo_have) {
     if (!(h->tau > h->fo_tau)) return fail(h, VH_E_STATE, "no step since the last freeze-out slice");
     const double* prev = h->fo_prev;
     const int r = c.boost_invariant
-                      ? vh_freezeout_2d_device(c.nx, c.ny, c.dx, c.dy, h->fo_tau, h->tau, prev, cur, prev + n, cur + n,
-                                               t_fo, out, cap, count, h->stream)
+                      ? vh_freezeout_2d_device(c.nx, c.ny, c.dx, c.dy, h->fo_tau, h->tau, prev, cur, prev + nc,
+                                               cur + nc, t_fo, out, cap, count, h->stream)
                       : vh_freezeout_3d_device(c.nx, c.ny, c.nz, c.dx, c.dy, c.dz, h->fo_tau, h->tau, prev, cur,
-                                               prev + n, cur + n, t_fo, out, cap, count, h->stream);
+                                               prev + nc, cur + nc, t_fo, out, cap, count, h->stream);
     if (r == VH_E_ARG && *count > cap)
       return fail(h, VH_E_ARG, "the surface has " + std::to_string(*count) + " elements, more than cap; the slice "
                                "is kept for a call with room for them");
@@ -382,7 +396,7 @@ static int ns_pi10(vh_handle* h, const DevPtrs<R>& P, double* out) {
 extern "C" int vh_get_conserved(vh_handle* h, double* var10) {
   if (!h || !var10) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
-  const size_t n = (size_t)h->C.n;
+  const size_t n = (size_t)canon_cells(h->C);
   std::vector<double> f(18 * n);
   int r = vh_get_state(h, f.data());
   if (r) return r;
@@ -402,7 +416,8 @@ extern "C" int vh_get_ns_pi(vh_handle* h, double* pi10) {
   double* buf = h->stage;  // 18 x n doubles; 10 are used
   int r = h->mixed ? ns_pi10<float>(h, h->pf, buf) : ns_pi10<double>(h, h->pd, buf);
   if (r) return r;
-  VH_CUDA(h, cudaMemcpyAsync(pi10, buf, 10 * sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+  (void)n;
+  if ((r = pitched_out(h, pi10, buf, 10))) return r;
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
   return VH_OK;
 }
@@ -447,7 +462,7 @@ extern "C" int vh_init_tmunu(vh_handle* h, double tau, const double* tmunu10, lo
   if (!h->C.cart && !(tau > 0)) return fail(h, VH_E_ARG, "Milne tau must be positive");
   const long long n = h->C.n;
   double* buf = h->stage;  // 18 x n doubles; the tensor takes 10
-  VH_CUDA(h, cudaMemcpyAsync(buf, tmunu10, 10 * sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+  if (int r = pitched_in(h, buf, tmunu10, 10)) return r;
   VH_CUDA(h, cudaMemsetAsync(h->red, 0, sizeof(unsigned long long), h->stream));
   if (h->mixed) {
     k_init_tmunu<float><<<grid1(n, 128), 128, 0, h->stream>>>(h->C, h->pf, tau, buf, h->red);
@@ -476,7 +491,7 @@ extern "C" int vh_init_prevu_tmunu(vh_handle* h, double tau_prev, const double* 
   if (!h->C.cart && !(tau_prev > 0)) return fail(h, VH_E_ARG, "Milne tau must be positive");
   const long long n = h->C.n;
   double* buf = h->stage;
-  VH_CUDA(h, cudaMemcpyAsync(buf, tmunu10, 10 * sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+  if (int r = pitched_in(h, buf, tmunu10, 10)) return r;
   VH_CUDA(h, cudaMemsetAsync(h->red, 0, sizeof(unsigned long long), h->stream));
   if (h->mixed) k_prevu_tmunu<float><<<grid1(n, 128), 128, 0, h->stream>>>(h->C, h->pf, tau_prev, buf, h->red);
   else k_prevu_tmunu<double><<<grid1(n, 128), 128, 0, h->stream>>>(h->C, h->pd, tau_prev, buf, h->red);
@@ -547,15 +562,22 @@ static int debug_terms(vh_handle* h, const DevPtrs<R>& P, double* res, double* s
   k_debug_src<R><<<grid1(n, 128), 128, 0, h->stream>>>(C, P, du16, src9, h->tau);
   VH_CUDA(h, cudaGetLastError());
   std::vector<R> tmp(16 * (size_t)n);
+  // device fields (rows of px cells) -> canonical doubles (rows of gx)
+  const long long nc = canon_cells(C), rows = (long long)C.gy * C.gz;
+  auto unpad = [&](double* dst, int nf) {
+    for (int q = 0; q < nf; q++)
+      for (long long r = 0; r < rows; r++)
+        for (int i = 0; i < C.gx; i++) dst[q * nc + r * C.gx + i] = (double)tmp[q * n + r * C.px + i];
+  };
   VH_CUDA(h, cudaMemcpyAsync(tmp.data(), P.res(0), sizeof(R) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
-  for (long long q = 0; q < 9 * n; q++) res[q] = (double)tmp[q];
+  unpad(res, 9);
   VH_CUDA(h, cudaMemcpyAsync(tmp.data(), src9, sizeof(R) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
-  for (long long q = 0; q < 9 * n; q++) src[q] = (double)tmp[q];
+  unpad(src, 9);
   VH_CUDA(h, cudaMemcpyAsync(tmp.data(), du16, sizeof(R) * 16 * n, cudaMemcpyDeviceToHost, h->stream));
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
-  for (long long q = 0; q < 16 * n; q++) du[q] = (double)tmp[q];
+  unpad(du, 16);
   VH_CUDA(h, cudaFreeAsync(src9, h->stream));
   VH_CUDA(h, cudaStreamSynchronize(h->stream));
   return VH_OK;

@@ -10,7 +10,7 @@ namespace vh {
 template <class R>
 __global__ void k_fill_tmunu(DevCfg C, DevPtrs<R> P, double tau) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= C.n) return;
+  if (c >= C.n || c % C.px >= C.gx) return;  // padding cells stay untouched
   const R t2 = C.cart ? (R)1 : (R)(tau * tau);
   R u[4], p[5];
   const R e = P.e()[c];
@@ -34,7 +34,7 @@ template <class R>
 __global__ void k_primitive(DevCfg C, DevPtrs<R> P, double tau, double* out) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long n = C.n;
-  if (c >= n) return;
+  if (c >= n || c % C.px >= C.gx) return;  // not the padding cells
   const R t2 = C.cart ? (R)1 : (R)(tau * tau);
   R u[4], p[5];
   const R e = P.e()[c];
@@ -140,7 +140,7 @@ template <class R>
 __global__ void k_init_tmunu(DevCfg C, DevPtrs<R> P, double tau, const double* T10, unsigned long long* nfail) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long n = C.n;
-  if (c >= n) return;
+  if (c >= n || c % C.px >= C.gx) return;  // not the padding cells
   double t[10], e = 0, u[4] = {1, 0, 0, 0};
 #pragma unroll
   for (int l = 0; l < 10; l++) t[l] = T10[(long long)l * n + c];
@@ -176,7 +176,7 @@ template <class R>
 __global__ void k_prevu_tmunu(DevCfg C, DevPtrs<R> P, double tau, const double* T10, unsigned long long* nfail) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long n = C.n;
-  if (c >= n) return;
+  if (c >= n || c % C.px >= C.gx) return;  // not the padding cells
   double t[10], e = 0, u[4] = {1, 0, 0, 0};
 #pragma unroll
   for (int l = 0; l < 10; l++) t[l] = T10[(long long)l * n + c];
@@ -193,7 +193,7 @@ template <class R>
 __global__ void k_du_full(DevCfg C, DevPtrs<R> P, R* du16, double ts) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C.n) return;
-  const int i = (int)(c % C.gx), j = (int)((c / C.gx) % C.gy), k = (int)(c / ((long long)C.gx * C.gy));
+  const int i = (int)(c % C.px), j = (int)((c / C.px) % C.gy), k = (int)(c / ((long long)C.px * C.gy));
   const bool ii = i >= C.il && i < C.ir, jj = j >= C.jl && j < C.jr, kk = k >= C.kl && k < C.kr;
 #pragma unroll 1
   for (int l = 0; l < 4; l++) {
@@ -206,13 +206,13 @@ __global__ void k_du_full(DevCfg C, DevPtrs<R> P, R* du16, double ts) {
       d1 = (L - Rr) / (R)C.dx;
     }
     if (ii && kk && j >= 2 && j < C.gy - 2) {
-      const long long s = C.gx;
+      const long long s = C.px;
       const R L = weno_left<R>(u[c - 2 * s], u[c - s], u[c], u[c + s], u[c + 2 * s]);
       const R Rr = weno_right<R>(u[c - 2 * s], u[c - s], u[c], u[c + s], u[c + 2 * s]);
       d2 = (L - Rr) / (R)C.dy;
     }
     if (!C.bi && ii && jj) {
-      const long long s = (long long)C.gx * C.gy;
+      const long long s = (long long)C.px * C.gy;
       const int Z = C.gz;
       R qm2, qm1, qc = u[c], qp1, qp2;
       if (k > 1 && k < Z - 2) { qm1 = u[c - s]; qm2 = u[c - 2 * s]; qp1 = u[c + s]; qp2 = u[c + 2 * s]; }
@@ -236,7 +236,7 @@ __global__ void k_du_full(DevCfg C, DevPtrs<R> P, R* du16, double ts) {
 template <class R>
 __global__ void k_ns_pi(DevCfg C, DevPtrs<R> P, const R* du16, double tau) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= C.n) return;
+  if (c >= C.n || c % C.px >= C.gx) return;  // not the padding cells
   R u[4], du[4][4];
   const R e = P.e()[c];
 #pragma unroll
@@ -264,7 +264,7 @@ __global__ void k_ns_pi(DevCfg C, DevPtrs<R> P, const R* du16, double tau) {
 template <class R>
 __global__ void k_ns_pi10(DevCfg C, DevPtrs<R> P, const R* du16, double tau, double* out10) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= C.n) return;
+  if (c >= C.n || c % C.px >= C.gx) return;  // not the padding cells
   double u[4], du[4][4];
   const double e = (double)P.e()[c];
 #pragma unroll
@@ -287,7 +287,7 @@ template <class R>
 __global__ void k_debug_src(DevCfg C, DevPtrs<R> P, const R* du16, R* src9, double tau) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C.n) return;
-  const int i = (int)(c % C.gx), j = (int)((c / C.gx) % C.gy), k = (int)(c / ((long long)C.gx * C.gy));
+  const int i = (int)(c % C.px), j = (int)((c / C.px) % C.gy), k = (int)(c / ((long long)C.px * C.gy));
   for (int l = 0; l < 9; l++) src9[l * C.n + c] = 0;
   if (!(i >= C.il && i < C.ir && j >= C.jl && j < C.jr && k >= C.kl && k < C.kr)) return;
   R u[4], p[5], du[4][4];
@@ -385,7 +385,7 @@ __global__ void k_cfl(DevCfg C, DevPtrs<R> P, double tau, unsigned long long* ou
     const int k = C.kl + (int)(t / ((long long)C.nx * C.ny));
     double a2 = 0;
     for (int d = 0; d < (C.bi ? 2 : 3); d++) {
-      const long long s = d == 0 ? 1 : (d == 1 ? (long long)C.gx : (long long)C.gx * C.gy);
+      const long long s = d == 0 ? 1 : (d == 1 ? (long long)C.px : (long long)C.px * C.gy);
       const int pos = d == 0 ? i : (d == 1 ? j : k);
       const int lo = d == 0 ? C.il : (d == 1 ? C.jl : C.kl), hi = d == 0 ? C.ir : (d == 1 ? C.jr : C.kr);
       R q[6];

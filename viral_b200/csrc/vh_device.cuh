@@ -17,9 +17,10 @@ constexpr int NG = 3;  // ghost layers (NEWEST5/maindef.h:369-371 BORDER)
 // Problem description passed by value to every kernel.
 struct DevCfg {
   int gx, gy, gz;              // ghost-inclusive extents
+  int px;                      // row pitch in cells (>= gx): a handle's rows are padded to 16 bytes
   int il, ir, jl, jr, kl, kr;  // interior bounds
   int nx, ny, nz;
-  long long n;                 // gx*gy*gz
+  long long n;                 // px*gy*gz: cells per array, padding included
   int cart, bi, recon, mirror;
   double dx, dy, dz;
   int eos_kind;
@@ -68,10 +69,10 @@ struct DevPtrs {
   }
 };
 
-enum : unsigned { ST_ROOT = 1u, ST_CAUSAL = 2u, ST_NEGE = 4u };
+enum : unsigned { ST_ROOT = 1u, ST_CAUSAL = 2u, ST_NEGE = 4u, ST_TMA = 8u };
 
 __host__ VH_HD inline long long cix(const DevCfg& C, int i, int j, int k) {
-  return ((long long)k * C.gy + j) * C.gx + i;
+  return ((long long)k * C.gy + j) * C.px + i;
 }
 
 // ------------------------------------------------------------------ EOS

@@ -14,6 +14,8 @@
 //               boundary.h:1-276).
 #pragma once
 
+#include <cuda.h>
+
 #include "vh_device.cuh"
 
 namespace vh {
@@ -193,6 +195,66 @@ __device__ __forceinline__ void pdl_wait_then_release() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// ---- TMA staging of a sweep's tile (cp.async.bulk.tensor, one mbarrier)
+//
+// The state is one 4D tensor (x over the padded row pitch, y, z, array):
+// the 52 arrays back to back.  A tile of the sweep along DIR is two box
+// copies: arrays 0..4 (e, u^mu) and the nine arrays of the conserved set it
+// reads (set A: pi 5..9 then T^{tau mu} 10..13; set B: T^{tau mu} 18..21
+// then pi 22..26).  The box's x start is rounded down to a 16-byte boundary
+// (4 floats, 2 doubles) and the box is wide enough for the tile from there;
+// cells outside the tensor are filled with zeros by the copy and, like the
+// cells outside the grid, never used.
+template <class R, int DIR, int NC>
+struct TmaBox {
+  static constexpr int XA = sizeof(R) == 4 ? 4 : 2;  // x alignment in cells
+  static constexpr int NA = 32;
+  // x extent: along x the 32-cell line plus the shift of the rounded start;
+  // across x the NC lines, whose tiles start at multiples of NC cells
+  static_assert(DIR == 0 || NC % XA == 0, "tiles across x start on 16-byte boundaries");
+  static constexpr int BX = DIR == 0 ? (NA + XA - 1 + XA - 1) / XA * XA : NC;
+  static constexpr int BY = DIR == 0 ? NC : (DIR == 1 ? NA : 1);
+  static constexpr int BZ = DIR == 2 ? NA : 1;
+  static constexpr int CELLS = BX * BY * BZ;
+  static constexpr unsigned BYTES5 = (unsigned)(CELLS * 5 * sizeof(R));
+  static constexpr unsigned BYTES9 = (unsigned)(CELLS * 9 * sizeof(R));
+  // the second box starts on a 128-byte boundary
+  static constexpr int OFF9 = (int)((BYTES5 + 127) / 128 * 128 / sizeof(R));
+  static constexpr size_t SPAN = (size_t)OFF9 * sizeof(R) + BYTES9;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// bounded wait for phase 0 of the barrier; false if it did not complete
+__device__ __forceinline__ bool mbar_wait0(unsigned long long* bar, int max_polls) {
+  for (int k = 0; k < max_polls; k++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(0u)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int f,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(f), "r"(smem_u32(bar))
+      : "memory");
+}
+
 template <class R>
 __device__ inline R shfl_dn(R v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 template <class R>
@@ -200,9 +262,10 @@ __device__ inline R shfl_up(R v, int d) { return __shfl_up_sync(0xffffffffu, v, 
 
 // One tile of the flux sweep along DIR: tile index bx along the direction,
 // by across it, bz the third axis (interior index).  NC*32 threads.
-template <class R, int DIR, int NC, int UNR = 1>
+template <class R, int DIR, int NC, int UNR = 1, bool TMA = false>
 __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, int use_b, R tau, R inv_h, R h,
-                                         int first, int bx, int by, int bz, DirSmem<R, DIR, NC>& sm) {
+                                         int first, int bx, int by, int bz, DirSmem<R, DIR, NC>& sm,
+                                         const CUtensorMap* map5 = nullptr, const CUtensorMap* map9 = nullptr) {
   using S = DirSmem<R, DIR, NC>;
   constexpr int NA = S::NA, TL = S::TL, LD = S::LD;
   static_assert(NA == 32, "one warp per line");
@@ -212,14 +275,17 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   else if (DIR == 1) { lo = C.jl; hi = C.jr; galong = C.gy; }
   else { lo = C.kl; hi = C.kr; galong = C.gz; }
   const int a0 = lo - NG + bx * TL;  // global along index of local 0
-  const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)C.gx : (long long)C.gx * C.gy);
+  const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)C.px : (long long)C.px * C.gy);
 
-  // cross coordinates of line c
+  // cross coordinates of line c.  Across x (the y and eta sweeps) the
+  // tiles start at multiples of NC cells from the row start, so that a
+  // tile's x segment sits on whole 32-byte sectors of the padded rows; the
+  // lines in the ghost cells are idle.
   auto cross_base = [&](int c, bool& ok) -> long long {
     int i, j, k;
     if (DIR == 0) { i = 0; j = C.jl + by * NC + c; k = C.kl + bz; ok = j < C.jr; }
-    else if (DIR == 1) { i = C.il + by * NC + c; j = 0; k = C.kl + bz; ok = i < C.ir; }
-    else { i = C.il + by * NC + c; j = C.jl + bz; k = 0; ok = i < C.ir; }
+    else if (DIR == 1) { i = by * NC + c; j = 0; k = C.kl + bz; ok = i >= C.il && i < C.ir; }
+    else { i = by * NC + c; j = C.jl + bz; k = 0; ok = i >= C.il && i < C.ir; }
     return cix(C, i, j, k);
   };
 
@@ -232,16 +298,67 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
     const int g = a0 + ta;
     const int s = tc * LD + ta;
     R F[9], V[9], spd = 0, uu[4] = {0, 0, 0, 0};
-    if (ok && g >= 0 && g < galong) {
+    const bool live = ok && g >= 0 && g < galong;
+    R e = 0, p[5], T[4];
+    if constexpr (TMA) {
+      // the tile arrives by two box copies into the front of the shared
+      // buffer (the flux arrays overwrite it after the barrier below)
+      using B = TmaBox<R, DIR, NC>;
+      static_assert(B::SPAN <= sizeof(DirSmem<R, DIR, NC>), "staging fits");
+      __shared__ __align__(8) unsigned long long bar;
+      R* raw = reinterpret_cast<R*>(&sm);
+      const int xc = DIR == 0 ? a0 : by * NC;  // first x of the tile
+      const int x0 = xc / B::XA * B::XA;               // rounded down to 16 bytes
+      const int y0 = DIR == 0 ? C.jl + by * NC : (DIR == 1 ? a0 : C.jl + bz);
+      const int z0 = DIR == 2 ? a0 : C.kl + bz;
+      // a box lands only on a 128-byte boundary of shared memory (the same
+      // address in every thread: the block leaves as a whole)
+      if (smem_u32(raw) & 127u) {
+        if (tid == 0) atomicOr(P.status, ST_TMA);
+        return;
+      }
+      if (tid == 0) mbar_init(&bar, 1);
+      __syncthreads();
+      if (tid == 0) {
+        mbar_expect_tx(&bar, B::BYTES5 + B::BYTES9);
+        tma_load_4d(raw, map5, x0, y0, z0, 0, &bar);
+        tma_load_4d(raw + B::OFF9, map9, x0, y0, z0, use_b ? 18 : 5, &bar);
+      }
+      // every thread waits for the copies (bounded); the block leaves as a
+      // whole if any of them gave up, after a second bounded wait for the
+      // copies still in flight, with the step flagged
+      const bool got = mbar_wait0(&bar, 1 << 22);
+      if (!__syncthreads_and(got)) {
+        if (tid == 0) atomicOr(P.status, ST_TMA);
+        mbar_wait0(&bar, 1 << 22);
+        return;
+      }
+      const int xl = DIR == 0 ? ta + (xc - x0) : tc + (xc - x0);
+      const int yl = DIR == 1 ? ta : (DIR == 0 ? tc : 0);
+      const int zl = DIR == 2 ? ta : 0;
+      const int o = (zl * B::BY + yl) * B::BX + xl;
+      if (live) {
+        e = raw[o];
+#pragma unroll
+        for (int l = 0; l < 4; l++) uu[l] = raw[(1 + l) * B::CELLS + o];
+        const R* c9 = raw + B::OFF9 + o;
+#pragma unroll
+        for (int l = 0; l < 4; l++) T[l] = c9[(use_b ? l : 5 + l) * B::CELLS];
+#pragma unroll
+        for (int l = 0; l < 5; l++) p[l] = c9[(use_b ? 4 + l : l) * B::CELLS];
+      }
+      __syncthreads();  // every thread has its cell before the buffer is reused
+    } else if (live) {
       const long long c = cb + (long long)g * stride;
-      R p[5], T[4];
-      const R e = P.e()[c];
+      e = P.e()[c];
 #pragma unroll
       for (int l = 0; l < 4; l++) uu[l] = P.u(l)[c];
 #pragma unroll
       for (int l = 0; l < 4; l++) T[l] = P.S(use_b, l)[c];
 #pragma unroll
       for (int l = 0; l < 5; l++) p[l] = P.S(use_b, 4 + l)[c];
+    }
+    if (live) {
       cell_terms<R, DIR>(C, tau, e, uu, p, T, g >= lo && g < hi, F, V, spd);
     } else {
 #pragma unroll
@@ -256,116 +373,186 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   __syncthreads();
 
   // ---- one warp per line: lane a reconstructs both face states of its
-  // stencil; the face right of lane a takes R from lane a + 1
+  // stencil; the face right of lane a takes R from lane a + 1.
+  // Along x the lanes of a warp are consecutive cells and write the
+  // divergence and the velocity derivative straight to the state arrays.
+  // Across x (TR) a warp's cells are a row apart; each warp leaves its
+  // results in its own line of shared memory (the slots its stencil has
+  // finished reading) and the block writes them row by row at the end.
+#ifndef VH_DEFER_X
+#define VH_DEFER_X 0
+#endif
+  constexpr bool TR = DIR != 0 || VH_DEFER_X;
   const int a = tid & 31, c = tid >> 5;
   bool ok;
   const long long cb = cross_base(c, ok);
-  if (!ok) return;  // whole warp: c is uniform in the warp (no barrier follows)
+  if (!TR && !ok) return;  // whole warp: c is uniform in the warp (no barrier follows)
   const int g = a0 + a;
   const int s = c * LD + a;
   const bool stencil = a >= 2 && a <= NA - 3;  // a-2..a+2 inside the tile
-  // face right of lane a exists for lanes 2..NA-4; it is a needed face when
-  // the cell right of it is in [lo, hi]
-  R amax = 0;
-  {
-    R L = 0, Rr = 0;
-    if (stencil) recon_lr<R>(C, sm.spd, s, L, Rr);
-    const R Rn = shfl_dn<R>(Rr, 1);
-    // the face left of the first interior cell takes no dissipation: its
-    // max speed sits in a ghost cell the reference never fills
-    // (NEWEST5/hydroKT.h:265-314 vs 435-440)
-    amax = (g + 1 == lo) ? (R)0 : fmax(fabs(L), fabs(Rn));
-  }
   const bool out = a >= 3 && a < 3 + TL && g < hi;  // interior cell of this tile
   const long long cell = cb + (long long)g * stride;
-  // the divergence accumulated by the previous sweeps: loaded before the
-  // flux loop so that the loads overlap the reconstruction
-  R racc[9];
+  if (ok) {
+    // face right of lane a exists for lanes 2..NA-4; it is a needed face
+    // when the cell right of it is in [lo, hi]
+    R amax = 0;
+    {
+      R L = 0, Rr = 0;
+      if (stencil) recon_lr<R>(C, sm.spd, s, L, Rr);
+      const R Rn = shfl_dn<R>(Rr, 1);
+      // the face left of the first interior cell takes no dissipation: its
+      // max speed sits in a ghost cell the reference never fills
+      // (NEWEST5/hydroKT.h:265-314 vs 435-440)
+      amax = (g + 1 == lo) ? (R)0 : fmax(fabs(L), fabs(Rn));
+    }
+    // the divergence accumulated by the previous sweeps: loaded before the
+    // flux loop so that the loads overlap the reconstruction
+    R racc[9];
 #pragma unroll
-  for (int l = 0; l < 9; l++) racc[l] = (!first && out) ? P.res(l)[cell] : (R)0;
+    for (int l = 0; l < 9; l++) racc[l] = (!TR && !first && out) ? P.res(l)[cell] : (R)0;
 #pragma unroll UNR
-  for (int l = 0; l < 9; l++) {
-    R fl = 0, fr = 0, vl = 0, vr = 0;
-    if (stencil) {
-      if constexpr (sizeof(R) == 4) {
-        if (C.recon == 0) {
-          // F^l and V^l of the stencil reconstructed as one pair
-          const float(*q)[2] = reinterpret_cast<const float(*)[2]>(sm.fv[l]);
-          F2 L2, R2, x0, x1, x2, x3, x4;
-          x0.v = ld_pair(q, s - 2); x1.v = ld_pair(q, s - 1); x2.v = ld_pair(q, s);
-          x3.v = ld_pair(q, s + 1); x4.v = ld_pair(q, s + 2);
-          weno_lr2(x0, x1, x2, x3, x4, L2, R2);
-          float a, b;
-          f2u(L2, a, b);
-          fl = a; vl = b;
-          f2u(R2, a, b);
-          fr = a; vr = b;
+    for (int l = 0; l < 9; l++) {
+      R fl = 0, fr = 0, vl = 0, vr = 0;
+      if (stencil) {
+        if constexpr (sizeof(R) == 4) {
+          if (C.recon == 0) {
+            // F^l and V^l of the stencil reconstructed as one pair
+            const float(*q)[2] = reinterpret_cast<const float(*)[2]>(sm.fv[l]);
+            F2 L2, R2, x0, x1, x2, x3, x4;
+            x0.v = ld_pair(q, s - 2); x1.v = ld_pair(q, s - 1); x2.v = ld_pair(q, s);
+            x3.v = ld_pair(q, s + 1); x4.v = ld_pair(q, s + 2);
+            weno_lr2(x0, x1, x2, x3, x4, L2, R2);
+            float a, b;
+            f2u(L2, a, b);
+            fl = a; vl = b;
+            f2u(R2, a, b);
+            fr = a; vr = b;
+          } else {
+            recon_lr<R, 2>(C, &sm.fv[l][0][0], s, fl, fr);
+            recon_lr<R, 2>(C, &sm.fv[l][0][1], s, vl, vr);
+          }
+        } else if (C.recon == 0) {
+          // F^l and V^l with one reciprocal between them
+          const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.fv[l]);
+          double a_[5], b_[5];
+#pragma unroll
+          for (int k = 0; k < 5; k++) {
+            const double2 v = ld_pair(q, s - 2 + k);
+            a_[k] = v.x;
+            b_[k] = v.y;
+          }
+          double flx, frx, vlx, vrx;
+          weno_lr_pair(a_, b_, flx, frx, vlx, vrx);
+          fl = flx; fr = frx; vl = vlx; vr = vrx;
         } else {
           recon_lr<R, 2>(C, &sm.fv[l][0][0], s, fl, fr);
           recon_lr<R, 2>(C, &sm.fv[l][0][1], s, vl, vr);
         }
-      } else if (C.recon == 0) {
-        // F^l and V^l with one reciprocal between them
-        const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.fv[l]);
-        double a_[5], b_[5];
-#pragma unroll
-        for (int k = 0; k < 5; k++) {
-          const double2 v = ld_pair(q, s - 2 + k);
-          a_[k] = v.x;
-          b_[k] = v.y;
-        }
-        double flx, frx, vlx, vrx;
-        weno_lr_pair(a_, b_, flx, frx, vlx, vrx);
-        fl = flx; fr = frx; vl = vlx; vr = vrx;
-      } else {
-        recon_lr<R, 2>(C, &sm.fv[l][0][0], s, fl, fr);
-        recon_lr<R, 2>(C, &sm.fv[l][0][1], s, vl, vr);
+      }
+      fr = shfl_dn<R>(fr, 1);
+      vr = shfl_dn<R>(vr, 1);
+      const R H = (R)0.5 * (fl + fr) - (R)0.5 * amax * (vr - vl);  // flux at the right face
+      const R Hl = shfl_up<R>(H, 1);                                // flux at the left face
+      const R r = -inv_h * (H - Hl);
+      if constexpr (TR) {
+        __syncwarp();  // the line's stencil reads of field l are done
+        if (out) sm.fv[l][s][0] = r;
+      } else if (out) {
+        P.res(l)[cell] = first ? r : racc[l] + r;
       }
     }
-    fr = shfl_dn<R>(fr, 1);
-    vr = shfl_dn<R>(vr, 1);
-    const R H = (R)0.5 * (fl + fr) - (R)0.5 * amax * (vr - vl);  // flux at the right face
-    const R Hl = shfl_up<R>(H, 1);                                // flux at the left face
+    // velocity derivative along DIR: (L - R)/h of the same stencil (genWENOder)
+    R dv[4] = {0, 0, 0, 0};
     if (out) {
-      const R r = -inv_h * (H - Hl);
-      P.res(l)[cell] = first ? r : racc[l] + r;
+#pragma unroll
+      for (int l = 0; l < 4; l += 2) {
+        R La, Ra, Lb, Rb;
+        if constexpr (sizeof(R) == 4) {
+          const float(*q)[2] = reinterpret_cast<const float(*)[2]>(sm.up[l >> 1]);
+          F2 L2, R2, x0, x1, x2, x3, x4;
+          x0.v = ld_pair(q, s - 2); x1.v = ld_pair(q, s - 1); x2.v = ld_pair(q, s);
+          x3.v = ld_pair(q, s + 1); x4.v = ld_pair(q, s + 2);
+          weno_lr2(x0, x1, x2, x3, x4, L2, R2);
+          f2u(L2, La, Lb);
+          f2u(R2, Ra, Rb);
+        } else {
+          const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.up[l >> 1]);
+          double a_[5], b_[5];
+#pragma unroll
+          for (int k = 0; k < 5; k++) {
+            const double2 v = ld_pair(q, s - 2 + k);
+            a_[k] = v.x;
+            b_[k] = v.y;
+          }
+          weno_lr_pair(a_, b_, La, Ra, Lb, Rb);
+        }
+        dv[l] = (La - Ra) * inv_h;
+        dv[l + 1] = (Lb - Rb) * inv_h;
+      }
+    }
+    if constexpr (TR) {
+      __syncwarp();  // the line's velocity stencils are read
+      if (out) {
+#pragma unroll
+        for (int l = 0; l < 4; l++) sm.up[l >> 1][s][l & 1] = dv[l];
+      }
+    } else if (out) {
+#pragma unroll
+      for (int l = 0; l < 4; l++) P.du(l * 3 + DIR)[cell] = dv[l];
     }
   }
-  // velocity derivative along DIR: (L - R)/h of the same stencil (genWENOder)
-  if (out) {
+  if constexpr (TR) {
+    __syncthreads();
+    // row by row: x fastest (along the line for x, over the tile's NC lines
+    // across x)
+    for (int t = tid; t < NC * TL; t += NC * NA) {
+      const int cc = DIR == 0 ? t / TL : t % NC, aa = 3 + (DIR == 0 ? t % TL : t / NC);
+      bool ok2;
+      const long long cb2 = cross_base(cc, ok2);
+      const int g2 = a0 + aa;
+      if (!ok2 || g2 >= hi) continue;
+      const long long cell2 = cb2 + (long long)g2 * stride;
+      const int s2 = cc * LD + aa;
 #pragma unroll
-    for (int l = 0; l < 4; l += 2) {
-      R La, Ra, Lb, Rb;
-      if constexpr (sizeof(R) == 4) {
-        const float(*q)[2] = reinterpret_cast<const float(*)[2]>(sm.up[l >> 1]);
-        F2 L2, R2, x0, x1, x2, x3, x4;
-        x0.v = ld_pair(q, s - 2); x1.v = ld_pair(q, s - 1); x2.v = ld_pair(q, s);
-        x3.v = ld_pair(q, s + 1); x4.v = ld_pair(q, s + 2);
-        weno_lr2(x0, x1, x2, x3, x4, L2, R2);
-        f2u(L2, La, Lb);
-        f2u(R2, Ra, Rb);
-      } else {
-        const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.up[l >> 1]);
-        double a_[5], b_[5];
-#pragma unroll
-        for (int k = 0; k < 5; k++) {
-          const double2 v = ld_pair(q, s - 2 + k);
-          a_[k] = v.x;
-          b_[k] = v.y;
-        }
-        weno_lr_pair(a_, b_, La, Ra, Lb, Rb);
+      for (int l = 0; l < 9; l++) {
+        const R r = sm.fv[l][s2][0];
+        P.res(l)[cell2] = first ? r : P.res(l)[cell2] + r;
       }
-      P.du(l * 3 + DIR)[cell] = (La - Ra) * inv_h;
-      P.du((l + 1) * 3 + DIR)[cell] = (Lb - Rb) * inv_h;
+#pragma unroll
+      for (int l = 0; l < 4; l++) P.du(l * 3 + DIR)[cell2] = sm.up[l >> 1][s2][l & 1];
     }
   }
 }
 
+// Blocks per SM the sweeps are compiled for.  FP64: 4 blocks of 256
+// threads (y, eta) and 7 of 128 (x) hold the registers to 64 and 72 a
+// thread, a few bytes of spill in the y and eta sweeps against a fourth
+// resident block (measured: the FP64 step 2 % faster than at 3 blocks and
+// 80 registers).  FP32: the counts the registers the sweeps need allow
+// anyway (48 a thread; 40 for the y and eta sweeps staged by TMA).
+template <class R, int DIR, bool TMA>
+struct DirOcc {
+  static constexpr int MIN_BLOCKS = sizeof(R) == 8 ? (DIR == 0 ? 7 : 4) : (DIR == 0 ? 10 : (TMA ? 6 : 5));
+};
+
+// the sweep with its tile staged by TMA (the handle's padded state)
 template <class R, int DIR>
-__global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC)
+__global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC, DirOcc<R, DIR, true>::MIN_BLOCKS)
+    k_dir_tma(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, R h, int first,
+              const __grid_constant__ CUtensorMap map5, const __grid_constant__ CUtensorMap map9) {
+  using S = DirSmem<R, DIR>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  pdl_wait_then_release();
+  if (*P.status) return;
+  dir_tile<R, DIR, S::NC, 1, true>(C, P, use_b, tau, inv_h, h, first, blockIdx.x, blockIdx.y, blockIdx.z,
+                                   *reinterpret_cast<S*>(smem_raw), &map5, &map9);
+}
+
+template <class R, int DIR>
+__global__ void __launch_bounds__(Tile<DIR, R>::NA* Tile<DIR, R>::NC, DirOcc<R, DIR, false>::MIN_BLOCKS)
     k_dir(DevCfg C, DevPtrs<R> P, int use_b, R tau, R inv_h, R h, int first) {
   using S = DirSmem<R, DIR>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   pdl_wait_then_release();
   if (*P.status) return;
   dir_tile<R, DIR, S::NC>(C, P, use_b, tau, inv_h, h, first, blockIdx.x, blockIdx.y, blockIdx.z,

@@ -170,6 +170,12 @@ class Hydro:
         self._chk(A.lib().vh_last_iterations(self.h, ctypes.byref(v)))
         return v.value
 
+    def sweep_uses_tma(self) -> bool:
+        """True when the flux sweeps stage their tiles by TMA box copies"""
+        v = ctypes.c_int()
+        self._chk(A.lib().vh_sweep_uses_tma(self.h, ctypes.byref(v)))
+        return bool(v.value)
+
     # ---- diagnostics
     def max_temperature(self) -> float:
         t = ctypes.c_double()
