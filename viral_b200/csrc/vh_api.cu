@@ -62,6 +62,7 @@ extern "C" int vh_create(const vh_config* cfg, vh_handle** out) {
   // of 16 bytes as the tensor maps require.  The padding cells are never
   // read; the C ABI's arrays keep the canonical unpadded layout.
   C.px = (C.gx + 7) / 8 * 8;
+  C.xt0 = 0;
   C.il = NG; C.ir = NG + cfg->nx; C.jl = NG; C.jr = NG + cfg->ny;
   C.kl = cfg->boost_invariant ? 0 : NG; C.kr = cfg->boost_invariant ? 1 : NG + cfg->nz;
   C.n = (long long)C.px * C.gy * C.gz;

@@ -66,6 +66,7 @@ __device__ inline DevCfg event_cfg(const DevCfg& C0, int nx, int ny) {
   C.nx = nx; C.ny = ny; C.nz = 1;
   C.gx = nx + 2 * NG; C.gy = ny + 2 * NG; C.gz = 1;
   C.px = C.gx;  // the pool keeps unpadded rows
+  C.xt0 = NG;
   C.il = NG; C.ir = NG + nx; C.jl = NG; C.jr = NG + ny; C.kl = 0; C.kr = 1;
   C.n = (long long)C.gx * C.gy;
   return C;
@@ -285,7 +286,7 @@ static int build_items(vh_batch* b) {
     for (int e = 0; e < b->n; e++) {
       for (int by = 0; by < (b->ny[e] + nc - 1) / nc; by++)
         for (int bx = 0; bx < (b->nx[e] + tl - 1) / tl; bx++) xs.push_back(make_int4(e, bx, by, 0));
-      for (int bx = 0; bx < (b->nx[e] + NG + nc - 1) / nc; bx++)  // tiles from the row start
+      for (int bx = 0; bx < (b->nx[e] + nc - 1) / nc; bx++)
         for (int by = 0; by < (b->ny[e] + tl - 1) / tl; by++) ys.push_back(make_int4(e, by, bx, 0));
     }
     b->n_xi[q] = (int)xs.size();
@@ -428,7 +429,7 @@ static int import_event(vh_batch* b, int ev, const double* host18, int pi_mode) 
   P.status = b->d_flag + ev;
   k_import_event<R><<<(unsigned)((n + 255) / 256), 256>>>(b->stage, P, n);
   DevCfg C = b->C0;
-  C.nx = b->nx[ev]; C.ny = b->ny[ev]; C.gx = C.nx + 6; C.gy = C.ny + 6; C.px = C.gx; C.ir = 3 + C.nx; C.jr = 3 + C.ny;
+  C.nx = b->nx[ev]; C.ny = b->ny[ev]; C.gx = C.nx + 6; C.gy = C.ny + 6; C.px = C.gx; C.xt0 = 3; C.ir = 3 + C.nx; C.jr = 3 + C.ny;
   C.il = C.jl = 3; C.n = n;
   if (pi_mode == VH_PI_NS) {
     R* du16 = reinterpret_cast<R*>(b->stage);  // staging is free again after the import

@@ -17,7 +17,8 @@ constexpr int NG = 3;  // ghost layers (NEWEST5/maindef.h:369-371 BORDER)
 // Problem description passed by value to every kernel.
 struct DevCfg {
   int gx, gy, gz;              // ghost-inclusive extents
-  int px;                      // row pitch in cells (>= gx): a handle's rows are padded to 16 bytes
+  int px;                      // row pitch in cells (>= gx): a handle's rows are padded to 8 cells
+  int xt0;                     // x of the first line of the y and eta sweeps' tiles (0 or il)
   int il, ir, jl, jr, kl, kr;  // interior bounds
   int nx, ny, nz;
   long long n;                 // px*gy*gz: cells per array, padding included

@@ -131,7 +131,7 @@ static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, dou
   } else if (dir == 1) {
     using T = Tile<1, R>;
     block = dim3(T::NA * T::NC);
-    grid = dim3((C.ny + T::NA - 7) / (T::NA - 6), (C.ir + T::NC - 1) / T::NC, nzi);
+    grid = dim3((C.ny + T::NA - 7) / (T::NA - 6), (C.ir - C.xt0 + T::NC - 1) / T::NC, nzi);
     sm = sizeof(DirSmem<R, 1>);
     if (h->tma)
       VH_CUDA(h, launch_step_kernel(h->pdl, k_dir_tma<R, 1>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h,
@@ -142,7 +142,7 @@ static int launch_dir(vh_handle* h, const DevPtrs<R>& P, int dir, int use_b, dou
   } else {
     using T = Tile<2, R>;
     block = dim3(T::NA * T::NC);
-    grid = dim3((C.nz + T::NA - 7) / (T::NA - 6), (C.ir + T::NC - 1) / T::NC, C.ny);
+    grid = dim3((C.nz + T::NA - 7) / (T::NA - 6), (C.ir - C.xt0 + T::NC - 1) / T::NC, C.ny);
     sm = sizeof(DirSmem<R, 2>);
     if (h->tma)
       VH_CUDA(h, launch_step_kernel(h->pdl, k_dir_tma<R, 2>, grid, block, sm, h->stream, C, P, use_b, (R)tau, inv_h,

@@ -278,18 +278,18 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)C.px : (long long)C.px * C.gy);
 
   // cross coordinates of line c.  Across x (the y and eta sweeps) the
-  // tiles start at multiples of NC cells from the row start, so that a
-  // tile's x segment sits on whole 32-byte sectors of the padded rows; the
-  // lines in the ghost cells are idle.
+  // tiles start at x = xt0 + by * NC: on a handle's padded rows xt0 = 0, so
+  // that a tile's x segment sits on whole 32-byte sectors (the lines in the
+  // ghost cells are idle); on unpadded rows xt0 = il.
   auto cross_base = [&](int c, bool& ok) -> long long {
     int i, j, k;
     if (DIR == 0) { i = 0; j = C.jl + by * NC + c; k = C.kl + bz; ok = j < C.jr; }
-    else if (DIR == 1) { i = by * NC + c; j = 0; k = C.kl + bz; ok = i >= C.il && i < C.ir; }
-    else { i = by * NC + c; j = C.jl + bz; k = 0; ok = i >= C.il && i < C.ir; }
+    else if (DIR == 1) { i = C.xt0 + by * NC + c; j = 0; k = C.kl + bz; ok = i >= C.il && i < C.ir; }
+    else { i = C.xt0 + by * NC + c; j = C.jl + bz; k = 0; ok = i >= C.il && i < C.ir; }
     return cix(C, i, j, k);
   };
 
-    // ---- load and per-cell terms (x-fastest thread order: coalesced)
+      // ---- load and per-cell terms (x-fastest thread order: coalesced)
   {
     const int ta = DIR == 0 ? tid % NA : tid / NC;
     const int tc = DIR == 0 ? tid / NA : tid % NC;
@@ -299,7 +299,7 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
     const int s = tc * LD + ta;
     R F[9], V[9], spd = 0, uu[4] = {0, 0, 0, 0};
     const bool live = ok && g >= 0 && g < galong;
-    R e = 0, p[5], T[4];
+    R e = 0, p[5], T[4];  // the TMA path's copy of the cell
     if constexpr (TMA) {
       // the tile arrives by two box copies into the front of the shared
       // buffer (the flux arrays overwrite it after the barrier below)
@@ -307,7 +307,7 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
       static_assert(B::SPAN <= sizeof(DirSmem<R, DIR, NC>), "staging fits");
       __shared__ __align__(8) unsigned long long bar;
       R* raw = reinterpret_cast<R*>(&sm);
-      const int xc = DIR == 0 ? a0 : by * NC;  // first x of the tile
+      const int xc = DIR == 0 ? a0 : C.xt0 + by * NC;  // first x of the tile
       const int x0 = xc / B::XA * B::XA;               // rounded down to 16 bytes
       const int y0 = DIR == 0 ? C.jl + by * NC : (DIR == 1 ? a0 : C.jl + bz);
       const int z0 = DIR == 2 ? a0 : C.kl + bz;
@@ -348,18 +348,23 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
         for (int l = 0; l < 5; l++) p[l] = c9[(use_b ? 4 + l : l) * B::CELLS];
       }
       __syncthreads();  // every thread has its cell before the buffer is reused
+      if (live) {
+        cell_terms<R, DIR>(C, tau, e, uu, p, T, g >= lo && g < hi, F, V, spd);
+      } else {
+#pragma unroll
+        for (int l = 0; l < 9; l++) { F[l] = 0; V[l] = 0; }
+      }
     } else if (live) {
       const long long c = cb + (long long)g * stride;
-      e = P.e()[c];
+      R p2[5], T2[4];
+      const R e2 = P.e()[c];
 #pragma unroll
       for (int l = 0; l < 4; l++) uu[l] = P.u(l)[c];
 #pragma unroll
-      for (int l = 0; l < 4; l++) T[l] = P.S(use_b, l)[c];
+      for (int l = 0; l < 4; l++) T2[l] = P.S(use_b, l)[c];
 #pragma unroll
-      for (int l = 0; l < 5; l++) p[l] = P.S(use_b, 4 + l)[c];
-    }
-    if (live) {
-      cell_terms<R, DIR>(C, tau, e, uu, p, T, g >= lo && g < hi, F, V, spd);
+      for (int l = 0; l < 5; l++) p2[l] = P.S(use_b, 4 + l)[c];
+      cell_terms<R, DIR>(C, tau, e2, uu, p2, T2, g >= lo && g < hi, F, V, spd);
     } else {
 #pragma unroll
       for (int l = 0; l < 9; l++) { F[l] = 0; V[l] = 0; }
@@ -379,10 +384,7 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
   // Across x (TR) a warp's cells are a row apart; each warp leaves its
   // results in its own line of shared memory (the slots its stencil has
   // finished reading) and the block writes them row by row at the end.
-#ifndef VH_DEFER_X
-#define VH_DEFER_X 0
-#endif
-  constexpr bool TR = DIR != 0 || VH_DEFER_X;
+  constexpr bool TR = DIR != 0;
   const int a = tid & 31, c = tid >> 5;
   bool ok;
   const long long cb = cross_base(c, ok);
@@ -513,11 +515,11 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
       if (!ok2 || g2 >= hi) continue;
       const long long cell2 = cb2 + (long long)g2 * stride;
       const int s2 = cc * LD + aa;
+      R acc[9];
 #pragma unroll
-      for (int l = 0; l < 9; l++) {
-        const R r = sm.fv[l][s2][0];
-        P.res(l)[cell2] = first ? r : P.res(l)[cell2] + r;
-      }
+      for (int l = 0; l < 9; l++) acc[l] = first ? (R)0 : P.res(l)[cell2];
+#pragma unroll
+      for (int l = 0; l < 9; l++) P.res(l)[cell2] = first ? sm.fv[l][s2][0] : acc[l] + sm.fv[l][s2][0];
 #pragma unroll
       for (int l = 0; l < 4; l++) P.du(l * 3 + DIR)[cell2] = sm.up[l >> 1][s2][l & 1];
     }

@@ -82,6 +82,7 @@ int fill_cfg(const vh_config* c, const double* eos_dev, double tau, DevCfg& C) {
   C.nx = c->nx; C.ny = c->ny; C.nz = c->boost_invariant ? 1 : c->nz;
   C.gx = c->nx + 2 * NG; C.gy = c->ny + 2 * NG; C.gz = c->boost_invariant ? 1 : c->nz + 2 * NG;
   C.px = C.gx;  // the caller's state is in the canonical, unpadded layout
+  C.xt0 = NG;
   C.il = NG; C.ir = NG + c->nx; C.jl = NG; C.jr = NG + c->ny;
   C.kl = c->boost_invariant ? 0 : NG; C.kr = c->boost_invariant ? 1 : NG + c->nz;
   C.n = (long long)C.gx * C.gy * C.gz;
@@ -121,11 +122,11 @@ int launch_dir_static(const DevCfg& C, const DevPtrs<double>& P, int dir, int us
     k_dir<double, 0><<<grid, dim3(T::NA * T::NC), sizeof(DirSmem<double, 0>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
   } else if (dir == 1) {
     using T = Tile<1, double>;
-    dim3 grid((C.ny + T::NA - 7) / (T::NA - 6), (C.ir + T::NC - 1) / T::NC, nzi);
+    dim3 grid((C.ny + T::NA - 7) / (T::NA - 6), (C.ir - C.xt0 + T::NC - 1) / T::NC, nzi);
     k_dir<double, 1><<<grid, dim3(T::NA * T::NC), sizeof(DirSmem<double, 1>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
   } else {
     using T = Tile<2, double>;
-    dim3 grid((C.nz + T::NA - 7) / (T::NA - 6), (C.ir + T::NC - 1) / T::NC, C.ny);
+    dim3 grid((C.nz + T::NA - 7) / (T::NA - 6), (C.ir - C.xt0 + T::NC - 1) / T::NC, C.ny);
     k_dir<double, 2><<<grid, dim3(T::NA * T::NC), sizeof(DirSmem<double, 2>), s>>>(C, P, use_b, tau, 1.0 / hh, hh, first);
   }
   return cudaGetLastError() == cudaSuccess ? VH_OK : VH_E_CUDA;
