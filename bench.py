@@ -228,6 +228,9 @@ def reference_procs() -> int:
 
 
 class ClockSampler:
+    """nvidia-smi samples (every 100 ms) around a timed region: entering waits
+    for the sampler's first line, leaving waits for one more, so that even a
+    region shorter than the interval is bracketed by samples taken under load."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
@@ -235,25 +238,48 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
+        self.lines = []
+        self.thread = None
+        self.first = 0
+        self.out = ""
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
+
+    def _wait_for(self, n: int, limit_s: float):
+        t0 = time.time()
+        while len(self.lines) < n and time.time() - t0 < limit_s and self.proc.poll() is None:
+            time.sleep(0.005)
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        self._wait_for(1, 5.0)
+        self.first = max(len(self.lines) - 1, 0)
         return self
 
     def __exit__(self, *a):
         self.out = ""
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out, _ = self.proc.communicate()
+        if not self.proc:
+            return
+        self._wait_for(len(self.lines) + 1, 1.0)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            self.proc.wait()
+        self.thread.join(timeout=5)
+        self.out = "".join(self.lines[self.first:])
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -346,66 +372,27 @@ def algorithmic_bytes(cfg, kernel: str) -> float:
 
 
 # DRAM bytes (read + write) per interior cell and launch, from one ncu capture
-# of the 121x121x31 case of the bench event (profiles/step_kernels_*.md and,
-# for the FP64 stage-1 update, profiles/update_kernel_*.md; the stage-2
-# figures predate the current update kernel), scaled to a full launch by the
-# cells processed
+# of the 121x121x31 case of the bench event (profiles/step_kernels_*.md for the
+# sweeps, profiles/update_kernel_*.md for the updates), scaled to a full launch
+# by the cells processed
 MEASURED_TRAFFIC_PER_CELL = {
-    ("fp64", "k_dir_x"): 150.0, ("fp64", "k_dir_y"): 239.0, ("fp64", "k_dir_eta"): 261.0,
-    ("fp64", "k_update_stage1"): 538.0, ("fp64", "k_update_stage2"): 651.0,
-    ("mixed", "k_dir_x"): 63.0, ("mixed", "k_dir_y"): 104.0, ("mixed", "k_dir_eta"): 114.0,
-    ("mixed", "k_update_stage1"): 200.0, ("mixed", "k_update_stage2"): 223.0,
+    ("fp64", "k_dir_x"): 153.0, ("fp64", "k_dir_y"): 230.0, ("fp64", "k_dir_eta"): 258.0,
+    ("fp64", "k_update_stage1"): 544.0, ("fp64", "k_update_stage2"): 561.0,
+    ("mixed", "k_dir_x"): 65.0, ("mixed", "k_dir_y"): 104.0, ("mixed", "k_dir_eta"): 114.0,
+    ("mixed", "k_update_stage1"): 192.0, ("mixed", "k_update_stage2"): 226.0,
 }
 
 
 # the bound that does hold for the step kernels: the share of peak of the
 # pipe or issue rate that limits each, from the same ncu captures
-# (profiles/step_kernels_*.md, profiles/update_kernel_*.md)
 MEASURED_COMPUTE_BOUND = {
-    ("fp64", "k_dir_x"): ("fp64 pipe", 0.719), ("fp64", "k_dir_y"): ("fp64 pipe", 0.646),
-    ("fp64", "k_dir_eta"): ("fp64 pipe", 0.682), ("fp64", "k_update_stage1"): ("fp64 pipe", 0.369),
-    ("fp64", "k_update_stage2"): ("fp64 pipe", 0.273),
-    ("mixed", "k_dir_x"): ("fma pipe", 0.677), ("mixed", "k_dir_y"): ("fma pipe", 0.584),
-    ("mixed", "k_dir_eta"): ("fma pipe", 0.632), ("mixed", "k_update_stage2"): ("issue", 0.498),
+    ("fp64", "k_dir_x"): ("fp64 pipe", 0.753), ("fp64", "k_dir_y"): ("fp64 pipe", 0.724),
+    ("fp64", "k_dir_eta"): ("fp64 pipe", 0.756), ("fp64", "k_update_stage1"): ("fp64 pipe", 0.314),
+    ("fp64", "k_update_stage2"): ("fp64 pipe", 0.315),
+    ("mixed", "k_dir_x"): ("fma pipe", 0.680), ("mixed", "k_dir_y"): ("fma pipe", 0.650),
+    ("mixed", "k_dir_eta"): ("fma pipe", 0.693), ("mixed", "k_update_stage1"): ("issue", 0.503),
+    ("mixed", "k_update_stage2"): ("issue", 0.507),
 }
-
-
-def measured_peaks():
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
-            d = json.load(fh)
-        return float(d["hbm_gbs"]), "measured"
-    except Exception:
-        return 6650.0, "fallback"
-
-
-def timed_steps(H, stream, k: int, dev: int):
-    """device ms of k steps of handle H on `stream` (CUDA events), with the
-    clocks sampled during them"""
-    import torch
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev) as clk:
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        H.step(k)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    return ev0.elapsed_time(ev1), clk.summary()
-
-
-KERNELS = ["k_dir_x", "k_dir_y", "k_dir_eta", "k_update_stage1", "k_update_stage2"]
-
-
-def kernel_times(H, cfg):
-    """per-launch device ms and share of each step kernel over 2 steps
-    (vh_time_kernels: events around every launch, outside the timed region)"""
-    kt = H.time_kernels(2)
-    launches = {"k_dir_x": 4, "k_dir_y": 4, "k_dir_eta": 0 if cfg.boost_invariant else 4, "k_update_stage1": 2,
-                "k_update_stage2": 2}
-    per_launch = {nm: (kt[q] / launches[nm] if launches[nm] else 0.0) for q, nm in enumerate(KERNELS)}
-    share = {nm: kt[q] / max(sum(kt), 1e-30) for q, nm in enumerate(KERNELS)}
-    top = max(KERNELS, key=lambda nm: kt[KERNELS.index(nm)])
-    return per_launch, share, top
 
 
 def roofline(cfg, precision: str, cells: int, per_launch: dict, share: dict, top: str) -> dict:
