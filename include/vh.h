@@ -359,11 +359,13 @@ const char* vh_batch_last_error(const vh_batch* b);
 
 /* Momentum anisotropy of the current state, summed in FP64 over the interior
  * cells: eps_p = sum(T^xx - T^yy) / sum(T^xx + T^yy), with
- * T^ij = (e + P) u^i u^j + P delta^ij + pi^ij.  Boost-invariant grids. */
+ * T^ij = (e + P) u^i u^j + P delta^ij + pi^ij.  Milne grids, summed over
+ * every interior cell (every eta slice of a 3+1D grid). */
 int vh_eps_p(vh_handle* h, double* eps_p);
 
 /* Discrete adjoint of eps_p after nsteps steps from the current state
- * (boost-invariant Milne grids, WENO reconstruction, copy boundaries).  Runs
+ * (Milne grids, boost-invariant or 3+1D, WENO reconstruction, copy
+ * boundaries; VH_E_UNSUPPORTED otherwise).  Runs
  * the forward in segments of checkpoint_every steps (the first segment takes
  * the remainder), checkpointing the state at each segment start, then the
  * reverse of every step, re-running each segment from its checkpoint (the

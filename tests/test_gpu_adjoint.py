@@ -232,10 +232,22 @@ def test_autograd_function_wraps_the_adjoint():
 
 
 def test_unsupported_configurations_are_refused():
-    cfg = C.glauber_config(nx=16, ny=16, nz=8, boost_invariant=False)
-    with Hydro(cfg) as h:
-        inp = C.glauber_inputs(cfg)
-        h.init_profile(inp["tau"], inp["e"], inp["ux"], inp["uy"], inp["ueta"], None, inp["pi_mode"])
+    """minmod reconstruction and Cartesian coordinates have no adjoint (3+1D
+    Milne grids do: tests/test_gpu_adjoint3.py)"""
+    for cfg in (C.glauber_config(nx=16, ny=16, nz=8, boost_invariant=False, recon=A.RECON_MINMOD),
+                C.glauber_config(nx=16, ny=16, boost_invariant=True, recon=A.RECON_MINMOD)):
+        with Hydro(cfg) as h:
+            inp = C.glauber_inputs(cfg)
+            h.init_profile(inp["tau"], inp["e"], inp["ux"], inp["uy"], inp["ueta"], None, inp["pi_mode"])
+            with pytest.raises(A.VhError) as ex:
+                h.adjoint_eps_p(2, 1)
+            assert ex.value.code == A.E_UNSUPPORTED
+    cart = C.cart_bjorken_config()
+    with Hydro(cart) as h:
+        n = h.n
+        s = np.zeros((A.NFIELDS, n))
+        s[0] = 1.0; s[1] = 1.0; s[14] = 1.0
+        h.set_state(s, cart.tau0)
         with pytest.raises(A.VhError) as ex:
             h.adjoint_eps_p(2, 1)
         assert ex.value.code == A.E_UNSUPPORTED

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvh.so")
 CHECK_LIB = os.path.join(HERE, "libvh_check.so")
 
-SOURCES = ["vh_api.cu", "vh_static.cu", "vh_batch.cu", "vh_adjoint.cu", "vh_cgc.cu", "vh_inputs.cpp", "vh_io.cpp",
+SOURCES = ["vh_api.cu", "vh_static.cu", "vh_batch.cu", "vh_adjoint.cu", "vh_adjoint3.cu", "vh_cgc.cu", "vh_inputs.cpp", "vh_io.cpp",
            "vh_freezeout.cpp", "vh_freezeout_dev.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

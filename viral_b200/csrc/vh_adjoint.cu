@@ -28,6 +28,7 @@
 #include "vh.h"
 #include "vh_adjoint.cuh"
 #include "vh_handle.cuh"
+#include "vh_adjoint_run.cuh"
 #include "vh_nvtx.h"
 
 namespace {
@@ -445,45 +446,6 @@ __global__ void __launch_bounds__(DirShape<R>::threads, 2) k_adj_dir(DirArgs<R> 
   }
 }
 
-// momentum anisotropy: per-block partial sums of T^xx - T^yy and T^xx + T^yy
-// over the interior cells, then one fixed-order sum (deterministic)
-constexpr int kObsBlocks = 148;
-template <class R>
-__global__ void __launch_bounds__(256) k_obs_part(DevCfg C, const R* S, long long n, double* part) {
-  double a = 0, b = 0;
-  const long long nint = (long long)C.nx * C.ny;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int i = C.il + (int)(t % C.nx), j = C.jl + (int)(t / C.nx);
-    const long long c = cix(C, i, j, 0);
-    double num, den;
-    obs_cell<R>(C, S[c], S[2 * n + c], S[3 * n + c], S[5 * n + c], S[6 * n + c], num, den);
-    a += num;
-    b += den;
-  }
-  __shared__ double sa[8], sb[8];
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    b += __shfl_down_sync(0xffffffffu, b, o);
-  }
-  if ((threadIdx.x & 31) == 0) { sa[threadIdx.x >> 5] = a; sb[threadIdx.x >> 5] = b; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double ta = 0, tb = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { ta += sa[w]; tb += sb[w]; }
-    part[2 * blockIdx.x] = ta;
-    part[2 * blockIdx.x + 1] = tb;
-  }
-}
-__global__ void k_obs_final(const double* part, int nb, double* out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double a = 0, b = 0;
-    for (int k = 0; k < nb; k++) { a += part[2 * k]; b += part[2 * k + 1]; }
-    out[0] = a;
-    out[1] = b;
-  }
-}
-
 // adjoint seed: d eps_p / d (e, u^x, u^y, pi^xx, pi^yy) of the final state
 template <class R>
 __global__ void k_obs_seed(DevCfg C, const R* S, long long n, const double* nd, R* xo) {
@@ -528,93 +490,10 @@ __global__ void k_adj_final(DevCfg C, const R* X0, long long n, const R* xo, con
   }
 }
 
-__global__ void k_sum_cells(const double* cacc, long long n, double* out2) {
-  __shared__ double s0[256], s1[256];
-  double a = 0, b = 0;
-  for (long long c = threadIdx.x; c < n; c += blockDim.x) { a += cacc[c]; b += cacc[n + c]; }
-  s0[threadIdx.x] = a;
-  s1[threadIdx.x] = b;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double ta = 0, tb = 0;
-    for (int k = 0; k < (int)blockDim.x; k++) { ta += s0[k]; tb += s1[k]; }
-    out2[0] = ta;
-    out2[1] = tb;
-  }
-}
-
 template <class R>
 size_t dir_smem(const DevCfg& C) {
   return (size_t)kDirWords * std::max(C.gx, C.gy) * sizeof(R);
 }
-
-// Carves the adjoint's device buffers out of one allocation kept in the
-// handle (grown when a call needs more), so repeated calls allocate nothing.
-struct Carve {
-  char* base = nullptr;
-  size_t off = 0;
-  template <class T>
-  T* take(size_t count) {
-    T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
-    off += (count * sizeof(T) + 255) / 256 * 256;
-    return p;
-  }
-};
-
-template <class R>
-int eps_p_device(vh_handle* h, const R* S, double* part, double* nd_dev, double* nd_host) {
-  const DevCfg& C = h->C;
-  k_obs_part<R><<<kObsBlocks, 256, 0, h->stream>>>(C, S, C.n, part);
-  k_obs_final<<<1, 32, 0, h->stream>>>(part, kObsBlocks, nd_dev);
-  VH_CUDA(h, cudaGetLastError());
-  if (nd_host) {
-    VH_CUDA(h, cudaMemcpyAsync(nd_host, nd_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    VH_CUDA(h, cudaStreamSynchronize(h->stream));
-  }
-  return VH_OK;
-}
-
-// One forward step that also records X_n (the state at the step start) and
-// Y_n (e, u and the conserved set after stage 1); the launches are those of
-// step_once.
-template <class R>
-int record_step(vh_handle* h, const DevPtrs<R>& P, R* xrec, R* yrec) {
-  const DevCfg& C = h->C;
-  const size_t nb = (size_t)C.n * sizeof(R);
-  const double tau = h->tau, ts = h->cfg.dtau;
-  cudaStream_t st = h->stream;
-  int r;
-  VH_CUDA(h, cudaMemcpyAsync(xrec, P.base0, 18 * nb, cudaMemcpyDeviceToDevice, st));
-  if ((r = stage_rhs<R>(h, P, 0, tau))) return r;
-  if ((r = stage_update<R, 1>(h, P, tau, ts))) return r;
-  VH_CUDA(h, cudaMemcpyAsync(yrec, P.base0, 5 * nb, cudaMemcpyDeviceToDevice, st));
-  VH_CUDA(h, cudaMemcpyAsync(yrec + 5 * C.n, P.base1, 9 * nb, cudaMemcpyDeviceToDevice, st));
-  if ((r = stage_rhs<R>(h, P, 1, tau + ts))) return r;
-  if ((r = stage_update<R, 2>(h, P, tau, ts))) return r;
-  h->tau = tau + ts;
-  return VH_OK;
-}
-
-// events bracketing the phases of one call, read once at its end
-struct PhaseClock {
-  std::vector<cudaEvent_t> ev;
-  ~PhaseClock() {
-    for (cudaEvent_t e : ev) cudaEventDestroy(e);
-  }
-  cudaError_t mark(cudaStream_t s, int* idx) {
-    cudaEvent_t e;
-    cudaError_t r = cudaEventCreate(&e);
-    if (r != cudaSuccess) return r;
-    ev.push_back(e);
-    *idx = (int)ev.size() - 1;
-    return cudaEventRecord(e, s);
-  }
-  float ms(int a, int b) const {
-    float t = 0;
-    cudaEventElapsedTime(&t, ev[a], ev[b]);
-    return t;
-  }
-};
 
 template <class R>
 int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double* eps_p, double* grad_state,
@@ -770,7 +649,7 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
   // ---- gradients of the initial state and of (etas0, etas1)
   k_adj_final<R><<<grid1(n, 256), 256, 0, st>>>(C, ck, n, xo, xd, grad_state ? gs_dev : nullptr,
                                                   grad_e ? ge_dev : nullptr);
-  k_sum_cells<<<1, 256, 0, st>>>(cacc, n, sums);
+  sum_cells(cacc, n, part, sums, st);
   VH_CUDA(h, cudaGetLastError());
   double cs[2];
   unsigned astat = 0;
@@ -802,7 +681,7 @@ int adjoint_run(vh_handle* h, const DevPtrs<R>& P, int nsteps, int every, double
 extern "C" int vh_eps_p(vh_handle* h, double* eps_p) {
   if (!h || !eps_p) return VH_E_ARG;
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
-  if (!h->C.bi) return fail(h, VH_E_UNSUPPORTED, "vh_eps_p: boost-invariant grids only");
+  if (h->C.cart) return fail(h, VH_E_UNSUPPORTED, "vh_eps_p: Milne grids only");
   double* buf = nullptr;
   VH_CUDA(h, cudaMallocAsync(&buf, sizeof(double) * (2 * kObsBlocks + 2), h->stream));
   double nd[2];
@@ -826,9 +705,10 @@ extern "C" int vh_adjoint_eps_p(vh_handle* h, int nsteps, int checkpoint_every, 
   if (!h->have_state) return fail(h, VH_E_STATE, "no state set");
   VhNvtxRange range("discrete adjoint of eps_p");
   const DevCfg& C = h->C;
-  if (C.cart || !C.bi || C.mirror || C.recon != VH_RECON_WENO5 || C.cold)
+  if (C.cart || C.mirror || C.recon != VH_RECON_WENO5 || C.cold)
     return fail(h, VH_E_UNSUPPORTED,
-                "vh_adjoint_eps_p: boost-invariant Milne grids with WENO reconstruction and copy boundaries only");
+                "vh_adjoint_eps_p: Milne grids with WENO reconstruction and copy boundaries only");
+  if (!C.bi) return adjoint3_eps_p(h, nsteps, checkpoint_every, eps_p, grad_state, grad_e, grad_etas);
   const size_t smem = h->mixed ? dir_smem<float>(C) : dir_smem<double>(C);
   if (smem > 227 * 1024)
     return fail(h, VH_E_UNSUPPORTED, "vh_adjoint_eps_p: grid line too long for the line kernel");

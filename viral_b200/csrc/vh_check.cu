@@ -7,6 +7,7 @@
 
 #include "vh.h"
 #include "vh_adjoint.cuh"
+#include "vh_adjoint3.cuh"
 #include "vh_aux.cuh"
 #include "vh_freezeout.cuh"
 
@@ -94,6 +95,55 @@ void vhc_obs_cell(const vh_config* c, double e, double u1, double u2, double p1,
 void vhc_obs_cell_vjp(const vh_config* c, double e, double u1, double u2, double N, double D, double* g5) {
   HostCfg h = make_cfg(c);
   obs_cell_vjp<double>(h.C, e, u1, u2, N, D, g5[0], g5[1], g5[2], g5[3], g5[4]);
+}
+// 3+1D pieces: x[14] = (e, u^mu, pi 5, T^{tau mu}); du16[l*4 + m] = d_m u^l
+void vhc_pi_dep(const double* u4, const double* p5, double t2, double* d5) {
+  const PiDep<double> d = pi_dep<double>(u4[0], u4[1], u4[2], u4[3], p5, t2);
+  d5[0] = d.tt; d5[1] = d.tx; d5[2] = d.ty; d5[3] = d.te; d5[4] = d.ee;
+}
+void vhc_pi_dep_vjp(const double* u4, const double* p5, double t2, const double* db5, double* ub4, double* pb5) {
+  const PiDep<double> db{db5[0], db5[1], db5[2], db5[3], db5[4]};
+  pi_dep_vjp<double>(u4[0], u4[1], u4[2], u4[3], p5, t2, db, ub4, pb5);
+}
+void vhc_cell_q3(const vh_config* c, int dir, double tau, const double* x, int interior, double* q) {
+  HostCfg h = make_cfg(c);
+  if (dir == 0) cell_q3<double, 0>(h.C, tau, x, interior, q);
+  else if (dir == 1) cell_q3<double, 1>(h.C, tau, x, interior, q);
+  else cell_q3<double, 2>(h.C, tau, x, interior, q);
+}
+void vhc_cell_q3_vjp(const vh_config* c, int dir, double tau, const double* x, int interior, const double* qb,
+                     double* xb) {
+  HostCfg h = make_cfg(c);
+  if (dir == 0) cell_q3_vjp<double, 0>(h.C, tau, x, interior, qb, xb);
+  else if (dir == 1) cell_q3_vjp<double, 1>(h.C, tau, x, interior, qb, xb);
+  else cell_q3_vjp<double, 2>(h.C, tau, x, interior, qb, xb);
+}
+void vhc_src3(const vh_config* c, double tau, double e, const double* u4, const double* p5, const double* du16,
+              double* out9) {
+  HostCfg h = make_cfg(c);
+  double du[4][4];
+  for (int l = 0; l < 4; l++)
+    for (int m = 0; m < 4; m++) du[l][m] = du16[l * 4 + m];
+  src3<double>(h.C, tau, e, u4, p5, du, out9);
+}
+void vhc_src3_vjp(const vh_config* c, double tau, double e, const double* u4, const double* p5, const double* du16,
+                  const double* ob9, double* eb, double* ub4, double* pb5, double* dub16, double* cb2) {
+  HostCfg h = make_cfg(c);
+  double du[4][4], dub[4][4];
+  for (int l = 0; l < 4; l++)
+    for (int m = 0; m < 4; m++) { du[l][m] = du16[l * 4 + m]; dub[l][m] = dub16[l * 4 + m]; }
+  src3_vjp<double>(h.C, tau, e, u4, p5, du, ob9, *eb, ub4, pb5, dub, cb2);
+  for (int l = 0; l < 4; l++)
+    for (int m = 0; m < 4; m++) dub16[l * 4 + m] = dub[l][m];
+}
+int vhc_con2prim4(const vh_config* c, const double* T4, const double* p5, double tau, double* x4) {
+  HostCfg h = make_cfg(c);
+  return con2prim(h.C, T4, p5, tau, x4);
+}
+int vhc_c2p_ift_vjp4(const vh_config* c, const double* T4, const double* p5, double tau, const double* x4,
+                     const double* xb4, double* Tb4, double* pb5) {
+  HostCfg h = make_cfg(c);
+  return c2p_ift_vjp4(h.C, T4, p5, tau, x4, xb4, Tb4, pb5) ? 0 : 1;
 }
 int vhc_landau(const double* T10, double tau, int cart, double* e, double* u4) {
   return landau_cell(T10, tau, cart != 0, *e, u4) ? 1 : 0;
