@@ -835,6 +835,7 @@ def adjoint_record(args) -> dict:
                     "e0_unit_directions_rel_err": [abs(float(np.dot(ge, d)) - f) / abs(f) for d, f in zip(dirs, fd_dirs)],
                     "c0_c1_rel_err": [abs(gc[k] - fd_c[k]) / abs(fd_c[k]) for k in range(2)]}
     first = "fp64" if "fp64" in res else "mixed"
+    res["milne_3d"] = adjoint3_record(args, stream)
     return {"metric": "adjoint/forward time ratio", "value": res[first]["ratio"], "unit": "x",
             "higher_is_better": False, "dtype": "f64" if first == "fp64" else "f32 (FP64 implicit-function solve)",
             "mixed_ratio": res["mixed"]["ratio"] if "mixed" in res else None, "detail": res, "clocks": clk.summary(),
@@ -842,6 +843,93 @@ def adjoint_record(args) -> dict:
                        "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "tau_fm": [0.6, 0.6 + 0.02 * nsteps],
                        "eta_over_s": "0.08 + 1.0 max(T - 0.154, 0)", "checkpoint_every": args.checkpoint_every,
                        "observable": "eps_p"}}
+
+
+def adjoint3_record(args, stream) -> dict:
+    """The 3+1D adjoint on the benchmarked event's grid: 161x161x41 Milne
+    cells (dx = 0.1 fm, d eta = 0.25), MC-Glauber b = 7 fm, seed 0, floor 0.5
+    GeV/fm^3, eta/s = 0.08 + 1.0 GeV^-1 max(T - 0.154 GeV, 0); 20 steps from
+    0.6 fm/c, checkpoints every 10; FP64 and mixed.  The gradient along two
+    seeded unit directions of e0 and along (c0, c1) against central
+    differences of the FP64 forward (h = 1e-4 for e0: the directional
+    derivatives are small and rounding dominates at 1e-6; 1e-6 for c)."""
+    import numpy as np
+    import torch
+    from viral_b200 import _abi as A
+    from viral_b200 import configs as C
+    nsteps, every, reps = 20, 10, 3
+    out, grads = {}, {}
+    inp = None
+
+    def cfg_of(prec, c=(0.08, 1.0)):
+        return C.glauber_config(nx=161, ny=161, nz=41, boost_invariant=False, precision=prec, etas0=c[0], etas1=c[1])
+
+    for name, prec in (("fp64", A.PREC_FP64), ("mixed", A.PREC_MIXED)):
+        cfg = cfg_of(prec)
+        if inp is None:
+            inp = C.glauber_inputs(cfg, b=7.0, seed=0, efloor_gev=C.ADJOINT_FLOOR_GEV)
+        H = C.make_hydro(cfg, inp)
+        A.check(A.lib().vh_set_stream(H.h, ctypes_void_p(stream.cuda_stream)), H.h)
+
+        def reinit():
+            H.init_profile(inp["tau"], inp["e"], inp["ux"], inp["uy"], inp["ueta"], inp["prevu"], inp["pi_mode"])
+            torch.cuda.synchronize()
+
+        def timed(fn):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1), r
+
+        fwd, adj = [], []
+        for rep in range(2 + reps):
+            reinit()
+            tf, _ = timed(lambda: (H.step(nsteps), H.eps_p())[1])
+            reinit()
+            ta, r = timed(lambda: H.adjoint_eps_p(nsteps, every, want_state=False))
+            if rep >= 2:
+                fwd.append(tf)
+                adj.append(ta)
+        ph = H.adjoint_phase_times()
+        H.close()
+        out[name] = {"forward_ms": statistics.median(fwd), "adjoint_ms": statistics.median(adj),
+                     "ratio": statistics.median(adj) / statistics.median(fwd), "eps_p": r[0],
+                     "adjoint_phases_ms": {"forward_with_checkpoints": ph[0], "recompute_with_records": ph[1],
+                                           "reverse": ph[2], "rest": ph[3]}}
+        grads[name] = (r[2], r[3])
+    if args.adjoint_fd > 0:
+        def eps_of(e0, c):
+            with C.make_hydro(cfg_of(A.PREC_FP64, c), dict(inp, e=e0)) as H2:
+                H2.step(nsteps)
+                return H2.eps_p()
+        gx, gy, gz = 167, 167, 47
+        m = np.zeros((gz, gy, gx), bool)
+        m[3:44, 3:164, 3:164] = True
+        m = m.reshape(-1)
+        rng = np.random.default_rng(4321)
+        c = np.array([0.08, 1.0])
+        dirs, fd = [], []
+        for _ in range(2):
+            v = rng.normal(size=int(m.sum()))
+            d = np.zeros_like(inp["e"])
+            d[m] = v / np.linalg.norm(v)
+            dirs.append(d)
+            fd.append((eps_of(inp["e"] + 1e-4 * d, c) - eps_of(inp["e"] - 1e-4 * d, c)) / 2e-4)
+        fdc = []
+        for k in range(2):
+            cp = c.copy(); cm = c.copy()
+            cp[k] *= 1 + 1e-6; cm[k] *= 1 - 1e-6
+            fdc.append((eps_of(inp["e"], cp) - eps_of(inp["e"], cm)) / (2e-6 * c[k]))
+        for name, (ge, gc) in grads.items():
+            out[name]["fd_check"] = {
+                "e0_unit_directions_rel_err": [abs(float(np.dot(ge, d)) - f) / abs(f) for d, f in zip(dirs, fd)],
+                "c0_c1_rel_err": [abs(gc[k] - fdc[k]) / abs(fdc[k]) for k in range(2)]}
+    out["config"] = {"workload": "glauber_161x161x41 adjoint (3+1D Milne)", "grid": [161, 161, 41], "b_fm": 7.0,
+                     "seed": 0, "floor_gev_fm3": C.ADJOINT_FLOOR_GEV, "steps": nsteps, "checkpoint_every": every,
+                     "eta_over_s": "0.08 + 1.0 max(T - 0.154, 0)", "observable": "eps_p over every eta slice"}
+    return out
 
 
 def adjoint_ratio(args):
