@@ -395,6 +395,44 @@ MEASURED_COMPUTE_BOUND = {
 }
 
 
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def timed_steps(H, stream, k: int, dev: int):
+    """device ms of k steps of handle H on `stream` (CUDA events), with the
+    clocks sampled during them"""
+    import torch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        H.step(k)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), clk.summary()
+
+
+KERNELS = ["k_dir_x", "k_dir_y", "k_dir_eta", "k_update_stage1", "k_update_stage2"]
+
+
+def kernel_times(H, cfg):
+    """per-launch device ms and share of each step kernel over 2 steps
+    (vh_time_kernels: events around every launch, outside the timed region)"""
+    kt = H.time_kernels(2)
+    launches = {"k_dir_x": 4, "k_dir_y": 4, "k_dir_eta": 0 if cfg.boost_invariant else 4, "k_update_stage1": 2,
+                "k_update_stage2": 2}
+    per_launch = {nm: (kt[q] / launches[nm] if launches[nm] else 0.0) for q, nm in enumerate(KERNELS)}
+    share = {nm: kt[q] / max(sum(kt), 1e-30) for q, nm in enumerate(KERNELS)}
+    top = max(KERNELS, key=lambda nm: kt[KERNELS.index(nm)])
+    return per_launch, share, top
+
+
 def roofline(cfg, precision: str, cells: int, per_launch: dict, share: dict, top: str) -> dict:
     peak, peak_kind = measured_peaks()
     ach = algorithmic_bytes(cfg, top) * cells / (per_launch[top] / 1e3) / 1e9

@@ -44,3 +44,29 @@ def test_both_arms_print_the_same_config():
     assert bench.line_config("glauber_161x161x41", "fp64", 1) == bench.line_config("glauber_161x161x41", "fp64", 1)
     c = bench.line_config("glauber_161x161x41", "fp64", 1)
     assert c["workload"] == "glauber_161x161x41" and c["interior_cells"] == 161 * 161 * 41
+
+
+def test_every_name_bench_uses_is_defined():
+    """bench.py's GPU paths cannot run here; at least every name they load is
+    defined somewhere in the module (a function, an import, an assignment, an
+    argument) or is a builtin"""
+    import ast
+    import builtins
+    with open(os.path.join(ROOT, "bench.py")) as fh:
+        tree = ast.parse(fh.read())
+    defined = set(dir(builtins)) | {"__file__"}
+    for n in ast.walk(tree):
+        if isinstance(n, (ast.FunctionDef, ast.ClassDef)):
+            defined.add(n.name)
+        elif isinstance(n, ast.Import):
+            defined.update(a.asname or a.name.split(".")[0] for a in n.names)
+        elif isinstance(n, ast.ImportFrom):
+            defined.update(a.asname or a.name for a in n.names)
+        elif isinstance(n, ast.Name) and isinstance(n.ctx, (ast.Store, ast.Del)):
+            defined.add(n.id)
+        elif isinstance(n, ast.arg):
+            defined.add(n.arg)
+        elif isinstance(n, ast.ExceptHandler) and n.name:
+            defined.add(n.name)
+    used = {n.id for n in ast.walk(tree) if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Load)}
+    assert not used - defined, sorted(used - defined)
