@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="glauber_161x161x41")
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    p.add_argument("--e2e-steps", type=int, default=8)
+    p.add_argument("--e2e-steps", type=int, default=12)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--precision-report", action="store_true",
                    help="run the workload to tau_end in FP64 and mixed precision; report errors and speedup")
@@ -497,32 +497,39 @@ def run_ours(args, rank, world, dist):
         "clocks": clocks,
         "gpu_launches": launches_per_step * args.steps,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n18 * 8, "d2h_bytes_per_step": n18 * 8,
-                "steps": args.e2e_steps,
-                "what": "every step: vh_set_state of the full 18-field state from pinned host memory, vh_step(1), "
-                        "vh_get_state of the full state into pinned host memory; two handles on two CUDA streams, "
-                        "each driven by its own host thread and each feeding its result back as its next input, "
-                        "take the steps in turn, so one handle's copies overlap the other's (PCIe is full duplex); "
-                        "device time from an event before the first call to one after the last, across both streams",
+                "steps": args.e2e_steps, "handles": E2E_HANDLES,
+                "what": ("every step: vh_set_state of the full 18-field state from pinned host memory, vh_step(1), "
+                         "vh_get_state of the full state into pinned host memory; %d handles on their own CUDA "
+                         "streams, each driven by its own host thread and each feeding its result back as its next "
+                         "input, take the steps in turn, so one handle's copies overlap the others' (PCIe is full "
+                         "duplex); device time from an event before the first call to one after the last, across "
+                         "all the streams" % E2E_HANDLES),
                 "serial_value": e2e_serial,
                 "serial_what": "the same calls on one handle, one step after the other"},
         "roofline": roofline(cfg, args.precision, cells, per_launch, share, top),
     }
 
 
-def e2e_runs(cfg, state0, tau0, steps: int, stream):
+E2E_HANDLES = 3
+
+
+def e2e_runs(cfg, state0, tau0, steps: int, stream, nh: int = E2E_HANDLES):
     """device milliseconds of `steps` end-to-end steps through the C ABI
     (vh_set_state from pinned host memory, vh_step(1), vh_get_state into it):
-    pipelined over two handles and two host threads, and serial on one"""
+    pipelined over nh handles, each on its own stream and host thread, and
+    serial on one.  Each handle's cycle is host-to-device copy, step,
+    device-to-host copy; with three in flight the copy engines of both
+    directions stay busy (two leave gaps)."""
     import threading
     import torch
     from viral_b200 import _abi as A
     from viral_b200.hydro import Hydro
     n18 = state0.size
-    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
-    hs = [Hydro(cfg) for _ in range(2)]
-    bufs = [torch.empty(n18, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+    streams = [torch.cuda.Stream() for _ in range(nh)]
+    hs = [Hydro(cfg) for _ in range(nh)]
+    bufs = [torch.empty(n18, dtype=torch.float64, pin_memory=True).numpy() for _ in range(nh)]
     try:
-        for k in range(2):
+        for k in range(nh):
             A.check(A.lib().vh_set_stream(hs[k].h, ctypes_void_p(streams[k].cuda_stream)), hs[k].h)
             bufs[k][:] = state0
             # one untimed round trip (the transfer buffer is allocated on first use)
@@ -546,18 +553,20 @@ def e2e_runs(cfg, state0, tau0, steps: int, stream):
 
         e0 = torch.cuda.Event(enable_timing=True)
         e0.record(streams[0])
-        streams[1].wait_event(e0)
-        threads = [threading.Thread(target=drive, args=(k, steps // 2 + (steps % 2 if k == 0 else 0)))
-                   for k in range(2)]
+        for k in range(1, nh):
+            streams[k].wait_event(e0)
+        threads = [threading.Thread(target=drive, args=(k, steps // nh + (1 if k < steps % nh else 0)))
+                   for k in range(nh)]
         for t in threads:
             t.start()
         for t in threads:
             t.join()
         if errors:
             raise errors[0]
-        e1 = torch.cuda.Event(enable_timing=True)
-        e1.record(streams[1])
-        streams[0].wait_event(e1)
+        for k in range(1, nh):
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record(streams[k])
+            streams[0].wait_event(e1)
         e2 = torch.cuda.Event(enable_timing=True)
         e2.record(streams[0])
         torch.cuda.synchronize()
