@@ -804,11 +804,16 @@ __device__ __forceinline__ unsigned update_cell(const DevCfg& C, const DevPtrs<R
   return root_cell<R, STAGE>(C, P, tau_n, ts, x, e, u, pu, q9, t_gev);
 }
 
-// one thread per interior cell; 5 blocks per SM (96 registers): the fastest
-// of 5 to 8 on the 161x161x41 event (4, at 128 registers, was slower in an
-// earlier version); fewer registers spill more than the extra warps hide
+// one thread per interior cell.  Blocks per SM: FP64 4 (128 registers),
+// mixed 5 (96 registers); measured on the 161x161x41 event, FP64 per step
+// 1.671 / 1.719 / 1.775 / 1.797 ms at 4 / 5 / 6 / 7 blocks (fewer spills
+// win), mixed 0.975 / 0.957 / 0.977 / 0.977 ms
+template <class R>
+struct UpdOcc {
+  static constexpr int MIN_BLOCKS = sizeof(R) == 8 ? 4 : 5;
+};
 template <class R, int STAGE>
-__global__ void __launch_bounds__(128, 5) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
+__global__ void __launch_bounds__(128, UpdOcc<R>::MIN_BLOCKS) k_update(DevCfg C, DevPtrs<R> P, double tau_n, double ts) {
   pdl_wait_then_release();
   if (*P.status) return;
   const long long nint = (long long)C.nx * C.ny * (C.kr - C.kl);
