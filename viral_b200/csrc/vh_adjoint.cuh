@@ -55,6 +55,35 @@ VH_HD inline void eos_d(const DevCfg& C, R e, R& P, R& dP, R& T, R& dT) {
 
 // ------------------------------------------------------------------ WENO
 
+// the weights' adjoint in the normalised form (alpha_k = d_k / E_k): five
+// reciprocals, but no product of E's, so its range is that of FP32 as well
+template <class R>
+VH_HD inline void weno_wvjp(const R* E, const R* e, const R* ql, const R* qr, R Lbar, R Rbar, R* qlb, R* qrb,
+                            R* eb) {
+  const R dl[3] = {(R)0.3, (R)0.6, (R)0.1}, dr[3] = {(R)0.1, (R)0.6, (R)0.3};
+  // five reciprocals instead of a division per use
+  const R iE[3] = {(R)1 / E[0], (R)1 / E[1], (R)1 / E[2]};
+  R al[3], ar[3], sl = 0, sr = 0;
+  for (int k = 0; k < 3; k++) { al[k] = dl[k] * iE[k]; ar[k] = dr[k] * iE[k]; sl += al[k]; sr += ar[k]; }
+  const R isl = (R)1 / sl, isr = (R)1 / sr;
+  R wl[3], wr[3];
+  for (int k = 0; k < 3; k++) { wl[k] = al[k] * isl; wr[k] = ar[k] * isr; }
+  // candidates
+  const R L6 = Lbar * ((R)1 / (R)6), R6 = Rbar * ((R)1 / (R)6);
+  R wlb[3], wrb[3];
+  for (int k = 0; k < 3; k++) {
+    qlb[k] = wl[k] * L6; qrb[k] = wr[k] * R6;
+    wlb[k] = ql[k] * L6; wrb[k] = qr[k] * R6;
+  }
+  R swl = 0, swr = 0;
+  for (int k = 0; k < 3; k++) { swl += wl[k] * wlb[k]; swr += wr[k] * wrb[k]; }
+  for (int k = 0; k < 3; k++) {
+    const R alb = (wlb[k] - swl) * isl, arb = (wrb[k] - swr) * isr;
+    const R Eb = -(alb * al[k] + arb * ar[k]) * iE[k];
+    eb[k] = Eb * (R)2 * e[k];  // d(e^2) and e = eps + beta: betabar = Ebar 2 e
+  }
+}
+
 // q = (q_{i-2}..q_{i+2}); adjoints Lbar of the face value at i+1/2 and Rbar
 // of the face value at i-1/2 are pulled back into qbar (accumulated)
 template <class R>
@@ -66,32 +95,35 @@ VH_HD inline void weno_lr_vjp(const R* q, R Lbar, R Rbar, R* qbar) {
   const R e[3] = {eps + c13 * a0 * a0 + (R)0.25 * g0 * g0, eps + c13 * a1 * a1 + (R)0.25 * g1 * g1,
                   eps + c13 * a2 * a2 + (R)0.25 * g2 * g2};
   const R E[3] = {e[0] * e[0], e[1] * e[1], e[2] * e[2]};
-  const R dl[3] = {(R)0.3, (R)0.6, (R)0.1}, dr[3] = {(R)0.1, (R)0.6, (R)0.3};
   const R ql[3] = {(R)2 * q[2] + (R)5 * q[3] - q[4], -q[1] + (R)5 * q[2] + (R)2 * q[3],
                    (R)2 * q[0] - (R)7 * q[1] + (R)11 * q[2]};
   const R qr[3] = {(R)11 * q[2] - (R)7 * q[3] + (R)2 * q[4], (R)2 * q[1] + (R)5 * q[2] - q[3],
                    -q[0] + (R)5 * q[1] + (R)2 * q[2]};
-  // five reciprocals instead of a division per use
-  const R iE[3] = {(R)1 / E[0], (R)1 / E[1], (R)1 / E[2]};
-  R al[3], ar[3], sl = 0, sr = 0;
-  for (int k = 0; k < 3; k++) { al[k] = dl[k] * iE[k]; ar[k] = dr[k] * iE[k]; sl += al[k]; sr += ar[k]; }
-  const R isl = (R)1 / sl, isr = (R)1 / sr;
-  R wl[3], wr[3];
-  for (int k = 0; k < 3; k++) { wl[k] = al[k] * isl; wr[k] = ar[k] * isr; }
-  // candidates
-  const R L6 = Lbar * ((R)1 / (R)6), R6 = Rbar * ((R)1 / (R)6);
-  R qlb[3], qrb[3], wlb[3], wrb[3];
-  for (int k = 0; k < 3; k++) {
-    qlb[k] = wl[k] * L6; qrb[k] = wr[k] * R6;
-    wlb[k] = ql[k] * L6; wrb[k] = qr[k] * R6;
-  }
-  R swl = 0, swr = 0;
-  for (int k = 0; k < 3; k++) { swl += wl[k] * wlb[k]; swr += wr[k] * wrb[k]; }
-  R eb[3];
-  for (int k = 0; k < 3; k++) {
-    const R alb = (wlb[k] - swl) * isl, arb = (wrb[k] - swr) * isr;
-    const R Eb = -(alb * al[k] + arb * ar[k]) * iE[k];
-    eb[k] = Eb * (R)2 * e[k];  // d(e^2) and e = eps + beta: betabar = Ebar 2 e
+  R qlb[3], qrb[3], eb[3];
+  if constexpr (sizeof(R) == 8) {
+    // the forward's product form (weights proportional to d_k prod_{j != k}
+    // E_j, both faces' normalisations through one reciprocal): one FP64
+    // reciprocal instead of five; the products stay far inside double range
+    const R P12 = E[1] * E[2], P02 = E[0] * E[2], P01 = E[0] * E[1];
+    const R nl[3] = {(R)0.3 * P12, (R)0.6 * P02, (R)0.1 * P01}, nr[3] = {(R)0.1 * P12, (R)0.6 * P02, (R)0.3 * P01};
+    const R numl = nl[0] * ql[0] + nl[1] * ql[1] + nl[2] * ql[2], denl = (R)6 * (nl[0] + nl[1] + nl[2]);
+    const R numr = nr[0] * qr[0] + nr[1] * qr[1] + nr[2] * qr[2], denr = (R)6 * (nr[0] + nr[1] + nr[2]);
+    const R inv = (R)1 / (denl * denr), idl = denr * inv, idr = denl * inv;
+    const R numlb = Lbar * idl, denlb = -Lbar * numl * idl * idl;
+    const R numrb = Rbar * idr, denrb = -Rbar * numr * idr * idr;
+    R nlb[3], nrb[3];
+    for (int k = 0; k < 3; k++) {
+      qlb[k] = nl[k] * numlb;
+      qrb[k] = nr[k] * numrb;
+      nlb[k] = ql[k] * numlb + (R)6 * denlb;
+      nrb[k] = qr[k] * numrb + (R)6 * denrb;
+    }
+    const R P12b = (R)0.3 * nlb[0] + (R)0.1 * nrb[0], P02b = (R)0.6 * (nlb[1] + nrb[1]),
+            P01b = (R)0.1 * nlb[2] + (R)0.3 * nrb[2];
+    const R Eb[3] = {P02b * E[2] + P01b * E[1], P12b * E[2] + P01b * E[0], P12b * E[1] + P02b * E[0]};
+    for (int k = 0; k < 3; k++) eb[k] = Eb[k] * (R)2 * e[k];
+  } else {
+    weno_wvjp<R>(E, e, ql, qr, Lbar, Rbar, qlb, qrb, eb);
   }
   const R a0b = eb[0] * (R)2 * c13 * a0, g0b = eb[0] * (R)0.5 * g0;
   const R a1b = eb[1] * (R)2 * c13 * a1, g1b = eb[1] * (R)0.5 * g1;
