@@ -255,6 +255,65 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// weno_lr_pair across a warp (FP64): lane a reconstructs both face states of
+// the two quantities of pair array q at line position s.  Neighbouring
+// stencils share terms: the second difference a lane centres on itself is
+// the one the stencil of lane a-1 needs on its right and lane a+1 on its
+// left, and the candidate polynomials 2q_j + 5q_{j+1} - q_{j+2} and
+// -q_{j-1} + 5q_j + 2q_{j+1} of lane a-1's left face are lane a's right-face
+// candidates; each is formed once and passed by shuffle.  Every lane of the
+// warp calls this (the stencil positions are clamped to the line, so lanes
+// whose stencil leaves it form values that nobody uses).  Same weights and
+// single reciprocal as weno_lr_pair.
+__device__ __forceinline__ void weno_lr_pair_warp(const double (*q)[2], int s, int a, double& La, double& Ra,
+                                                  double& Lb, double& Rb) {
+  const int lo = s - a, hi = s - a + 31;
+  double x[5][2];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    int i = s - 2 + k;
+    i = (i < lo || i > hi) ? s : i;
+    const double2 v = ld_pair(q, i);
+    x[k][0] = v.x;
+    x[k][1] = v.y;
+  }
+  const double c13 = 13. / 12., eps = 1e-6;
+  double num[4], den[4];
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const double qm2 = x[0][m], qm1 = x[1][m], qc = x[2][m], qp1 = x[3][m], qp2 = x[4][m];
+    // the squared second difference centred on this lane, and the ones
+    // centred on the neighbours
+    const double d1 = qm1 - 2 * qc + qp1, s1 = d1 * d1;
+    const double s0 = __shfl_down_sync(0xffffffffu, s1, 1), s2 = __shfl_up_sync(0xffffffffu, s1, 1);
+    const double g0 = 3 * qc - 4 * qp1 + qp2, g1 = qm1 - qp1, g2 = qm2 - 4 * qm1 + 3 * qc;
+    const double b0 = fma(c13, s0, 0.25 * (g0 * g0)), b1 = fma(c13, s1, 0.25 * (g1 * g1)),
+                 b2 = fma(c13, s2, 0.25 * (g2 * g2));
+    const double e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+    const double E0 = e0 * e0, E1 = e1 * e1, E2 = e2 * e2;
+    const double P12 = E1 * E2, P02 = E0 * E2, P01 = E0 * E1;
+    const double nl0 = 0.3 * P12, nl1 = 0.6 * P02, nl2 = 0.1 * P01;
+    const double nr0 = 0.1 * P12, nr1 = nl1, nr2 = 0.3 * P01;
+    const double ql0 = 2 * qc + 5 * qp1 - qp2;
+    const double ql1 = -qm1 + 5 * qc + 2 * qp1;
+    const double ql2 = 2 * qm2 - 7 * qm1 + 11 * qc;
+    const double qr0 = 11 * qc - 7 * qp1 + 2 * qp2;
+    const double qr1 = __shfl_up_sync(0xffffffffu, ql0, 1);  // 2 q_{a-1} + 5 q_a - q_{a+1}
+    const double qr2 = __shfl_up_sync(0xffffffffu, ql1, 1);  // -q_{a-2} + 5 q_{a-1} + 2 q_a
+    num[2 * m] = nl0 * ql0 + nl1 * ql1 + nl2 * ql2;
+    den[2 * m] = 6 * (nl0 + nl1 + nl2);
+    num[2 * m + 1] = nr0 * qr0 + nr1 * qr1 + nr2 * qr2;
+    den[2 * m + 1] = 6 * (nr0 + nr1 + nr2);
+  }
+  const double d01 = den[0] * den[1], d23 = den[2] * den[3];
+  const double inv = 1.0 / (d01 * d23);
+  const double i01 = d23 * inv, i23 = d01 * inv;
+  La = num[0] * den[1] * i01;
+  Ra = num[1] * den[0] * i01;
+  Lb = num[2] * den[3] * i23;
+  Rb = num[3] * den[2] * i23;
+}
+
 template <class R>
 __device__ inline R shfl_dn(R v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 template <class R>
@@ -433,22 +492,18 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
             recon_lr<R, 2>(C, &sm.fv[l][0][0], s, fl, fr);
             recon_lr<R, 2>(C, &sm.fv[l][0][1], s, vl, vr);
           }
-        } else if (C.recon == 0) {
-          // F^l and V^l with one reciprocal between them
-          const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.fv[l]);
-          double a_[5], b_[5];
-#pragma unroll
-          for (int k = 0; k < 5; k++) {
-            const double2 v = ld_pair(q, s - 2 + k);
-            a_[k] = v.x;
-            b_[k] = v.y;
-          }
-          double flx, frx, vlx, vrx;
-          weno_lr_pair(a_, b_, flx, frx, vlx, vrx);
-          fl = flx; fr = frx; vl = vlx; vr = vrx;
-        } else {
+        } else if (C.recon != 0) {
           recon_lr<R, 2>(C, &sm.fv[l][0][0], s, fl, fr);
           recon_lr<R, 2>(C, &sm.fv[l][0][1], s, vl, vr);
+        }
+      }
+      if constexpr (sizeof(R) == 8) {
+        if (C.recon == 0) {
+          // F^l and V^l with one reciprocal between them; every lane takes
+          // part (the stencils' shared terms travel by shuffle)
+          double flx, frx, vlx, vrx;
+          weno_lr_pair_warp(reinterpret_cast<const double(*)[2]>(sm.fv[l]), s, a, flx, frx, vlx, vrx);
+          if (stencil) { fl = flx; fr = frx; vl = vlx; vr = vrx; }
         }
       }
       fr = shfl_dn<R>(fr, 1);
@@ -465,11 +520,11 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
     }
     // velocity derivative along DIR: (L - R)/h of the same stencil (genWENOder)
     R dv[4] = {0, 0, 0, 0};
-    if (out) {
 #pragma unroll
-      for (int l = 0; l < 4; l += 2) {
-        R La, Ra, Lb, Rb;
-        if constexpr (sizeof(R) == 4) {
+    for (int l = 0; l < 4; l += 2) {
+      R La = 0, Ra = 0, Lb = 0, Rb = 0;
+      if constexpr (sizeof(R) == 4) {
+        if (out) {
           const float(*q)[2] = reinterpret_cast<const float(*)[2]>(sm.up[l >> 1]);
           F2 L2, R2, x0, x1, x2, x3, x4;
           x0.v = ld_pair(q, s - 2); x1.v = ld_pair(q, s - 1); x2.v = ld_pair(q, s);
@@ -477,17 +532,12 @@ __device__ __forceinline__ void dir_tile(const DevCfg& C, const DevPtrs<R>& P, i
           weno_lr2(x0, x1, x2, x3, x4, L2, R2);
           f2u(L2, La, Lb);
           f2u(R2, Ra, Rb);
-        } else {
-          const double(*q)[2] = reinterpret_cast<const double(*)[2]>(sm.up[l >> 1]);
-          double a_[5], b_[5];
-#pragma unroll
-          for (int k = 0; k < 5; k++) {
-            const double2 v = ld_pair(q, s - 2 + k);
-            a_[k] = v.x;
-            b_[k] = v.y;
-          }
-          weno_lr_pair(a_, b_, La, Ra, Lb, Rb);
         }
+      } else {
+        // every lane takes part (shuffles); the out lanes keep the result
+        weno_lr_pair_warp(reinterpret_cast<const double(*)[2]>(sm.up[l >> 1]), s, a, La, Ra, Lb, Rb);
+      }
+      if (out) {
         dv[l] = (La - Ra) * inv_h;
         dv[l + 1] = (Lb - Rb) * inv_h;
       }
