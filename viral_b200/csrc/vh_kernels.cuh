@@ -1,13 +1,13 @@
 // Kernels of one RK stage of the viscous KT step and its helpers.
 //
 // A stage is D+1 launches (D = 2 or 3 directions):
-//   k_dir<DIR>  one per direction: stages a tile of cells plus 3 halo cells
-//               along DIR in shared memory as (F^DIR, tau T^{tau mu}, pi,
-//               speed), forms WENO5 (or minmod) face states and the KT flux
-//               at every face of the tile, adds the flux difference to the
-//               divergence accumulator, and writes the WENO velocity
-//               derivative along DIR (NEWEST5/hydroKT.h:16-491,
-//               NEWEST5/Source.h:3-101).
+//   k_dir<DIR>  one per direction (k_dir_tma when the tile arrives by TMA
+//               box copies): stages a tile of cells plus 3 halo cells along
+//               DIR in shared memory as (F^DIR, tau T^{tau mu}, pi, speed),
+//               forms WENO5 (or minmod) face states and the KT flux at every
+//               face of the tile, adds the flux difference to the divergence
+//               accumulator, and writes the WENO velocity derivative along
+//               DIR (NEWEST5/hydroKT.h:16-491, NEWEST5/Source.h:3-101).
 //   k_update    one thread per interior cell: sources, RK2 combination,
 //               FP64 root-find, and the ghost copy of boundary cells
 //               (NEWEST5/Source.h:165-433, time.h:1-387, multiroot.h:331-493,
@@ -201,9 +201,11 @@ __device__ __forceinline__ void pdl_wait_then_release() {
 // the 52 arrays back to back.  A tile of the sweep along DIR is two box
 // copies: arrays 0..4 (e, u^mu) and the nine arrays of the conserved set it
 // reads (set A: pi 5..9 then T^{tau mu} 10..13; set B: T^{tau mu} 18..21
-// then pi 22..26).  The box's x start is rounded down to a 16-byte boundary
-// (4 floats, 2 doubles) and the box is wide enough for the tile from there;
-// cells outside the tensor are filled with zeros by the copy and, like the
+// then pi 22..26).  Along x the box's start is rounded down to a 16-byte
+// boundary (4 floats, 2 doubles) and the box is wide enough for the tile
+// from there; across x (the y and eta sweeps) the tile starts on a multiple
+// of NC cells of the padded row, so the box is exactly the tile's NC lines.
+// Cells outside the tensor are filled with zeros by the copy and, like the
 // cells outside the grid, never used.
 template <class R, int DIR, int NC>
 struct TmaBox {
