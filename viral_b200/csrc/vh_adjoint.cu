@@ -1,5 +1,6 @@
 // Discrete adjoint of the viscous KT step for boost-invariant Milne grids
-// (2+1D, WENO5, copy boundaries): gradients of the momentum anisotropy
+// (2+1D, WENO5, copy boundaries; 3+1D grids: vh_adjoint3.cu, dispatched from
+// vh_adjoint_eps_p below): gradients of the momentum anisotropy
 // eps_p = sum(T^xx - T^yy) / sum(T^xx + T^yy) at the final time with
 // respect to the initial state and to the eta/s(T) parameters.
 //

@@ -1,5 +1,7 @@
 // Pieces shared by the discrete adjoints (boost-invariant and 3+1D): the
-// workspace carve, the recording forward step and the phase clock.
+// workspace carve, the recording forward step, the phase clock, the
+// observable's sums and the fixed-order sum of the per-cell parameter
+// gradients.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -67,8 +69,8 @@ struct PhaseClock {
 };
 
 // momentum anisotropy: per-block partial sums of T^xx - T^yy and T^xx + T^yy
-// over the interior cells (every eta slice of a 3+1D grid)
-// over the interior cells, then one fixed-order sum (deterministic)
+// over the interior cells (every eta slice of a 3+1D grid), then one
+// fixed-order sum (deterministic)
 constexpr int kObsBlocks = 148;
 template <class R>
 __global__ void __launch_bounds__(256) k_obs_part(DevCfg C, const R* S, long long n, double* part) {
